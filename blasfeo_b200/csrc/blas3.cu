@@ -1,0 +1,395 @@
+// Level-3 (and the level-2 pieces the solve chains need) on panel-major
+// device matrices: gemm_nt, syrk_ln, trsm_rltn, trmm_rlnn, gemv_n, trsv_lnn,
+// trsv_ltn.  Single-instance, uniform-batch and variable-size-batch entry
+// points share one kernel per routine.
+//
+// gemm_nt / syrk_ln (blasfeo_hp_pm/d_blas3_lib4.c:727, :5400): D = beta*C +
+// alpha*A*B^T, syrk writing only the lower triangle.  One CTA computes a BMxBN
+// output tile of one instance; K is walked in BK-deep slices staged in shared
+// memory (coalesced loads: a 4-row panel slice is one contiguous run), each
+// thread accumulates a TMxTN register tile.  C is read only when beta != 0
+// (as the HP AVX2 kernels do).
+#include "common.cuh"
+#include "kernels.cuh"
+
+namespace {
+
+template <typename T, int BM, int BN, int BK, int TM, int TN, bool LOWER>
+__global__ void __launch_bounds__((BM / TM) * (BN / TN))
+k_gemm_nt(SizeArg sz, T alpha, MatArg<T> A, MatArg<T> B, T beta, MatArg<T> C, MatArg<T> D, int tiles_n) {
+	constexpr int NT = (BM / TM) * (BN / TN);
+	constexpr int PADA = 16 / sizeof(T) * 2;  // keeps 16-byte alignment, staggers banks
+	__shared__ __align__(16) T sA[BK][BM + PADA];
+	__shared__ __align__(16) T sB[BK][BN + PADA];
+
+	// grid.x = instance (up to 2^31-1 instances), grid.y = output tile
+	const int b = blockIdx.x;
+	const int m = sz.M(b), n = sz.N(b), k = sz.K(b);
+	const int tmi = blockIdx.y / tiles_n, tni = blockIdx.y % tiles_n;
+	const int i0 = tmi * BM, j0 = tni * BN;
+	if (i0 >= m || j0 >= n) return;
+	if (LOWER && j0 > i0 + BM - 1) return;
+	const PMat<T> a = A.get(b), bm = B.get(b), c = C.get(b), d = D.get(b);
+
+	const int tid = threadIdx.x;
+	const int tx = tid % (BN / TN), ty = tid / (BN / TN);
+	T acc[TM][TN];
+#pragma unroll
+	for (int r = 0; r < TM; r++)
+#pragma unroll
+		for (int q = 0; q < TN; q++) acc[r][q] = T(0);
+
+	for (int k0 = 0; k0 < k; k0 += BK) {
+		// element e of the slice -> (row, col): 4 consecutive e are the 4 rows of
+		// one panel column, so consecutive threads read consecutive addresses
+		for (int e = tid; e < BM * BK; e += NT) {
+			int p = e / (4 * BK), rem = e % (4 * BK);
+			int kk = rem >> 2, r = p * 4 + (rem & 3);
+			int gi = i0 + r, gk = k0 + kk;
+			sA[kk][r] = (gi < m && gk < k) ? a.at(gi, gk) : T(0);
+		}
+		for (int e = tid; e < BN * BK; e += NT) {
+			int p = e / (4 * BK), rem = e % (4 * BK);
+			int kk = rem >> 2, r = p * 4 + (rem & 3);
+			int gj = j0 + r, gk = k0 + kk;
+			sB[kk][r] = (gj < n && gk < k) ? bm.at(gj, gk) : T(0);
+		}
+		__syncthreads();
+#pragma unroll 4
+		for (int kk = 0; kk < BK; kk++) {
+			T av[TM], bv[TN];
+#pragma unroll
+			for (int r = 0; r < TM; r++) av[r] = sA[kk][ty * TM + r];
+#pragma unroll
+			for (int q = 0; q < TN; q++) bv[q] = sB[kk][tx * TN + q];
+#pragma unroll
+			for (int r = 0; r < TM; r++)
+#pragma unroll
+				for (int q = 0; q < TN; q++) acc[r][q] = fma(av[r], bv[q], acc[r][q]);
+		}
+		__syncthreads();
+	}
+#pragma unroll
+	for (int r = 0; r < TM; r++) {
+		int gi = i0 + ty * TM + r;
+		if (gi >= m) continue;
+#pragma unroll
+		for (int q = 0; q < TN; q++) {
+			int gj = j0 + tx * TN + q;
+			if (gj >= n) continue;
+			if (LOWER && gj > gi) continue;
+			T v = alpha * acc[r][q];
+			if (beta != T(0)) v = fma(beta, c.at(gi, gj), v);
+			d.at(gi, gj) = v;
+		}
+	}
+}
+
+template <typename T, int BM, int BN, int BK, int TM, int TN, bool LOWER>
+int launch_gemm_cfg(int batch, SizeArg sz, int max_m, int max_n, T alpha, MatArg<T> A, MatArg<T> B, T beta,
+                    MatArg<T> C, MatArg<T> D, cudaStream_t s) {
+	int tm = cdiv(max_m, BM), tn = cdiv(max_n, BN);
+	dim3 grid(batch, tm * tn);
+	k_gemm_nt<T, BM, BN, BK, TM, TN, LOWER><<<grid, (BM / TM) * (BN / TN), 0, s>>>(sz, alpha, A, B, beta, C, D, tn);
+	return bf::check_launch();
+}
+
+}  // namespace
+
+namespace bf {
+
+template <typename T, bool LOWER>
+int gemm_nt_launch(int batch, SizeArg sz, int max_m, int max_n, int max_k, T alpha, MatArg<T> A, MatArg<T> B,
+                   T beta, MatArg<T> C, MatArg<T> D, cudaStream_t s, int variant) {
+	if (batch <= 0 || max_m <= 0 || max_n <= 0) return BLASFEO_B200_OK;
+	if (variant < 0) {
+		int mx = max_m > max_n ? max_m : max_n;
+		variant = mx > 48 ? 2 : (mx > 16 ? 1 : 0);
+	}
+	(void)max_k;
+	switch (variant) {
+	case 0: return launch_gemm_cfg<T, 16, 16, 16, 2, 2, LOWER>(batch, sz, max_m, max_n, alpha, A, B, beta, C, D, s);
+	case 1: return launch_gemm_cfg<T, 32, 32, 16, 2, 2, LOWER>(batch, sz, max_m, max_n, alpha, A, B, beta, C, D, s);
+	case 2: return launch_gemm_cfg<T, 64, 64, 16, 4, 4, LOWER>(batch, sz, max_m, max_n, alpha, A, B, beta, C, D, s);
+	default: return launch_gemm_cfg<T, 32, 32, 16, 4, 4, LOWER>(batch, sz, max_m, max_n, alpha, A, B, beta, C, D, s);
+	}
+}
+template int gemm_nt_launch<double, false>(int, SizeArg, int, int, int, double, MatArg<double>, MatArg<double>, double,
+                                           MatArg<double>, MatArg<double>, cudaStream_t, int);
+template int gemm_nt_launch<double, true>(int, SizeArg, int, int, int, double, MatArg<double>, MatArg<double>, double,
+                                          MatArg<double>, MatArg<double>, cudaStream_t, int);
+template int gemm_nt_launch<float, false>(int, SizeArg, int, int, int, float, MatArg<float>, MatArg<float>, float,
+                                          MatArg<float>, MatArg<float>, cudaStream_t, int);
+template int gemm_nt_launch<float, true>(int, SizeArg, int, int, int, float, MatArg<float>, MatArg<float>, float,
+                                         MatArg<float>, MatArg<float>, cudaStream_t, int);
+
+}  // namespace bf
+
+namespace {
+
+// dA[l] = 1 / A(l,l): the inverse diagonal trsm_rltn multiplies by
+// (blasfeo_hp_pm/d_blas3_lib4.c:4162-4178)
+template <typename T>
+__global__ void k_invdiag(SizeArg sz, MatArg<T> A) {
+	int b = blockIdx.x;
+	int n = sz.N(b);
+	int l = blockIdx.y * blockDim.x + threadIdx.x;
+	if (l >= n) return;
+	PMat<T> a = A.get(b);
+	a.d[l] = T(1) / a.at(l, l);
+}
+
+// D = alpha * B * A^{-T}, A lower non-unit: one thread per row of D, columns
+// left to right, each column multiplied by the cached inverse diagonal
+// (kernel/generic/kernel_dgemm_4x4_lib4.c:5970 kernel_dtrsm_nt_rl_inv).
+template <typename T>
+__global__ void k_trsm_rltn(SizeArg sz, T alpha, MatArg<T> A, MatArg<T> B, MatArg<T> D) {
+	int b = blockIdx.x;
+	int m = sz.M(b), n = sz.N(b);
+	int i = blockIdx.y * blockDim.x + threadIdx.x;
+	if (i >= m) return;
+	PMat<T> a = A.get(b), bb = B.get(b), d = D.get(b);
+	const T *inv = a.d;
+	for (int j = 0; j < n; j++) {
+		T c = alpha * bb.at(i, j);
+		for (int l = 0; l < j; l++) c = fma(-d.at(i, l), a.at(j, l), c);
+		d.at(i, j) = c * inv[j];
+	}
+}
+
+// D = alpha * B * A, A lower non-unit (blasfeo_hp_pm/d_blas3_lib4.c:4893).
+// D must not alias B.
+template <typename T>
+__global__ void k_trmm_rlnn(SizeArg sz, T alpha, MatArg<T> A, MatArg<T> B, MatArg<T> D) {
+	int b = blockIdx.x;
+	int m = sz.M(b), n = sz.N(b);
+	long long idx = (long long)blockIdx.y * blockDim.x + threadIdx.x;
+	if (idx >= (long long)m * n) return;
+	int i = (int)(idx % m), j = (int)(idx / m);
+	PMat<T> a = A.get(b), bb = B.get(b), d = D.get(b);
+	T c = T(0);
+	for (int l = j; l < n; l++) c = fma(bb.at(i, l), a.at(l, j), c);
+	d.at(i, j) = alpha * c;
+}
+
+template <typename T>
+__global__ void k_gemv_n(int m, int n, T alpha, PMat<T> a, const T *x, T beta, const T *y, T *z) {
+	int i = blockIdx.x * blockDim.x + threadIdx.x;
+	if (i >= m) return;
+	T c = T(0);
+	for (int l = 0; l < n; l++) c = fma(a.at(i, l), x[l], c);
+	z[i] = alpha * c + beta * y[i];
+}
+
+// triangular solves with one warp: lane r owns rows r, r+32, ...; each step
+// broadcasts the freshly solved unknown.
+template <typename T, bool TRANS>
+__global__ void k_trsv_l(int m, PMat<T> a, const T *x, T *z) {
+	extern __shared__ __align__(16) unsigned char smem_raw[];
+	T *w = (T *)smem_raw;
+	int lane = threadIdx.x;
+	for (int i = lane; i < m; i += 32) w[i] = x[i];
+	__syncwarp();
+	if (!TRANS) {
+		for (int j = 0; j < m; j++) {
+			T zj = w[j] * (T(1) / a.at(j, j));
+			__syncwarp();
+			for (int i = j + 1 + lane; i < m; i += 32) w[i] = fma(-a.at(i, j), zj, w[i]);
+			if (lane == 0) w[j] = zj;
+			__syncwarp();
+		}
+	} else {
+		for (int j = m - 1; j >= 0; j--) {
+			T zj = w[j] * (T(1) / a.at(j, j));
+			__syncwarp();
+			for (int i = lane; i < j; i += 32) w[i] = fma(-a.at(j, i), zj, w[i]);
+			if (lane == 0) w[j] = zj;
+			__syncwarp();
+		}
+	}
+	for (int i = lane; i < m; i += 32) z[i] = w[i];
+}
+
+template <typename T>
+int trsm_core(int batch, int m, int n, T alpha, MatArg<T> A, int ai, int aj, int *use_dA, MatArg<T> B, MatArg<T> D,
+              cudaStream_t s) {
+	SizeArg sz = uniform_sizes(m, n, 0);
+	// inverse diagonal of A into A's dA, reused when already valid
+	bool need = !(ai == 0 && aj == 0 && *use_dA >= n);
+	if (need) {
+		k_invdiag<T><<<dim3(batch, cdiv(n, 128)), 128, 0, s>>>(sz, A);
+		*use_dA = (ai == 0 && aj == 0) ? n : 0;
+	}
+	k_trsm_rltn<T><<<dim3(batch, cdiv(m, 64)), 64, 0, s>>>(sz, alpha, A, B, D);
+	return bf::check_launch();
+}
+
+template <typename T, typename S>
+void gemm_single(int m, int n, int k, T alpha, S *sA, int ai, int aj, S *sB, int bi, int bj, T beta, S *sC, int ci,
+                 int cj, S *sD, int di, int dj, bool lower) {
+	if (m <= 0 || n <= 0) return;
+	sD->use_dA = 0;
+	SizeArg sz = uniform_sizes(m, n, k);
+	MatArg<T> A = single_arg<T>(sA, ai, aj), B = single_arg<T>(sB, bi, bj), C = single_arg<T>(sC, ci, cj),
+	          D = single_arg<T>(sD, di, dj);
+	if (lower)
+		bf::gemm_nt_launch<T, true>(1, sz, m, n, k, alpha, A, B, beta, C, D, bf::cur_stream(), -1);
+	else
+		bf::gemm_nt_launch<T, false>(1, sz, m, n, k, alpha, A, B, beta, C, D, bf::cur_stream(), -1);
+	bf::finish_single();
+}
+
+template <typename T, typename BT>
+int gemm_batch(int batch, int m, int n, int k, T alpha, BT *sA, int ai, int aj, BT *sB, int bi, int bj, T beta,
+               BT *sC, int ci, int cj, BT *sD, int di, int dj, void *stream, bool lower) {
+	if (batch < 0 || !sA || !sB || !sC || !sD) return BLASFEO_B200_EINVAL;
+	if (m <= 0 || n <= 0 || batch == 0) return BLASFEO_B200_OK;
+	sD->use_dA = 0;
+	SizeArg sz = uniform_sizes(m, n, k);
+	MatArg<T> A = batch_arg<T>(sA, ai, aj), B = batch_arg<T>(sB, bi, bj), C = batch_arg<T>(sC, ci, cj),
+	          D = batch_arg<T>(sD, di, dj);
+	if (lower) return bf::gemm_nt_launch<T, true>(batch, sz, m, n, k, alpha, A, B, beta, C, D, (cudaStream_t)stream, -1);
+	return bf::gemm_nt_launch<T, false>(batch, sz, m, n, k, alpha, A, B, beta, C, D, (cudaStream_t)stream, -1);
+}
+
+template <typename T, typename S>
+void trsm_single(int m, int n, T alpha, S *sA, int ai, int aj, S *sB, int bi, int bj, S *sD, int di, int dj) {
+	if (m <= 0 || n <= 0) return;
+	sD->use_dA = 0;
+	trsm_core<T>(1, m, n, alpha, single_arg<T>(sA, ai, aj), ai, aj, &sA->use_dA, single_arg<T>(sB, bi, bj),
+	             single_arg<T>(sD, di, dj), bf::cur_stream());
+	bf::finish_single();
+}
+
+template <typename T, typename BT>
+int trsm_batch(int batch, int m, int n, T alpha, BT *sA, int ai, int aj, BT *sB, int bi, int bj, BT *sD, int di,
+               int dj, void *stream) {
+	if (batch < 0 || !sA || !sB || !sD) return BLASFEO_B200_EINVAL;
+	if (m <= 0 || n <= 0 || batch == 0) return BLASFEO_B200_OK;
+	sD->use_dA = 0;
+	return trsm_core<T>(batch, m, n, alpha, batch_arg<T>(sA, ai, aj), ai, aj, &sA->use_dA, batch_arg<T>(sB, bi, bj),
+	                    batch_arg<T>(sD, di, dj), (cudaStream_t)stream);
+}
+
+template <typename T, typename S>
+void trmm_single(int m, int n, T alpha, S *sA, int ai, int aj, S *sB, int bi, int bj, S *sD, int di, int dj) {
+	if (m <= 0 || n <= 0) return;
+	sD->use_dA = 0;
+	long long tot = (long long)m * n;
+	k_trmm_rlnn<T><<<dim3(1, (unsigned)((tot + 127) / 128)), 128, 0, bf::cur_stream()>>>(
+	    uniform_sizes(m, n, 0), alpha, single_arg<T>(sA, ai, aj), single_arg<T>(sB, bi, bj), single_arg<T>(sD, di, dj));
+	bf::finish_single();
+}
+
+PMat<double> pm1(struct blasfeo_dmat *s, int ri, int cj) {
+	PMat<double> p;
+	p.p = s->pA;
+	p.d = s->dA;
+	p.cn = s->cn;
+	p.ri = ri;
+	p.cj = cj;
+	return p;
+}
+
+}  // namespace
+
+extern "C" {
+
+void blasfeo_dgemm_nt(int m, int n, int k, double alpha, struct blasfeo_dmat *sA, int ai, int aj,
+                      struct blasfeo_dmat *sB, int bi, int bj, double beta, struct blasfeo_dmat *sC, int ci, int cj,
+                      struct blasfeo_dmat *sD, int di, int dj) {
+	gemm_single<double>(m, n, k, alpha, sA, ai, aj, sB, bi, bj, beta, sC, ci, cj, sD, di, dj, false);
+}
+void blasfeo_dsyrk_ln(int m, int k, double alpha, struct blasfeo_dmat *sA, int ai, int aj, struct blasfeo_dmat *sB,
+                      int bi, int bj, double beta, struct blasfeo_dmat *sC, int ci, int cj, struct blasfeo_dmat *sD,
+                      int di, int dj) {
+	gemm_single<double>(m, m, k, alpha, sA, ai, aj, sB, bi, bj, beta, sC, ci, cj, sD, di, dj, true);
+}
+void blasfeo_sgemm_nt(int m, int n, int k, float alpha, struct blasfeo_smat *sA, int ai, int aj,
+                      struct blasfeo_smat *sB, int bi, int bj, float beta, struct blasfeo_smat *sC, int ci, int cj,
+                      struct blasfeo_smat *sD, int di, int dj) {
+	gemm_single<float>(m, n, k, alpha, sA, ai, aj, sB, bi, bj, beta, sC, ci, cj, sD, di, dj, false);
+}
+void blasfeo_ssyrk_ln(int m, int k, float alpha, struct blasfeo_smat *sA, int ai, int aj, struct blasfeo_smat *sB,
+                      int bi, int bj, float beta, struct blasfeo_smat *sC, int ci, int cj, struct blasfeo_smat *sD,
+                      int di, int dj) {
+	gemm_single<float>(m, m, k, alpha, sA, ai, aj, sB, bi, bj, beta, sC, ci, cj, sD, di, dj, true);
+}
+void blasfeo_dtrsm_rltn(int m, int n, double alpha, struct blasfeo_dmat *sA, int ai, int aj, struct blasfeo_dmat *sB,
+                        int bi, int bj, struct blasfeo_dmat *sD, int di, int dj) {
+	trsm_single<double>(m, n, alpha, sA, ai, aj, sB, bi, bj, sD, di, dj);
+}
+void blasfeo_strsm_rltn(int m, int n, float alpha, struct blasfeo_smat *sA, int ai, int aj, struct blasfeo_smat *sB,
+                        int bi, int bj, struct blasfeo_smat *sD, int di, int dj) {
+	trsm_single<float>(m, n, alpha, sA, ai, aj, sB, bi, bj, sD, di, dj);
+}
+void blasfeo_dtrmm_rlnn(int m, int n, double alpha, struct blasfeo_dmat *sA, int ai, int aj, struct blasfeo_dmat *sB,
+                        int bi, int bj, struct blasfeo_dmat *sD, int di, int dj) {
+	trmm_single<double>(m, n, alpha, sA, ai, aj, sB, bi, bj, sD, di, dj);
+}
+void blasfeo_strmm_rlnn(int m, int n, float alpha, struct blasfeo_smat *sA, int ai, int aj, struct blasfeo_smat *sB,
+                        int bi, int bj, struct blasfeo_smat *sD, int di, int dj) {
+	trmm_single<float>(m, n, alpha, sA, ai, aj, sB, bi, bj, sD, di, dj);
+}
+
+void blasfeo_dgemv_n(int m, int n, double alpha, struct blasfeo_dmat *sA, int ai, int aj, struct blasfeo_dvec *sx,
+                     int xi, double beta, struct blasfeo_dvec *sy, int yi, struct blasfeo_dvec *sz, int zi) {
+	if (m <= 0) return;
+	k_gemv_n<double><<<cdiv(m, 128), 128, 0, bf::cur_stream()>>>(m, n, alpha, pm1(sA, ai, aj), sx->pa + xi, beta,
+	                                                              sy->pa + yi, sz->pa + zi);
+	bf::finish_single();
+}
+void blasfeo_dtrsv_lnn(int m, struct blasfeo_dmat *sA, int ai, int aj, struct blasfeo_dvec *sx, int xi,
+                       struct blasfeo_dvec *sz, int zi) {
+	if (m <= 0) return;
+	k_trsv_l<double, false><<<1, 32, m * sizeof(double), bf::cur_stream()>>>(m, pm1(sA, ai, aj), sx->pa + xi, sz->pa + zi);
+	bf::finish_single();
+}
+void blasfeo_dtrsv_ltn(int m, struct blasfeo_dmat *sA, int ai, int aj, struct blasfeo_dvec *sx, int xi,
+                       struct blasfeo_dvec *sz, int zi) {
+	if (m <= 0) return;
+	k_trsv_l<double, true><<<1, 32, m * sizeof(double), bf::cur_stream()>>>(m, pm1(sA, ai, aj), sx->pa + xi, sz->pa + zi);
+	bf::finish_single();
+}
+
+int blasfeo_dgemm_nt_batch(int batch, int m, int n, int k, double alpha, struct blasfeo_dmat_batch *sA, int ai, int aj,
+                           struct blasfeo_dmat_batch *sB, int bi, int bj, double beta, struct blasfeo_dmat_batch *sC,
+                           int ci, int cj, struct blasfeo_dmat_batch *sD, int di, int dj, void *stream) {
+	return gemm_batch<double>(batch, m, n, k, alpha, sA, ai, aj, sB, bi, bj, beta, sC, ci, cj, sD, di, dj, stream, false);
+}
+int blasfeo_dsyrk_ln_batch(int batch, int m, int k, double alpha, struct blasfeo_dmat_batch *sA, int ai, int aj,
+                           struct blasfeo_dmat_batch *sB, int bi, int bj, double beta, struct blasfeo_dmat_batch *sC,
+                           int ci, int cj, struct blasfeo_dmat_batch *sD, int di, int dj, void *stream) {
+	return gemm_batch<double>(batch, m, m, k, alpha, sA, ai, aj, sB, bi, bj, beta, sC, ci, cj, sD, di, dj, stream, true);
+}
+int blasfeo_sgemm_nt_batch(int batch, int m, int n, int k, float alpha, struct blasfeo_smat_batch *sA, int ai, int aj,
+                           struct blasfeo_smat_batch *sB, int bi, int bj, float beta, struct blasfeo_smat_batch *sC,
+                           int ci, int cj, struct blasfeo_smat_batch *sD, int di, int dj, void *stream) {
+	return gemm_batch<float>(batch, m, n, k, alpha, sA, ai, aj, sB, bi, bj, beta, sC, ci, cj, sD, di, dj, stream, false);
+}
+int blasfeo_ssyrk_ln_batch(int batch, int m, int k, float alpha, struct blasfeo_smat_batch *sA, int ai, int aj,
+                           struct blasfeo_smat_batch *sB, int bi, int bj, float beta, struct blasfeo_smat_batch *sC,
+                           int ci, int cj, struct blasfeo_smat_batch *sD, int di, int dj, void *stream) {
+	return gemm_batch<float>(batch, m, m, k, alpha, sA, ai, aj, sB, bi, bj, beta, sC, ci, cj, sD, di, dj, stream, true);
+}
+int blasfeo_dtrsm_rltn_batch(int batch, int m, int n, double alpha, struct blasfeo_dmat_batch *sA, int ai, int aj,
+                             struct blasfeo_dmat_batch *sB, int bi, int bj, struct blasfeo_dmat_batch *sD, int di,
+                             int dj, void *stream) {
+	return trsm_batch<double>(batch, m, n, alpha, sA, ai, aj, sB, bi, bj, sD, di, dj, stream);
+}
+int blasfeo_strsm_rltn_batch(int batch, int m, int n, float alpha, struct blasfeo_smat_batch *sA, int ai, int aj,
+                             struct blasfeo_smat_batch *sB, int bi, int bj, struct blasfeo_smat_batch *sD, int di,
+                             int dj, void *stream) {
+	return trsm_batch<float>(batch, m, n, alpha, sA, ai, aj, sB, bi, bj, sD, di, dj, stream);
+}
+
+int blasfeo_dgemm_nt_vbatch(int batch, const int *m, const int *n, const int *k, int max_m, int max_n, int max_k,
+                            double alpha, const struct blasfeo_dmat *sA, const struct blasfeo_dmat *sB, double beta,
+                            const struct blasfeo_dmat *sC, const struct blasfeo_dmat *sD, void *stream) {
+	if (batch < 0 || !m || !n || !k || !sA || !sB || !sC || !sD) return BLASFEO_B200_EINVAL;
+	return bf::gemm_nt_launch<double, false>(batch, var_sizes(m, n, k), max_m, max_n, max_k, alpha,
+	                                         vbatch_arg<double>(sA), vbatch_arg<double>(sB), beta,
+	                                         vbatch_arg<double>(sC), vbatch_arg<double>(sD), (cudaStream_t)stream, -1);
+}
+
+}  // extern "C"

@@ -1,0 +1,16 @@
+// Launchers shared between translation units.
+#pragma once
+#include "common.cuh"
+
+namespace bf {
+
+// D = beta*C + alpha*A*B^T (LOWER: lower triangle only); variant < 0 picks a tile by size
+template <typename T, bool LOWER>
+int gemm_nt_launch(int batch, SizeArg sz, int max_m, int max_n, int max_k, T alpha, MatArg<T> A, MatArg<T> B,
+                   T beta, MatArg<T> C, MatArg<T> D, cudaStream_t s, int variant);
+
+// D = chol(C) lower, inverse diagonal into D's dA, info (device, may be null)
+template <typename T>
+int potrf_launch(int batch, SizeArg sz, int max_m, MatArg<T> C, MatArg<T> D, int *info, cudaStream_t s);
+
+}  // namespace bf

@@ -1,0 +1,552 @@
+// LAPACK-level routines on panel-major device matrices: potrf_l,
+// syrk_dpotrf_ln, getrf_rp, geqrf (single, uniform batch, variable batch).
+// One CTA factors one instance.
+//
+// potrf_l (blasfeo_hp_pm/d_lapack_lib4.c:918): when the lower triangle fits in
+// shared memory the matrix is loaded once (coalesced 4-row panel runs),
+// factored there by chol_smem (chol.cuh) and written back once: HBM traffic is
+// one read and one write of the lower triangle.  Larger matrices use an
+// unblocked right-looking factorization directly in global memory (L1/L2
+// resident for BLASFEO-sized problems).
+//
+// getrf_rp (blasfeo_hp_pm/d_lapack_lib4.c:2396): right-looking LU with row
+// pivoting; per column a CTA-wide argmax (first index of the largest |a|,
+// kernel/generic/kernel_dgetrf_pivot_lib4.c:84), a full-row swap, scaling by
+// the reciprocal pivot (0 for a zero pivot) and a rank-1 update.  The
+// element-wise operation order equals the reference's (one subtraction per
+// earlier column, in column order).
+//
+// geqrf (blasfeo_hp_pm/d_lapack_lib4.c:3444): Householder QR, one reflector
+// per column with LAPACK dlarfg signs (kernel/generic/kernel_dgeqrf_4_lib4.c:
+// 80-96); the column norm is a CTA reduction in the working precision, the
+// reflector is applied to every trailing column by one thread per column.
+#include <climits>
+
+#include "chol.cuh"
+#include "common.cuh"
+#include "kernels.cuh"
+
+namespace {
+
+__host__ __device__ inline size_t align16(size_t x) { return (x + 15) / 16 * 16; }
+
+// shared-memory plan of the potrf kernel for matrices up to max_n
+struct PotrfSmem {
+	size_t s_bytes, dinv_off, invl_off, scratch_off, bad_off, total;
+};
+template <typename T>
+__host__ __device__ inline PotrfSmem potrf_smem_plan(int max_n) {
+	PotrfSmem p;
+	int P = (max_n + 3) / 4;
+	p.s_bytes = align16((size_t)lp_size(max_n) * sizeof(T));
+	p.dinv_off = p.s_bytes;
+	p.invl_off = p.dinv_off + align16((size_t)4 * P * sizeof(double));
+	p.scratch_off = p.invl_off + align16(256 * sizeof(T));
+	p.bad_off = p.scratch_off + align16(16 * 17 * sizeof(double));
+	p.total = p.bad_off + 16;
+	return p;
+}
+
+// load the lower triangle of C (n x n at the view's offsets) into lower panels,
+// identity in the padding
+template <typename T>
+__device__ void load_lower_panels(T *S, int n, const PMat<T> &c) {
+	const int P = (n + 3) >> 2;
+	const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+	for (int p = warp; p < P; p += nw) {
+		T *dst = S + lp_off(p);
+		const int cnt = 16 * (p + 1);
+		for (int e = lane; e < cnt; e += 32) {
+			int i = 4 * p + (e & 3), j = e >> 2;
+			T v;
+			if (i < n && j < n)
+				v = (j <= i) ? c.at(i, j) : T(0);
+			else
+				v = (i == j) ? T(1) : T(0);
+			dst[e] = v;
+		}
+	}
+}
+
+// write the lower triangle (j <= i < n) of the lower panels into D
+template <typename T>
+__device__ void store_lower_panels(const T *S, int n, const PMat<T> &d) {
+	const int P = (n + 3) >> 2;
+	const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+	for (int p = warp; p < P; p += nw) {
+		const T *src = S + lp_off(p);
+		const int cnt = 16 * (p + 1);
+		for (int e = lane; e < cnt; e += 32) {
+			int i = 4 * p + (e & 3), j = e >> 2;
+			if (i < n && j <= i) d.at(i, j) = src[e];
+		}
+	}
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256) k_potrf_smem(SizeArg sz, MatArg<T> C, MatArg<T> D, int *info, int max_n) {
+	extern __shared__ __align__(16) unsigned char smem[];
+	const int b = blockIdx.x;
+	const int n = sz.M(b);
+	if (n <= 0) return;
+	PotrfSmem pl = potrf_smem_plan<T>(max_n);
+	T *S = (T *)smem;
+	double *dinv = (double *)(smem + pl.dinv_off);
+	T *invL = (T *)(smem + pl.invl_off);
+	double *scratch = (double *)(smem + pl.scratch_off);
+	int *bad = (int *)(smem + pl.bad_off);
+	const PMat<T> c = C.get(b), d = D.get(b);
+	if (threadIdx.x == 0) *bad = 0;
+	load_lower_panels<T>(S, n, c);
+	__syncthreads();
+	chol_smem<T>(S, n, dinv, invL, 0, scratch, bad);
+	store_lower_panels<T>(S, n, d);
+	for (int j = threadIdx.x; j < n; j += blockDim.x) d.d[j] = (T)dinv[j];
+	if (info && threadIdx.x == 0) info[b] = *bad;
+}
+
+// unblocked right-looking Cholesky in global memory (any size)
+template <typename T>
+__global__ void __launch_bounds__(256) k_potrf_global(SizeArg sz, MatArg<T> C, MatArg<T> D, int *info) {
+	__shared__ double s_inv;
+	__shared__ int s_bad;
+	const int b = blockIdx.x;
+	const int n = sz.M(b);
+	if (n <= 0) return;
+	const PMat<T> c = C.get(b), d = D.get(b);
+	const int tid = threadIdx.x, nt = blockDim.x;
+	for (long long e = tid; e < (long long)n * n; e += nt) {
+		int i = (int)(e % n), j = (int)(e / n);
+		if (j <= i) d.at(i, j) = c.at(i, j);
+	}
+	if (tid == 0) s_bad = 0;
+	__syncthreads();
+	for (int j = 0; j < n; j++) {
+		if (tid == 0) {
+			double dd, inv;
+			double cc = (double)d.at(j, j);
+			chol_pivot(cc, dd, inv);
+			if (!(cc > 0.0) && s_bad == 0) s_bad = j + 1;
+			d.at(j, j) = (T)dd;
+			d.d[j] = (T)inv;
+			s_inv = inv;
+		}
+		__syncthreads();
+		const T inv = (T)s_inv;
+		for (int i = j + 1 + tid; i < n; i += nt) d.at(i, j) *= inv;
+		__syncthreads();
+		const int r = n - j - 1;
+		for (long long e = tid; e < (long long)r * r; e += nt) {
+			int i = j + 1 + (int)(e % r), l = j + 1 + (int)(e / r);
+			if (l <= i) d.at(i, l) = fma(-d.at(i, j), d.at(l, j), d.at(i, l));
+		}
+		__syncthreads();
+	}
+	if (info && tid == 0) info[b] = s_bad;
+}
+
+// CTA-wide argmax of |x| with first-index tie-break; returns index (valid in all threads)
+template <typename T>
+__device__ int block_argmax_first(T v, int idx, int *s_idx, T *s_val) {
+	const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+#pragma unroll
+	for (int off = 16; off > 0; off >>= 1) {
+		T ov = __shfl_down_sync(0xffffffffu, v, off);
+		int oi = __shfl_down_sync(0xffffffffu, idx, off);
+		if (ov > v || (ov == v && oi < idx)) {
+			v = ov;
+			idx = oi;
+		}
+	}
+	if (lane == 0) {
+		s_val[warp] = v;
+		s_idx[warp] = idx;
+	}
+	__syncthreads();
+	if (threadIdx.x == 0) {
+		T bv = s_val[0];
+		int bi = s_idx[0];
+		for (int w = 1; w < nw; w++)
+			if (s_val[w] > bv || (s_val[w] == bv && s_idx[w] < bi)) {
+				bv = s_val[w];
+				bi = s_idx[w];
+			}
+		s_idx[32] = bi;
+	}
+	__syncthreads();
+	int r = s_idx[32];
+	__syncthreads();
+	return r;
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256) k_getrf_global(SizeArg sz, MatArg<T> C, MatArg<T> D, int *ipiv,
+                                                       long long ipiv_stride, int *info) {
+	__shared__ int s_idx[33];
+	__shared__ T s_val[32];
+	__shared__ int s_bad;
+	const int b = blockIdx.x;
+	const int m = sz.M(b), n = sz.N(b);
+	if (m <= 0 || n <= 0) return;
+	const PMat<T> c = C.get(b), d = D.get(b);
+	const int tid = threadIdx.x, nt = blockDim.x;
+	int *piv = ipiv + ipiv_stride * b;
+	for (long long e = tid; e < (long long)m * n; e += nt) {
+		int i = (int)(e % m), j = (int)(e / m);
+		d.at(i, j) = c.at(i, j);
+	}
+	if (tid == 0) s_bad = 0;
+	__syncthreads();
+	const int mn = m < n ? m : n;
+	for (int j = 0; j < mn; j++) {
+		// pivot search over rows j..m-1
+		T best = T(-1);
+		int bi = INT_MAX;
+		for (int i = j + tid; i < m; i += nt) {
+			T a = dev_abs(d.at(i, j));
+			if (a > best) {
+				best = a;
+				bi = i;
+			}
+		}
+		const int ip = block_argmax_first<T>(best, bi, s_idx, s_val);
+		if (ip != j)
+			for (int l = tid; l < n; l += nt) {
+				T t = d.at(j, l);
+				d.at(j, l) = d.at(ip, l);
+				d.at(ip, l) = t;
+			}
+		__syncthreads();
+		const T p = d.at(j, j);
+		const T inv = (p != T(0)) ? T(1) / p : T(0);
+		if (tid == 0) {
+			piv[j] = ip;
+			d.d[j] = inv;
+			if (p == T(0) && s_bad == 0) s_bad = j + 1;
+		}
+		for (int i = j + 1 + tid; i < m; i += nt) d.at(i, j) *= inv;
+		__syncthreads();
+		const int rm = m - j - 1, rn = n - j - 1;
+		for (long long e = tid; e < (long long)rm * rn; e += nt) {
+			int i = j + 1 + (int)(e % rm), l = j + 1 + (int)(e / rm);
+			d.at(i, l) = fma(-d.at(i, j), d.at(j, l), d.at(i, l));
+		}
+		__syncthreads();
+	}
+	if (info && tid == 0) info[b] = s_bad;
+}
+
+template <typename T>
+__device__ T block_sum(T v, T *s_red) {
+	const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+#pragma unroll
+	for (int off = 16; off > 0; off >>= 1) v += __shfl_down_sync(0xffffffffu, v, off);
+	if (lane == 0) s_red[warp] = v;
+	__syncthreads();
+	if (threadIdx.x == 0) {
+		T s = T(0);
+		for (int w = 0; w < nw; w++) s += s_red[w];
+		s_red[32] = s;
+	}
+	__syncthreads();
+	T r = s_red[32];
+	__syncthreads();
+	return r;
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256) k_geqrf_global(SizeArg sz, MatArg<T> C, MatArg<T> D) {
+	__shared__ T s_red[33];
+	__shared__ T s_tau, s_sc, s_beta;
+	const int b = blockIdx.x;
+	const int m = sz.M(b), n = sz.N(b);
+	if (m <= 0 || n <= 0) return;
+	const PMat<T> c = C.get(b), d = D.get(b);
+	T *tau = d.d + d.ri;
+	const int tid = threadIdx.x, nt = blockDim.x;
+	for (long long e = tid; e < (long long)m * n; e += nt) {
+		int i = (int)(e % m), j = (int)(e / m);
+		d.at(i, j) = c.at(i, j);
+	}
+	__syncthreads();
+	const int kmax = m < n ? m : n;
+	for (int j = 0; j < kmax; j++) {
+		T part = T(0);
+		for (int i = j + 1 + tid; i < m; i += nt) {
+			T x = d.at(i, j);
+			part = fma(x, x, part);
+		}
+		const T s = block_sum<T>(part, s_red);
+		if (tid == 0) {
+			if (s == T(0)) {
+				s_tau = T(0);
+				s_sc = T(1);
+				s_beta = d.at(j, j);
+			} else {
+				T alpha = d.at(j, j);
+				T beta = sqrt(fma(alpha, alpha, s));
+				if (alpha > T(0)) beta = -beta;
+				s_tau = (beta - alpha) / beta;
+				s_sc = T(1) / (alpha - beta);
+				s_beta = beta;
+			}
+			tau[j] = s_tau;
+		}
+		__syncthreads();
+		const T t = s_tau;
+		if (s != T(0)) {
+			for (int i = j + 1 + tid; i < m; i += nt) d.at(i, j) *= s_sc;
+			if (tid == 0) d.at(j, j) = s_beta;
+		}
+		__syncthreads();
+		for (int col = j + 1 + tid; col < n; col += nt) {
+			T w = d.at(j, col);
+			for (int i = j + 1; i < m; i++) w = fma(d.at(i, j), d.at(i, col), w);
+			w = -t * w;
+			d.at(j, col) += w;
+			for (int i = j + 1; i < m; i++) d.at(i, col) = fma(w, d.at(i, j), d.at(i, col));
+		}
+		__syncthreads();
+	}
+}
+
+}  // namespace
+
+namespace bf {
+
+template <typename T>
+int potrf_launch(int batch, SizeArg sz, int max_m, MatArg<T> C, MatArg<T> D, int *info, cudaStream_t s) {
+	if (batch <= 0 || max_m <= 0) return BLASFEO_B200_OK;
+	PotrfSmem pl = potrf_smem_plan<T>(max_m);
+	if (pl.total <= max_smem_optin()) {
+		if (pl.total > 48 * 1024)
+			cudaFuncSetAttribute(k_potrf_smem<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pl.total);
+		int threads = max_m <= 32 ? 64 : (max_m <= 96 ? 128 : 256);
+		k_potrf_smem<T><<<batch, threads, pl.total, s>>>(sz, C, D, info, max_m);
+	} else {
+		k_potrf_global<T><<<batch, 256, 0, s>>>(sz, C, D, info);
+	}
+	return check_launch();
+}
+template int potrf_launch<double>(int, SizeArg, int, MatArg<double>, MatArg<double>, int *, cudaStream_t);
+template int potrf_launch<float>(int, SizeArg, int, MatArg<float>, MatArg<float>, int *, cudaStream_t);
+
+}  // namespace bf
+
+namespace {
+
+template <typename T, typename S>
+void potrf_single(int m, S *sC, int ci, int cj, S *sD, int di, int dj) {
+	if (m <= 0) return;
+	sD->use_dA = (di == 0 && dj == 0) ? m : 0;
+	bf::potrf_launch<T>(1, uniform_sizes(m, m, 0), m, single_arg<T>(sC, ci, cj), single_arg<T>(sD, di, dj), nullptr,
+	                    bf::cur_stream());
+	bf::finish_single();
+}
+
+template <typename T, typename BT>
+int potrf_batch(int batch, int m, BT *sC, int ci, int cj, BT *sD, int di, int dj, int *info, void *stream) {
+	if (batch < 0 || !sC || !sD) return BLASFEO_B200_EINVAL;
+	if (m <= 0 || batch == 0) return BLASFEO_B200_OK;
+	sD->use_dA = (di == 0 && dj == 0) ? m : 0;
+	return bf::potrf_launch<T>(batch, uniform_sizes(m, m, 0), m, batch_arg<T>(sC, ci, cj), batch_arg<T>(sD, di, dj),
+	                           info, (cudaStream_t)stream);
+}
+
+template <typename T, typename S>
+void syrk_potrf_single(int m, int k, S *sA, int ai, int aj, S *sB, int bi, int bj, S *sC, int ci, int cj, S *sD,
+                       int di, int dj) {
+	if (m <= 0) return;
+	cudaStream_t s = bf::cur_stream();
+	MatArg<T> D = single_arg<T>(sD, di, dj);
+	bf::gemm_nt_launch<T, true>(1, uniform_sizes(m, m, k), m, m, k, T(1), single_arg<T>(sA, ai, aj),
+	                            single_arg<T>(sB, bi, bj), T(1), single_arg<T>(sC, ci, cj), D, s, -1);
+	sD->use_dA = (di == 0 && dj == 0) ? m : 0;
+	bf::potrf_launch<T>(1, uniform_sizes(m, m, 0), m, D, D, nullptr, s);
+	bf::finish_single();
+}
+
+template <typename T, typename BT>
+int syrk_potrf_batch(int batch, int m, int k, BT *sA, int ai, int aj, BT *sB, int bi, int bj, BT *sC, int ci, int cj,
+                     BT *sD, int di, int dj, int *info, void *stream) {
+	if (batch < 0 || !sA || !sB || !sC || !sD) return BLASFEO_B200_EINVAL;
+	if (m <= 0 || batch == 0) return BLASFEO_B200_OK;
+	cudaStream_t s = (cudaStream_t)stream;
+	MatArg<T> D = batch_arg<T>(sD, di, dj);
+	int st = bf::gemm_nt_launch<T, true>(batch, uniform_sizes(m, m, k), m, m, k, T(1), batch_arg<T>(sA, ai, aj),
+	                                     batch_arg<T>(sB, bi, bj), T(1), batch_arg<T>(sC, ci, cj), D, s, -1);
+	if (st) return st;
+	sD->use_dA = (di == 0 && dj == 0) ? m : 0;
+	return bf::potrf_launch<T>(batch, uniform_sizes(m, m, 0), m, D, D, info, s);
+}
+
+template <typename T>
+int getrf_launch(int batch, SizeArg sz, MatArg<T> C, MatArg<T> D, int *ipiv, long long ipiv_stride, int *info,
+                 cudaStream_t s) {
+	k_getrf_global<T><<<batch, 256, 0, s>>>(sz, C, D, ipiv, ipiv_stride, info);
+	return bf::check_launch();
+}
+
+template <typename T, typename S>
+void getrf_single(int m, int n, S *sC, int ci, int cj, S *sD, int di, int dj, int *ipiv) {
+	if (m <= 0 || n <= 0) return;
+	if (!ipiv) {
+		bf::set_error(BLASFEO_B200_EINVAL);
+		return;
+	}
+	sD->use_dA = (di == 0 && dj == 0) ? 1 : 0;
+	cudaStream_t s = bf::cur_stream();
+	int mn = m < n ? m : n;
+	int *dpiv = (int *)bf::workspace(mn * sizeof(int), s);
+	if (!dpiv) {
+		bf::set_error(BLASFEO_B200_ENOMEM);
+		return;
+	}
+	getrf_launch<T>(1, uniform_sizes(m, n, 0), single_arg<T>(sC, ci, cj), single_arg<T>(sD, di, dj), dpiv, 0, nullptr, s);
+	if (bf::check_launch() != BLASFEO_B200_OK) return;
+	// the pivot vector is a host array in the reference API: always complete the copy
+	if (cudaMemcpyAsync(ipiv, dpiv, mn * sizeof(int), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+	    cudaStreamSynchronize(s) != cudaSuccess)
+		bf::set_error(BLASFEO_B200_ECUDA);
+}
+
+template <typename T, typename BT>
+int getrf_batch(int batch, int m, int n, BT *sC, int ci, int cj, BT *sD, int di, int dj, int *ipiv, int *info,
+                void *stream) {
+	if (batch < 0 || !sC || !sD || !ipiv) return BLASFEO_B200_EINVAL;
+	if (m <= 0 || n <= 0 || batch == 0) return BLASFEO_B200_OK;
+	sD->use_dA = (di == 0 && dj == 0) ? 1 : 0;
+	int mn = m < n ? m : n;
+	return getrf_launch<T>(batch, uniform_sizes(m, n, 0), batch_arg<T>(sC, ci, cj), batch_arg<T>(sD, di, dj), ipiv, mn,
+	                       info, (cudaStream_t)stream);
+}
+
+template <typename T, typename S>
+void geqrf_single(int m, int n, S *sC, int ci, int cj, S *sD, int di, int dj) {
+	if (m <= 0 || n <= 0) return;
+	sD->use_dA = 0;
+	k_geqrf_global<T><<<1, 256, 0, bf::cur_stream()>>>(uniform_sizes(m, n, 0), single_arg<T>(sC, ci, cj),
+	                                                   single_arg<T>(sD, di, dj));
+	bf::finish_single();
+}
+
+template <typename T, typename BT>
+int geqrf_batch(int batch, int m, int n, BT *sC, int ci, int cj, BT *sD, int di, int dj, void *stream) {
+	if (batch < 0 || !sC || !sD) return BLASFEO_B200_EINVAL;
+	if (m <= 0 || n <= 0 || batch == 0) return BLASFEO_B200_OK;
+	sD->use_dA = 0;
+	k_geqrf_global<T><<<batch, 256, 0, (cudaStream_t)stream>>>(uniform_sizes(m, n, 0), batch_arg<T>(sC, ci, cj),
+	                                                             batch_arg<T>(sD, di, dj));
+	return bf::check_launch();
+}
+
+// geqrf work size of the HP reference (blasfeo_hp_pm/d_lapack_lib4.c:3433-3440)
+template <typename T>
+int geqrf_ws(int m, int n) {
+	int cm = (m + 3) / 4 * 4;
+	int cn = (n + 3) / 4 * 4;
+	return 4 * (cm + cn) * (int)sizeof(T);
+}
+
+}  // namespace
+
+extern "C" {
+
+void blasfeo_dpotrf_l(int m, struct blasfeo_dmat *sC, int ci, int cj, struct blasfeo_dmat *sD, int di, int dj) {
+	potrf_single<double>(m, sC, ci, cj, sD, di, dj);
+}
+void blasfeo_spotrf_l(int m, struct blasfeo_smat *sC, int ci, int cj, struct blasfeo_smat *sD, int di, int dj) {
+	potrf_single<float>(m, sC, ci, cj, sD, di, dj);
+}
+void blasfeo_dsyrk_dpotrf_ln(int m, int k, struct blasfeo_dmat *sA, int ai, int aj, struct blasfeo_dmat *sB, int bi,
+                             int bj, struct blasfeo_dmat *sC, int ci, int cj, struct blasfeo_dmat *sD, int di, int dj) {
+	syrk_potrf_single<double>(m, k, sA, ai, aj, sB, bi, bj, sC, ci, cj, sD, di, dj);
+}
+void blasfeo_ssyrk_spotrf_ln(int m, int k, struct blasfeo_smat *sA, int ai, int aj, struct blasfeo_smat *sB, int bi,
+                             int bj, struct blasfeo_smat *sC, int ci, int cj, struct blasfeo_smat *sD, int di, int dj) {
+	syrk_potrf_single<float>(m, k, sA, ai, aj, sB, bi, bj, sC, ci, cj, sD, di, dj);
+}
+void blasfeo_dgetrf_rp(int m, int n, struct blasfeo_dmat *sC, int ci, int cj, struct blasfeo_dmat *sD, int di, int dj,
+                       int *ipiv) {
+	getrf_single<double>(m, n, sC, ci, cj, sD, di, dj, ipiv);
+}
+void blasfeo_sgetrf_rp(int m, int n, struct blasfeo_smat *sC, int ci, int cj, struct blasfeo_smat *sD, int di, int dj,
+                       int *ipiv) {
+	getrf_single<float>(m, n, sC, ci, cj, sD, di, dj, ipiv);
+}
+int blasfeo_dgeqrf_worksize(int m, int n) { return geqrf_ws<double>(m, n); }
+int blasfeo_sgeqrf_worksize(int m, int n) { return geqrf_ws<float>(m, n); }
+void blasfeo_dgeqrf(int m, int n, struct blasfeo_dmat *sC, int ci, int cj, struct blasfeo_dmat *sD, int di, int dj,
+                    void *work) {
+	(void)work;
+	geqrf_single<double>(m, n, sC, ci, cj, sD, di, dj);
+}
+void blasfeo_sgeqrf(int m, int n, struct blasfeo_smat *sC, int ci, int cj, struct blasfeo_smat *sD, int di, int dj,
+                    void *work) {
+	(void)work;
+	geqrf_single<float>(m, n, sC, ci, cj, sD, di, dj);
+}
+
+int blasfeo_dpotrf_l_batch(int batch, int m, struct blasfeo_dmat_batch *sC, int ci, int cj,
+                           struct blasfeo_dmat_batch *sD, int di, int dj, int *info, void *stream) {
+	return potrf_batch<double>(batch, m, sC, ci, cj, sD, di, dj, info, stream);
+}
+int blasfeo_spotrf_l_batch(int batch, int m, struct blasfeo_smat_batch *sC, int ci, int cj,
+                           struct blasfeo_smat_batch *sD, int di, int dj, int *info, void *stream) {
+	return potrf_batch<float>(batch, m, sC, ci, cj, sD, di, dj, info, stream);
+}
+int blasfeo_dsyrk_dpotrf_ln_batch(int batch, int m, int k, struct blasfeo_dmat_batch *sA, int ai, int aj,
+                                  struct blasfeo_dmat_batch *sB, int bi, int bj, struct blasfeo_dmat_batch *sC, int ci,
+                                  int cj, struct blasfeo_dmat_batch *sD, int di, int dj, int *info, void *stream) {
+	return syrk_potrf_batch<double>(batch, m, k, sA, ai, aj, sB, bi, bj, sC, ci, cj, sD, di, dj, info, stream);
+}
+int blasfeo_ssyrk_spotrf_ln_batch(int batch, int m, int k, struct blasfeo_smat_batch *sA, int ai, int aj,
+                                  struct blasfeo_smat_batch *sB, int bi, int bj, struct blasfeo_smat_batch *sC, int ci,
+                                  int cj, struct blasfeo_smat_batch *sD, int di, int dj, int *info, void *stream) {
+	return syrk_potrf_batch<float>(batch, m, k, sA, ai, aj, sB, bi, bj, sC, ci, cj, sD, di, dj, info, stream);
+}
+int blasfeo_dgetrf_rp_batch(int batch, int m, int n, struct blasfeo_dmat_batch *sC, int ci, int cj,
+                            struct blasfeo_dmat_batch *sD, int di, int dj, int *ipiv, int *info, void *stream) {
+	return getrf_batch<double>(batch, m, n, sC, ci, cj, sD, di, dj, ipiv, info, stream);
+}
+int blasfeo_sgetrf_rp_batch(int batch, int m, int n, struct blasfeo_smat_batch *sC, int ci, int cj,
+                            struct blasfeo_smat_batch *sD, int di, int dj, int *ipiv, int *info, void *stream) {
+	return getrf_batch<float>(batch, m, n, sC, ci, cj, sD, di, dj, ipiv, info, stream);
+}
+int blasfeo_dgeqrf_batch(int batch, int m, int n, struct blasfeo_dmat_batch *sC, int ci, int cj,
+                         struct blasfeo_dmat_batch *sD, int di, int dj, void *stream) {
+	return geqrf_batch<double>(batch, m, n, sC, ci, cj, sD, di, dj, stream);
+}
+int blasfeo_sgeqrf_batch(int batch, int m, int n, struct blasfeo_smat_batch *sC, int ci, int cj,
+                         struct blasfeo_smat_batch *sD, int di, int dj, void *stream) {
+	return geqrf_batch<float>(batch, m, n, sC, ci, cj, sD, di, dj, stream);
+}
+
+int blasfeo_dpotrf_l_vbatch(int batch, const int *m, int max_m, const struct blasfeo_dmat *sC,
+                            const struct blasfeo_dmat *sD, int *info, void *stream) {
+	if (batch < 0 || !m || !sC || !sD) return BLASFEO_B200_EINVAL;
+	return bf::potrf_launch<double>(batch, var_sizes(m, m, nullptr), max_m, vbatch_arg<double>(sC),
+	                                vbatch_arg<double>(sD), info, (cudaStream_t)stream);
+}
+int blasfeo_dgetrf_rp_vbatch(int batch, const int *m, const int *n, int max_m, int max_n,
+                             const struct blasfeo_dmat *sC, const struct blasfeo_dmat *sD, int *ipiv, int ipiv_stride,
+                             int *info, void *stream) {
+	if (batch < 0 || !m || !n || !sC || !sD || !ipiv) return BLASFEO_B200_EINVAL;
+	(void)max_m;
+	(void)max_n;
+	if (batch == 0) return BLASFEO_B200_OK;
+	return getrf_launch<double>(batch, var_sizes(m, n, nullptr), vbatch_arg<double>(sC), vbatch_arg<double>(sD), ipiv,
+	                            ipiv_stride, info, (cudaStream_t)stream);
+}
+int blasfeo_dgeqrf_vbatch(int batch, const int *m, const int *n, int max_m, int max_n, const struct blasfeo_dmat *sC,
+                          const struct blasfeo_dmat *sD, void *stream) {
+	if (batch < 0 || !m || !n || !sC || !sD) return BLASFEO_B200_EINVAL;
+	(void)max_m;
+	(void)max_n;
+	if (batch == 0) return BLASFEO_B200_OK;
+	k_geqrf_global<double><<<batch, 256, 0, (cudaStream_t)stream>>>(var_sizes(m, n, nullptr), vbatch_arg<double>(sC),
+	                                                                 vbatch_arg<double>(sD));
+	return bf::check_launch();
+}
+
+}  // extern "C"

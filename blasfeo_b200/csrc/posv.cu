@@ -1,0 +1,671 @@
+// Fused factor + solve for variable-size batches of SPD systems A x = b.
+//
+// The chain being fused is the reference's dpotrf_l followed by dtrsv_lnn and
+// dtrsv_ltn (blasfeo_hp_pm/d_lapack_lib4.c:918; blasfeo_hp_pm/d_blas2_lib4.c).
+// One CTA solves one system at a time and is persistent: it pulls systems from
+// a list sorted by decreasing n (largest first), one list per size class, each
+// class launched with the shared memory its largest member needs.
+//
+//   plain (T = double): lower triangle -> shared memory (lower panels, one HBM
+//     read), chol_smem, blocked forward/backward substitution (16x16 diagonal
+//     blocks by warp shuffles), x written once.  Matrices whose FP64 lower
+//     panels do not fit shared memory take the global-memory path
+//     (k_posv_global) instead.
+//   mixed (T = float): lower triangle converted to FP32 in shared memory,
+//     chol_smem with FP64 diagonal blocks (pivots, reciprocals, block
+//     inverses), then iterative refinement: residual r = b - A x in FP64 from
+//     the FP64 matrix in global memory (L2-resident while the CTA works on
+//     it), correction solves in FP32 with the stored block inverses, x += d in
+//     FP64, stopping when ||r||_inf <= tol * ||A||_inf * ||x||_inf.
+#include <climits>
+
+#include "chol.cuh"
+#include "common.cuh"
+#include "kernels.cuh"
+
+namespace {
+
+constexpr int POSV_MAX_CLASSES = 8;
+
+struct ClassTable {
+	int nclass;
+	int upper[POSV_MAX_CLASSES];  // inclusive upper bound of n per class (ascending)
+};
+
+// workspace: [0] list (batch ints)  [then] per class: start, count, counter
+struct PosvWs {
+	int *list;
+	int *start;
+	int *count;
+	int *counter;
+	int *hist;  // 1 + max n buckets
+};
+
+__host__ __device__ inline size_t a16(size_t x) { return (x + 15) / 16 * 16; }
+
+// Sort systems by decreasing n (counting sort over n) and split into classes.
+// Single CTA.
+__global__ void k_posv_classify(int batch, const int *__restrict__ nvec, int max_n, ClassTable ct, PosvWs ws) {
+	extern __shared__ int sh[];
+	int *hist = sh;               // max_n + 2 buckets
+	int *off = sh + (max_n + 2);  // max_n + 2
+	const int tid = threadIdx.x, nt = blockDim.x;
+	for (int i = tid; i < max_n + 2; i += nt) hist[i] = 0;
+	__syncthreads();
+	for (int i = tid; i < batch; i += nt) {
+		int n = nvec[i];
+		n = n < 0 ? 0 : (n > max_n ? max_n + 1 : n);
+		atomicAdd(&hist[n], 1);
+	}
+	__syncthreads();
+	if (tid == 0) {
+		// descending n: bucket max_n+1 (oversize) first ... bucket 0 last
+		int acc = 0;
+		for (int v = max_n + 1; v >= 0; v--) {
+			off[v] = acc;
+			acc += hist[v];
+		}
+		for (int c = 0; c < ct.nclass; c++) {
+			int lo = (c == 0) ? 1 : ct.upper[c - 1] + 1;
+			int hi = ct.upper[c];
+			if (c == ct.nclass - 1) hi = max_n + 1;  // last class takes oversize too (kernel rejects)
+			int s = INT_MAX, cnt = 0;
+			for (int v = hi; v >= lo; v--) {
+				if (hist[v]) {
+					if (off[v] < s) s = off[v];
+					cnt += hist[v];
+				}
+			}
+			ws.start[c] = (cnt ? s : 0);
+			ws.count[c] = cnt;
+			ws.counter[c] = 0;
+		}
+	}
+	__syncthreads();
+	for (int i = tid; i < batch; i += nt) {
+		int n = nvec[i];
+		n = n < 0 ? 0 : (n > max_n ? max_n + 1 : n);
+		int pos = atomicAdd(&off[n], 1);
+		ws.list[pos] = i;
+	}
+}
+
+// shared-memory plan of the posv kernel
+struct PosvPlan {
+	size_t S_off, inv_off, dinv_off, scr_off, w_off, x_off, r_off, ybuf_off, misc_off, total;
+};
+template <typename T, bool MIXED>
+__host__ __device__ inline PosvPlan posv_plan(int max_n) {
+	PosvPlan p;
+	const int P = (max_n + 3) / 4;
+	const int NB = (max_n + 15) / 16;
+	const int nv = NB * 16;
+	p.S_off = 0;
+	p.inv_off = p.S_off + a16((size_t)lp_size(max_n) * sizeof(T));
+	p.dinv_off = p.inv_off + a16((size_t)(MIXED ? NB : 1) * 256 * sizeof(T));
+	p.scr_off = p.dinv_off + a16((size_t)4 * P * sizeof(double));
+	p.w_off = p.scr_off + a16(16 * 17 * sizeof(double));
+	p.x_off = p.w_off + a16((size_t)nv * sizeof(T));
+	p.r_off = p.x_off + (MIXED ? a16((size_t)nv * sizeof(double)) : 0);
+	p.ybuf_off = p.r_off + (MIXED ? a16((size_t)nv * sizeof(double)) : 0);
+	p.misc_off = p.ybuf_off + a16(16 * sizeof(T));
+	p.total = p.misc_off + 64 * sizeof(double);
+	return p;
+}
+
+// Forward substitution w := L^{-1} w on the lower panels, 16-row blocks.
+// With block inverses (invL_all != null) the diagonal block is a 16x16
+// product; otherwise warp 0 substitutes with the FP64 reciprocal pivots.
+template <typename T>
+__device__ void trsv_fwd(const T *S, int n, const T *invL_all, const double *dinv, T *w, T *ybuf) {
+	const int tid = threadIdx.x, nt = blockDim.x;
+	const int NB = (n + 15) >> 4;
+	for (int K = 0; K < NB; K++) {
+		const int c0 = 16 * K;
+		const int nbk = min(16, n - c0);
+		if (invL_all) {
+			if (tid < 16) {
+				const T *inv = invL_all + (size_t)K * 256;
+				T s = T(0);
+#pragma unroll
+				for (int l = 0; l < 16; l++)
+					if (l <= tid) s = fma(inv[tid * 16 + l], w[c0 + l], s);
+				ybuf[tid] = (tid < nbk) ? s : T(0);
+			}
+		} else if (tid < 32) {
+			const int lane = tid;
+			T v = (lane < nbk) ? w[c0 + lane] : T(0);
+			for (int k = 0; k < nbk; k++) {
+				T yk = __shfl_sync(0xffffffffu, v, k) * (T)dinv[c0 + k];
+				if (lane == k) v = yk;
+				if (lane > k && lane < nbk) v = fma(-S[lp_off((c0 + lane) >> 2) + 4 * (c0 + k) + ((c0 + lane) & 3)], yk, v);
+			}
+			if (lane < 16) ybuf[lane] = (lane < nbk) ? v : T(0);
+		}
+		__syncthreads();
+		for (int r = c0 + 16 + tid; r < n; r += nt) {
+			const T *row = S + lp_off(r >> 2) + 4 * c0 + (r & 3);
+			T s = w[r];
+#pragma unroll
+			for (int l = 0; l < 16; l++) s = fma(-row[4 * l], ybuf[l], s);
+			w[r] = s;
+		}
+		if (tid < nbk) w[c0 + tid] = ybuf[tid];
+		__syncthreads();
+	}
+}
+
+// Backward substitution w := L^{-T} w.
+template <typename T>
+__device__ void trsv_bwd(const T *S, int n, const T *invL_all, const double *dinv, T *w, T *ybuf) {
+	const int tid = threadIdx.x, nt = blockDim.x;
+	const int NB = (n + 15) >> 4;
+	for (int K = NB - 1; K >= 0; K--) {
+		const int c0 = 16 * K;
+		const int nbk = min(16, n - c0);
+		if (invL_all) {
+			if (tid < 16) {
+				const T *inv = invL_all + (size_t)K * 256;
+				T s = T(0);
+#pragma unroll
+				for (int l = 0; l < 16; l++)
+					if (l >= tid && l < nbk) s = fma(inv[l * 16 + tid], w[c0 + l], s);
+				ybuf[tid] = (tid < nbk) ? s : T(0);
+			}
+		} else if (tid < 32) {
+			const int lane = tid;
+			T v = (lane < nbk) ? w[c0 + lane] : T(0);
+			for (int k = nbk - 1; k >= 0; k--) {
+				T xk = __shfl_sync(0xffffffffu, v, k) * (T)dinv[c0 + k];
+				if (lane == k) v = xk;
+				if (lane < k) v = fma(-S[lp_off((c0 + k) >> 2) + 4 * (c0 + lane) + ((c0 + k) & 3)], xk, v);
+			}
+			if (lane < 16) ybuf[lane] = (lane < nbk) ? v : T(0);
+		}
+		__syncthreads();
+		for (int j = tid; j < c0; j += nt) {
+			T s = w[j];
+			for (int k = 0; k < nbk; k++) {
+				const int r = c0 + k;
+				s = fma(-S[lp_off(r >> 2) + 4 * j + (r & 3)], ybuf[k], s);
+			}
+			w[j] = s;
+		}
+		if (tid < nbk) w[c0 + tid] = ybuf[tid];
+		__syncthreads();
+	}
+}
+
+template <typename T>
+__device__ double block_max(double v, double *red) {
+	const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+#pragma unroll
+	for (int off = 16; off > 0; off >>= 1) v = fmax(v, __shfl_down_sync(0xffffffffu, v, off));
+	if (lane == 0) red[warp] = v;
+	__syncthreads();
+	if (threadIdx.x == 0) {
+		double m = 0.0;
+		for (int w = 0; w < nw; w++) m = fmax(m, red[w]);
+		red[32] = m;
+	}
+	__syncthreads();
+	double r = red[32];
+	__syncthreads();
+	return r;
+}
+
+// r = b - A x (FP64), A symmetric given by its lower triangle in global
+// memory; one warp per 4-row tile row, lanes over 4x4 tiles (128-byte
+// contiguous loads), transposed contributions accumulated with shared
+// atomics.  Also returns the row sums of |A| in asum when want_norm.
+__device__ void sym_residual(const PMat<double> &a, int n, const double *b, const double *x, double *r,
+                             double *asum, bool want_norm) {
+	const int tid = threadIdx.x, nt = blockDim.x;
+	const int lane = tid & 31, warp = tid >> 5, nw = nt >> 5;
+	const int P = (n + 3) >> 2;
+	for (int i = tid; i < 4 * P; i += nt) {
+		r[i] = (i < n) ? b[i] : 0.0;
+		if (want_norm) asum[i] = 0.0;
+	}
+	__syncthreads();
+	for (int ti = warp; ti < P; ti += nw) {
+		double acc0 = 0.0, acc1 = 0.0, acc2 = 0.0, acc3 = 0.0;
+		double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
+		const double xi0 = x[4 * ti], xi1 = x[4 * ti + 1], xi2 = x[4 * ti + 2], xi3 = x[4 * ti + 3];
+		const double *prow = a.p + (size_t)(4 * ti) * a.cn;
+		for (int tj = lane; tj <= ti; tj += 32) {
+			const double *t = prow + 16 * tj;
+			double e[16];
+#pragma unroll
+			for (int q = 0; q < 8; q++) {
+				double2 v = __ldg((const double2 *)(t + 2 * q));
+				e[2 * q] = v.x;
+				e[2 * q + 1] = v.y;
+			}
+			// mask entries outside the matrix (padding rows/cols may hold anything)
+#pragma unroll
+			for (int q = 0; q < 4; q++)
+#pragma unroll
+				for (int rr = 0; rr < 4; rr++) {
+					int gi = 4 * ti + rr, gj = 4 * tj + q;
+					bool ok = gi < n && gj < n && (tj < ti || gj <= gi);
+					if (!ok) e[4 * q + rr] = 0.0;
+				}
+			const double xj0 = x[4 * tj], xj1 = x[4 * tj + 1], xj2 = x[4 * tj + 2], xj3 = x[4 * tj + 3];
+			// rows of ti: A_tile * x_tj
+			acc0 = fma(e[0], xj0, fma(e[4], xj1, fma(e[8], xj2, fma(e[12], xj3, acc0))));
+			acc1 = fma(e[1], xj0, fma(e[5], xj1, fma(e[9], xj2, fma(e[13], xj3, acc1))));
+			acc2 = fma(e[2], xj0, fma(e[6], xj1, fma(e[10], xj2, fma(e[14], xj3, acc2))));
+			acc3 = fma(e[3], xj0, fma(e[7], xj1, fma(e[11], xj2, fma(e[15], xj3, acc3))));
+			if (want_norm) {
+				s0 += fabs(e[0]) + fabs(e[4]) + fabs(e[8]) + fabs(e[12]);
+				s1 += fabs(e[1]) + fabs(e[5]) + fabs(e[9]) + fabs(e[13]);
+				s2 += fabs(e[2]) + fabs(e[6]) + fabs(e[10]) + fabs(e[14]);
+				s3 += fabs(e[3]) + fabs(e[7]) + fabs(e[11]) + fabs(e[15]);
+			}
+			if (tj < ti) {
+				// transposed part: rows of tj get A_tile^T * x_ti
+				double c0 = fma(e[0], xi0, fma(e[1], xi1, fma(e[2], xi2, e[3] * xi3)));
+				double c1 = fma(e[4], xi0, fma(e[5], xi1, fma(e[6], xi2, e[7] * xi3)));
+				double c2 = fma(e[8], xi0, fma(e[9], xi1, fma(e[10], xi2, e[11] * xi3)));
+				double c3 = fma(e[12], xi0, fma(e[13], xi1, fma(e[14], xi2, e[15] * xi3)));
+				atomicAdd(&r[4 * tj], -c0);
+				atomicAdd(&r[4 * tj + 1], -c1);
+				atomicAdd(&r[4 * tj + 2], -c2);
+				atomicAdd(&r[4 * tj + 3], -c3);
+				if (want_norm) {
+					atomicAdd(&asum[4 * tj], fabs(e[0]) + fabs(e[1]) + fabs(e[2]) + fabs(e[3]));
+					atomicAdd(&asum[4 * tj + 1], fabs(e[4]) + fabs(e[5]) + fabs(e[6]) + fabs(e[7]));
+					atomicAdd(&asum[4 * tj + 2], fabs(e[8]) + fabs(e[9]) + fabs(e[10]) + fabs(e[11]));
+					atomicAdd(&asum[4 * tj + 3], fabs(e[12]) + fabs(e[13]) + fabs(e[14]) + fabs(e[15]));
+				}
+			} else {
+				// diagonal tile: the strictly-upper part is the mirror of the lower part
+				acc0 = fma(e[1], xi1, fma(e[2], xi2, fma(e[3], xi3, acc0)));
+				acc1 = fma(e[6], xi2, fma(e[7], xi3, acc1));
+				acc2 = fma(e[11], xi3, acc2);
+				if (want_norm) {
+					s0 += fabs(e[1]) + fabs(e[2]) + fabs(e[3]);
+					s1 += fabs(e[6]) + fabs(e[7]);
+					s2 += fabs(e[11]);
+				}
+			}
+		}
+#pragma unroll
+		for (int off = 16; off > 0; off >>= 1) {
+			acc0 += __shfl_down_sync(0xffffffffu, acc0, off);
+			acc1 += __shfl_down_sync(0xffffffffu, acc1, off);
+			acc2 += __shfl_down_sync(0xffffffffu, acc2, off);
+			acc3 += __shfl_down_sync(0xffffffffu, acc3, off);
+			if (want_norm) {
+				s0 += __shfl_down_sync(0xffffffffu, s0, off);
+				s1 += __shfl_down_sync(0xffffffffu, s1, off);
+				s2 += __shfl_down_sync(0xffffffffu, s2, off);
+				s3 += __shfl_down_sync(0xffffffffu, s3, off);
+			}
+		}
+		if (lane == 0) {
+			atomicAdd(&r[4 * ti], -acc0);
+			atomicAdd(&r[4 * ti + 1], -acc1);
+			atomicAdd(&r[4 * ti + 2], -acc2);
+			atomicAdd(&r[4 * ti + 3], -acc3);
+			if (want_norm) {
+				atomicAdd(&asum[4 * ti], s0);
+				atomicAdd(&asum[4 * ti + 1], s1);
+				atomicAdd(&asum[4 * ti + 2], s2);
+				atomicAdd(&asum[4 * ti + 3], s3);
+			}
+		}
+	}
+	__syncthreads();
+}
+
+template <typename T, bool MIXED>
+__global__ void __launch_bounds__(256) k_posv(int cls, int max_n, PosvWs ws, const int *__restrict__ nvec,
+                                              const DevDesc<double> *__restrict__ sA,
+                                              const DevVec<double> *__restrict__ sb,
+                                              const DevVec<double> *__restrict__ sx, int max_iter, double tol,
+                                              int *iters, double *berr, int *info) {
+	extern __shared__ __align__(16) unsigned char smem[];
+	const PosvPlan pl = posv_plan<T, MIXED>(max_n);
+	T *S = (T *)(smem + pl.S_off);
+	T *invL = (T *)(smem + pl.inv_off);
+	double *dinv = (double *)(smem + pl.dinv_off);
+	double *scratch = (double *)(smem + pl.scr_off);
+	T *w = (T *)(smem + pl.w_off);
+	double *xs = (double *)(smem + pl.x_off);
+	double *rs = (double *)(smem + pl.r_off);
+	T *ybuf = (T *)(smem + pl.ybuf_off);
+	double *misc = (double *)(smem + pl.misc_off);
+	int *s_bad = (int *)(misc + 40);
+	int *s_item = (int *)(misc + 41);
+	const int tid = threadIdx.x, nt = blockDim.x;
+	const int start = ws.start[cls], count = ws.count[cls];
+
+	for (;;) {
+		if (tid == 0) {
+			int k = atomicAdd(&ws.counter[cls], 1);
+			*s_item = (k < count) ? ws.list[start + k] : -1;
+			*s_bad = 0;
+		}
+		__syncthreads();
+		const int sys = *s_item;
+		if (sys < 0) break;
+		const int n = nvec[sys];
+		if (n <= 0 || n > max_n) {
+			if (tid == 0) {
+				if (info) info[sys] = (n <= 0) ? 0 : -2;
+				if (iters) iters[sys] = 0;
+			}
+			__syncthreads();
+			continue;
+		}
+		PMat<double> a;
+		a.p = sA[sys].pA;
+		a.d = sA[sys].dA;
+		a.cn = sA[sys].cn;
+		a.ri = 0;
+		a.cj = 0;
+		const double *bg = sb[sys].pa;
+		double *xg = sx[sys].pa;
+		const int P = (n + 3) >> 2;
+		const int nv = ((n + 15) >> 4) * 16;
+
+		// lower triangle -> lower panels (converted to T), identity padding
+		{
+			const int warp = tid >> 5, lane = tid & 31, nw = nt >> 5;
+			for (int p = warp; p < P; p += nw) {
+				T *dst = S + lp_off(p);
+				const double *src = a.p + (size_t)(4 * p) * a.cn;
+				const int cnt = 16 * (p + 1);
+				for (int e = 2 * lane; e < cnt; e += 64) {
+					double2 v = __ldg((const double2 *)(src + e));
+					int i0 = 4 * p + (e & 3), j0 = e >> 2;
+					T v0, v1;
+					// e is even: elements e, e+1 are rows i0, i0+1 of column j0
+					if (i0 < n && j0 < n) v0 = (j0 <= i0) ? (T)v.x : T(0);
+					else v0 = (i0 == j0) ? T(1) : T(0);
+					if (i0 + 1 < n && j0 < n) v1 = (j0 <= i0 + 1) ? (T)v.y : T(0);
+					else v1 = (i0 + 1 == j0) ? T(1) : T(0);
+					dst[e] = v0;
+					dst[e + 1] = v1;
+				}
+			}
+			for (int i = tid; i < nv; i += nt) w[i] = (i < n) ? (T)bg[i] : T(0);
+			if (MIXED)
+				for (int i = tid; i < nv; i += nt) xs[i] = 0.0;
+		}
+		__syncthreads();
+		chol_smem<T>(S, n, dinv, invL, MIXED ? 256 : 0, scratch, s_bad);
+
+		if (!MIXED) {
+			trsv_fwd<T>(S, n, nullptr, dinv, w, ybuf);
+			trsv_bwd<T>(S, n, nullptr, dinv, w, ybuf);
+			for (int i = tid; i < n; i += nt) xg[i] = (double)w[i];
+			if (tid == 0) {
+				if (info) info[sys] = *s_bad;
+				if (iters) iters[sys] = 0;
+			}
+			__syncthreads();
+			continue;
+		}
+
+		// mixed: refinement loop; the first pass solves with r = b
+		double anorm = 0.0, bnorm_res = 0.0;
+		int it = 0;
+		bool conv = false;
+		double scale = 1.0;
+		{
+			double m = 0.0;
+			for (int i = tid; i < n; i += nt) m = fmax(m, fabs(bg[i]));
+			m = block_max<T>(m, misc);
+			scale = (m > 0.0) ? 1.0 / m : 1.0;
+			for (int i = tid; i < nv; i += nt) w[i] = (i < n) ? (T)(bg[i] * scale) : T(0);
+			__syncthreads();
+		}
+		for (;;) {
+			trsv_fwd<T>(S, n, invL, dinv, w, ybuf);
+			trsv_bwd<T>(S, n, invL, dinv, w, ybuf);
+			for (int i = tid; i < n; i += nt) xs[i] += (double)w[i] / scale;
+			__syncthreads();
+			sym_residual(a, n, bg, xs, rs, nullptr, false);
+			// norms
+			double rm = 0.0, xm = 0.0;
+			for (int i = tid; i < n; i += nt) {
+				rm = fmax(rm, fabs(rs[i]));
+				xm = fmax(xm, fabs(xs[i]));
+			}
+			rm = block_max<T>(rm, misc);
+			xm = block_max<T>(xm, misc);
+			if (it == 0) {
+				// ||A||_inf from the lower triangle: row i sums row part + column part
+				double am = 0.0;
+				for (int i = tid; i < n; i += nt) {
+					double s = 0.0;
+					for (int j = 0; j <= i; j++) s += fabs(a.at(i, j));
+					for (int j = i + 1; j < n; j++) s += fabs(a.at(j, i));
+					am = fmax(am, s);
+				}
+				anorm = block_max<T>(am, misc);
+			}
+			it++;
+			bnorm_res = (anorm > 0.0 && xm > 0.0) ? rm / (anorm * xm) : (rm == 0.0 ? 0.0 : INFINITY);
+			if (bnorm_res <= tol) {
+				conv = true;
+				break;
+			}
+			if (it > max_iter) break;
+			scale = (rm > 0.0) ? 1.0 / rm : 1.0;
+			for (int i = tid; i < nv; i += nt) w[i] = (i < n) ? (T)(rs[i] * scale) : T(0);
+			__syncthreads();
+		}
+		for (int i = tid; i < n; i += nt) xg[i] = xs[i];
+		if (tid == 0) {
+			if (iters) iters[sys] = it - 1;
+			if (berr) berr[sys] = bnorm_res;
+			if (info) info[sys] = *s_bad ? *s_bad : (conv ? 0 : -1);
+		}
+		__syncthreads();
+	}
+}
+
+// Global-memory path for systems whose FP64 lower panels exceed shared memory:
+// factor in a per-CTA workspace slot (unblocked right-looking), then one-warp
+// substitutions.
+__global__ void __launch_bounds__(256) k_posv_global(int cls, int max_n, PosvWs ws, const int *__restrict__ nvec,
+                                                     const DevDesc<double> *__restrict__ sA,
+                                                     const DevVec<double> *__restrict__ sb,
+                                                     const DevVec<double> *__restrict__ sx, double *slots,
+                                                     int *info) {
+	__shared__ int s_item, s_bad;
+	__shared__ double s_inv;
+	const int tid = threadIdx.x, nt = blockDim.x;
+	const int start = ws.start[cls], count = ws.count[cls];
+	const size_t slot_elems = (size_t)max_n * max_n + 2 * (size_t)max_n;
+	double *L = slots + slot_elems * blockIdx.x;  // column-major n x n
+	double *dv = L + (size_t)max_n * max_n;
+	double *wv = dv + max_n;
+	for (;;) {
+		if (tid == 0) {
+			int k = atomicAdd(&ws.counter[cls], 1);
+			s_item = (k < count) ? ws.list[start + k] : -1;
+			s_bad = 0;
+		}
+		__syncthreads();
+		const int sys = s_item;
+		if (sys < 0) break;
+		const int n = nvec[sys];
+		if (n <= 0 || n > max_n) {
+			if (tid == 0 && info) info[sys] = (n <= 0) ? 0 : -2;
+			__syncthreads();
+			continue;
+		}
+		PMat<double> a;
+		a.p = sA[sys].pA;
+		a.cn = sA[sys].cn;
+		a.ri = a.cj = 0;
+		for (long long e = tid; e < (long long)n * n; e += nt) {
+			int i = (int)(e % n), j = (int)(e / n);
+			if (j <= i) L[e] = a.at(i, j);
+		}
+		__syncthreads();
+		for (int j = 0; j < n; j++) {
+			if (tid == 0) {
+				double d, inv;
+				double c = L[(size_t)j * n + j];
+				chol_pivot(c, d, inv);
+				if (!(c > 0.0) && s_bad == 0) s_bad = j + 1;
+				L[(size_t)j * n + j] = d;
+				dv[j] = inv;
+				s_inv = inv;
+			}
+			__syncthreads();
+			for (int i = j + 1 + tid; i < n; i += nt) L[(size_t)j * n + i] *= s_inv;
+			__syncthreads();
+			const int r = n - j - 1;
+			for (long long e = tid; e < (long long)r * r; e += nt) {
+				int i = j + 1 + (int)(e % r), l = j + 1 + (int)(e / r);
+				if (l <= i) L[(size_t)l * n + i] = fma(-L[(size_t)j * n + i], L[(size_t)j * n + l], L[(size_t)l * n + i]);
+			}
+			__syncthreads();
+		}
+		// solves by warp 0
+		if (tid < 32) {
+			const double *bg = sb[sys].pa;
+			for (int i = tid; i < n; i += 32) wv[i] = bg[i];
+			__syncwarp();
+			for (int j = 0; j < n; j++) {
+				double zj = wv[j] * dv[j];
+				__syncwarp();
+				for (int i = j + 1 + tid; i < n; i += 32) wv[i] = fma(-L[(size_t)j * n + i], zj, wv[i]);
+				if (tid == 0) wv[j] = zj;
+				__syncwarp();
+			}
+			for (int j = n - 1; j >= 0; j--) {
+				double zj = wv[j] * dv[j];
+				__syncwarp();
+				for (int i = tid; i < j; i += 32) wv[i] = fma(-L[(size_t)i * n + j], zj, wv[i]);
+				if (tid == 0) wv[j] = zj;
+				__syncwarp();
+			}
+			double *xg = sx[sys].pa;
+			for (int i = tid; i < n; i += 32) xg[i] = wv[i];
+			if (tid == 0 && info) info[sys] = s_bad;
+		}
+		__syncthreads();
+	}
+}
+
+struct PosvClassCfg {
+	int upper;
+	int threads;
+};
+
+template <typename T, bool MIXED>
+int posv_run(int batch, const int *n, int max_n, const void *sA, const void *sb, const void *sx, int max_iter,
+             double tol, int *iters, double *berr, int *info, void *work, size_t work_bytes, cudaStream_t s) {
+	if (batch < 0 || !n || !sA || !sb || !sx || max_n < 0) return BLASFEO_B200_EINVAL;
+	if (batch == 0 || max_n == 0) return BLASFEO_B200_OK;
+	// size classes: shared memory and CTA size follow the largest member
+	const size_t smem_cap = bf::max_smem_optin();
+	ClassTable ct;
+	PosvClassCfg cfg[POSV_MAX_CLASSES];
+	const int uppers[] = {16, 32, 64, 96, 128, 160, 192, 256};
+	int nc = 0;
+	int smem_limit_n = 0;  // largest n the shared-memory kernel takes
+	for (int v = 4; v <= 4096; v += 4)
+		if (posv_plan<T, MIXED>(v).total <= smem_cap) smem_limit_n = v;
+	for (int u : uppers) {
+		if (nc >= POSV_MAX_CLASSES - 1) break;
+		int uu = u < smem_limit_n ? u : smem_limit_n;
+		if (nc > 0 && uu <= cfg[nc - 1].upper) continue;
+		cfg[nc].upper = uu;
+		cfg[nc].threads = uu <= 32 ? 64 : (uu <= 96 ? 128 : 256);
+		nc++;
+		if (uu >= max_n) break;
+	}
+	bool need_global = max_n > cfg[nc - 1].upper;
+	if (need_global) {
+		cfg[nc].upper = max_n;
+		cfg[nc].threads = 256;
+		nc++;
+	}
+	ct.nclass = nc;
+	for (int c = 0; c < nc; c++) ct.upper[c] = cfg[c].upper;
+
+	// workspace
+	const int gslots = need_global ? 2 * bf::num_sms() : 0;
+	size_t need = a16((size_t)batch * sizeof(int)) + 4 * a16(POSV_MAX_CLASSES * sizeof(int));
+	size_t slot_bytes = ((size_t)max_n * max_n + 2 * (size_t)max_n) * sizeof(double);
+	size_t slots_off = need;
+	need += (size_t)gslots * slot_bytes;
+	char *wsp = (char *)work;
+	if (!wsp) {
+		wsp = (char *)bf::workspace(need, s);
+		if (!wsp) return BLASFEO_B200_ENOMEM;
+	} else if (work_bytes < need) {
+		return BLASFEO_B200_ENOMEM;
+	}
+	PosvWs ws;
+	ws.list = (int *)wsp;
+	char *q = wsp + a16((size_t)batch * sizeof(int));
+	ws.start = (int *)q;
+	q += a16(POSV_MAX_CLASSES * sizeof(int));
+	ws.count = (int *)q;
+	q += a16(POSV_MAX_CLASSES * sizeof(int));
+	ws.counter = (int *)q;
+	q += a16(POSV_MAX_CLASSES * sizeof(int));
+	ws.hist = (int *)q;
+	k_posv_classify<<<1, 1024, 2 * (max_n + 2) * sizeof(int), s>>>(batch, n, max_n, ct, ws);
+	if (bf::check_launch()) return BLASFEO_B200_ECUDA;
+	const int sms = bf::num_sms();
+	for (int c = 0; c < nc; c++) {
+		const bool glob = need_global && c == nc - 1;
+		if (glob) {
+			k_posv_global<<<gslots, 256, 0, s>>>(c, max_n, ws, n, (const DevDesc<double> *)sA,
+			                                     (const DevVec<double> *)sb, (const DevVec<double> *)sx,
+			                                     (double *)(wsp + slots_off), info);
+		} else {
+			PosvPlan pl = posv_plan<T, MIXED>(cfg[c].upper);
+			if (pl.total > 48 * 1024)
+				cudaFuncSetAttribute(k_posv<T, MIXED>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pl.total);
+			int per_sm = 0;
+			cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_posv<T, MIXED>, cfg[c].threads, pl.total);
+			if (per_sm < 1) per_sm = 1;
+			int grid = sms * per_sm;
+			if (grid > batch) grid = batch;
+			k_posv<T, MIXED><<<grid, cfg[c].threads, pl.total, s>>>(c, cfg[c].upper, ws, n, (const DevDesc<double> *)sA,
+			                                                        (const DevVec<double> *)sb,
+			                                                        (const DevVec<double> *)sx, max_iter, tol, iters,
+			                                                        berr, info);
+		}
+		if (bf::check_launch()) return BLASFEO_B200_ECUDA;
+	}
+	return BLASFEO_B200_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+size_t blasfeo_dposv_worksize(int batch) {
+	// list + class tables; the global-memory slots of very large systems are
+	// sized separately by the library workspace when work == NULL
+	return a16((size_t)(batch > 0 ? batch : 0) * sizeof(int)) + 4 * a16(POSV_MAX_CLASSES * sizeof(int));
+}
+
+int blasfeo_dposv_l_vbatch(int batch, const int *n, int max_n, const struct blasfeo_dmat *sA,
+                           const struct blasfeo_dvec *sb, const struct blasfeo_dvec *sx, int *info, void *work,
+                           size_t work_bytes, void *stream) {
+	return posv_run<double, false>(batch, n, max_n, sA, sb, sx, 0, 0.0, nullptr, nullptr, info, work, work_bytes,
+	                               (cudaStream_t)stream);
+}
+
+int blasfeo_dsposv_l_vbatch(int batch, const int *n, int max_n, const struct blasfeo_dmat *sA,
+                            const struct blasfeo_dvec *sb, const struct blasfeo_dvec *sx, int max_iter, double tol,
+                            int *iters, double *berr, int *info, void *work, size_t work_bytes, void *stream) {
+	return posv_run<float, true>(batch, n, max_n, sA, sb, sx, max_iter, tol, iters, berr, info, work, work_bytes,
+	                             (cudaStream_t)stream);
+}
+
+}  // extern "C"

@@ -1,0 +1,127 @@
+// Library state: error recording, the stream of the single-instance entry
+// points, the synchronous/asynchronous switch, and the library-owned device
+// workspace used when a caller passes no workspace.
+#include <mutex>
+#include <vector>
+
+#include "common.cuh"
+
+namespace bf {
+
+static thread_local int g_last_error = BLASFEO_B200_OK;
+static thread_local cudaStream_t g_stream = nullptr;
+static thread_local int g_sync = 1;
+
+void set_error(int status) {
+	if (status != BLASFEO_B200_OK) g_last_error = status;
+}
+
+int check_launch() {
+	cudaError_t e = cudaGetLastError();
+	if (e != cudaSuccess) {
+		set_error(BLASFEO_B200_ECUDA);
+		return BLASFEO_B200_ECUDA;
+	}
+	return BLASFEO_B200_OK;
+}
+
+cudaStream_t cur_stream() { return g_stream; }
+bool sync_mode() { return g_sync != 0; }
+
+int finish_single() {
+	int st = check_launch();
+	if (st == BLASFEO_B200_OK && g_sync) {
+		if (cudaStreamSynchronize(g_stream) != cudaSuccess) {
+			set_error(BLASFEO_B200_ECUDA);
+			st = BLASFEO_B200_ECUDA;
+		}
+	}
+	return st;
+}
+
+struct Workspace {
+	void *ptr = nullptr;
+	size_t bytes = 0;
+};
+static std::mutex g_ws_mutex;
+static std::vector<Workspace> g_ws;
+
+void *workspace(size_t bytes, cudaStream_t s) {
+	int dev = 0;
+	if (cudaGetDevice(&dev) != cudaSuccess) return nullptr;
+	std::lock_guard<std::mutex> lock(g_ws_mutex);
+	if ((int)g_ws.size() <= dev) g_ws.resize(dev + 1);
+	Workspace &w = g_ws[dev];
+	if (w.bytes >= bytes && w.ptr) return w.ptr;
+	// growing: wait for work that may still use the old buffer
+	if (w.ptr) {
+		cudaStreamSynchronize(s);
+		cudaDeviceSynchronize();
+		cudaFree(w.ptr);
+		w.ptr = nullptr;
+		w.bytes = 0;
+	}
+	size_t want = bytes < (size_t(1) << 20) ? (size_t(1) << 20) : bytes;
+	want = (want + 4095) / 4096 * 4096;
+	if (cudaMalloc(&w.ptr, want) != cudaSuccess) {
+		cudaGetLastError();
+		w.ptr = nullptr;
+		return nullptr;
+	}
+	w.bytes = want;
+	return w.ptr;
+}
+
+int num_sms() {
+	static int sms[64] = {0};
+	int dev = 0;
+	cudaGetDevice(&dev);
+	if (dev < 0 || dev >= 64) return 148;
+	if (!sms[dev]) {
+		int v = 0;
+		cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev);
+		sms[dev] = v > 0 ? v : 148;
+	}
+	return sms[dev];
+}
+
+size_t max_smem_optin() {
+	static int v[64] = {0};
+	int dev = 0;
+	cudaGetDevice(&dev);
+	if (dev < 0 || dev >= 64) return 227 * 1024;
+	if (!v[dev]) {
+		int x = 0;
+		cudaDeviceGetAttribute(&x, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+		v[dev] = x > 0 ? x : 227 * 1024;
+	}
+	return (size_t)v[dev];
+}
+
+}  // namespace bf
+
+extern "C" {
+
+int blasfeo_b200_last_error(void) {
+	int e = bf::g_last_error;
+	bf::g_last_error = BLASFEO_B200_OK;
+	return e;
+}
+
+const char *blasfeo_b200_error_string(int status) {
+	switch (status) {
+	case BLASFEO_B200_OK: return "ok";
+	case BLASFEO_B200_EINVAL: return "invalid argument";
+	case BLASFEO_B200_ECUDA: return "CUDA error";
+	case BLASFEO_B200_ENOMEM: return "workspace too small or allocation failed";
+	case BLASFEO_B200_ENOTSUP: return "size not supported by this kernel";
+	default: return "unknown status";
+	}
+}
+
+void blasfeo_b200_set_stream(void *stream) { bf::g_stream = (cudaStream_t)stream; }
+void *blasfeo_b200_get_stream(void) { return (void *)bf::g_stream; }
+void blasfeo_b200_set_sync(int sync) { bf::g_sync = sync; }
+int blasfeo_b200_version(void) { return 100; }
+
+}  // extern "C"

@@ -1,0 +1,260 @@
+/*
+ * blasfeo_b200 -- BLASFEO's level-3 / LAPACK hot path for NVIDIA B200 (sm_100a).
+ *
+ * C ABI of libblasfeo_b200.so.  Plain C types only: pointers, sizes, and the
+ * BLASFEO descriptor structs.  CUDA streams are passed as `void *` (a
+ * cudaStream_t; NULL = the legacy default stream).
+ *
+ * Drop-in part: the functions named blasfeo_d* / blasfeo_s* below keep the
+ * names, argument lists and argument meanings of BLASFEO 0.1.4.2's BLASFEO API
+ * (panel-major, LA=HIGH_PERFORMANCE), with one difference: the memory handed
+ * to blasfeo_create_dmat / blasfeo_create_dvec is DEVICE memory (cudaMalloc),
+ * so pA / dA / pa point into HBM.  The descriptor structs live in host memory
+ * and have the reference's exact field layout.  Citations name the reference
+ * prototype each entry point replaces (paths relative to the BLASFEO tree).
+ *
+ * Semantics kept from the reference:
+ *   - panel-major storage with panel size 4 for both precisions: element (i,j)
+ *     at pA[(i - i%4)*cn + 4*j + i%4]  (include/blasfeo_common.h:112);
+ *   - pA followed by dA in the buffer, 64-byte rounded memsize;
+ *   - dA holds the inverse diagonal after potrf/getrf (use_dA set), the cached
+ *     inverse diagonal that trsm_rltn reuses, and tau after geqrf;
+ *   - non-positive Cholesky pivot -> L_jj = 0, inverse 0, no error;
+ *     zero LU pivot -> inverse 0; pivot = first row of the largest |a|;
+ *     ipiv 0-based absolute row indices.
+ * Differences: no exit(1) on unsupported offsets -- every offset is supported;
+ * the single-instance calls synchronise their stream before returning unless
+ * blasfeo_b200_set_sync(0) is in effect; errors are recorded and readable with
+ * blasfeo_b200_last_error().
+ *
+ * Batched part (no reference counterpart; the reference is single-instance):
+ *   *_batch   uniform batch, all instances the same size, stored as a strided
+ *             slab (struct blasfeo_dmat_batch); asynchronous on `stream`.
+ *   *_vbatch  variable-size batch: device arrays of per-instance sizes and of
+ *             per-instance descriptors (struct blasfeo_dmat in device memory,
+ *             pA/dA pointing to device memory); asynchronous on `stream`.
+ * Batched calls return a status code (0 = launched) and, where given, write a
+ * per-instance info[] (device memory): 0 = ok, j+1 = first bad pivot at j.
+ */
+#ifndef BLASFEO_B200_H_
+#define BLASFEO_B200_H_
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define BLASFEO_B200_PS 4
+
+/* ---- descriptors: include/blasfeo_common.h:67-110 (identical layout) ---- */
+struct blasfeo_dmat {
+	double *mem;  /* device memory passed to create */
+	double *pA;   /* device: pm*cn panel-major doubles */
+	double *dA;   /* device: inverse diagonal / tau, min(m,n) rounded to 16 */
+	int m, n, pm, cn;
+	int use_dA;   /* host-side flag: dA holds a valid inverse diagonal for use_dA columns */
+	int memsize;
+};
+struct blasfeo_smat {
+	float *mem; float *pA; float *dA;
+	int m, n, pm, cn;
+	int use_dA;
+	int memsize;
+};
+struct blasfeo_dvec { double *mem; double *pa; int m, pm, memsize; };
+struct blasfeo_svec { float *mem; float *pa; int m, pm, memsize; };
+
+/* uniform batch: `batch` consecutive instances, instance b's storage starts at
+ * mem + b*stride elements and is laid out exactly as blasfeo_create_dmat lays
+ * out one matrix (pA, then dA). */
+struct blasfeo_dmat_batch {
+	double *mem; double *pA; double *dA;
+	int m, n, pm, cn;
+	int use_dA;
+	int batch;
+	long long stride;   /* elements between instances */
+	size_t memsize;     /* bytes of the whole slab */
+};
+struct blasfeo_smat_batch {
+	float *mem; float *pA; float *dA;
+	int m, n, pm, cn;
+	int use_dA;
+	int batch;
+	long long stride;
+	size_t memsize;
+};
+
+/* status codes */
+#define BLASFEO_B200_OK 0
+#define BLASFEO_B200_EINVAL 1      /* bad argument (size, NULL pointer, out of range) */
+#define BLASFEO_B200_ECUDA 2       /* a CUDA call failed */
+#define BLASFEO_B200_ENOMEM 3      /* workspace too small / allocation failed */
+#define BLASFEO_B200_ENOTSUP 4     /* size beyond what the kernel supports */
+
+/* ---- library state ---- */
+int blasfeo_b200_last_error(void);                  /* last status of a void entry point, then cleared */
+const char *blasfeo_b200_error_string(int status);
+void blasfeo_b200_set_stream(void *stream);         /* stream of the single-instance entry points (per host thread) */
+void *blasfeo_b200_get_stream(void);
+void blasfeo_b200_set_sync(int sync);               /* 1 (default): single-instance calls synchronise before return */
+int blasfeo_b200_version(void);
+
+/* ---- storage: auxiliary/d_aux_lib4.c:1519,1548,1575,1588 / include/blasfeo_d_aux.h ---- */
+size_t blasfeo_memsize_dmat(int m, int n);
+size_t blasfeo_memsize_diag_dmat(int m, int n);
+void blasfeo_create_dmat(int m, int n, struct blasfeo_dmat *sA, void *memory);
+size_t blasfeo_memsize_dvec(int m);
+void blasfeo_create_dvec(int m, struct blasfeo_dvec *sa, void *memory);
+size_t blasfeo_memsize_smat(int m, int n);
+size_t blasfeo_memsize_diag_smat(int m, int n);
+void blasfeo_create_smat(int m, int n, struct blasfeo_smat *sA, void *memory);
+size_t blasfeo_memsize_svec(int m);
+void blasfeo_create_svec(int m, struct blasfeo_svec *sa, void *memory);
+
+/* host column-major A (lda) <-> device panel-major sA: auxiliary/d_aux_lib4.c:1607 (pack), :2238 (unpack) */
+void blasfeo_pack_dmat(int m, int n, double *A, int lda, struct blasfeo_dmat *sA, int ai, int aj);
+void blasfeo_unpack_dmat(int m, int n, struct blasfeo_dmat *sA, int ai, int aj, double *A, int lda);
+void blasfeo_pack_dvec(int m, double *x, int xi, struct blasfeo_dvec *sa, int ai);
+void blasfeo_unpack_dvec(int m, struct blasfeo_dvec *sa, int ai, double *x, int xi);
+void blasfeo_pack_smat(int m, int n, float *A, int lda, struct blasfeo_smat *sA, int ai, int aj);
+void blasfeo_unpack_smat(int m, int n, struct blasfeo_smat *sA, int ai, int aj, float *A, int lda);
+void blasfeo_pack_svec(int m, float *x, int xi, struct blasfeo_svec *sa, int ai);
+void blasfeo_unpack_svec(int m, struct blasfeo_svec *sa, int ai, float *x, int xi);
+/* include/blasfeo_d_aux.h:115 dgecp, :141 ddiare, :162 drowsw */
+void blasfeo_dgecp(int m, int n, struct blasfeo_dmat *sA, int ai, int aj, struct blasfeo_dmat *sB, int bi, int bj);
+void blasfeo_ddiare(int kmax, double alpha, struct blasfeo_dmat *sA, int ai, int aj);
+void blasfeo_drowsw(int kmax, struct blasfeo_dmat *sA, int ai, int aj, struct blasfeo_dmat *sC, int ci, int cj);
+void blasfeo_sgecp(int m, int n, struct blasfeo_smat *sA, int ai, int aj, struct blasfeo_smat *sB, int bi, int bj);
+void blasfeo_sdiare(int kmax, float alpha, struct blasfeo_smat *sA, int ai, int aj);
+void blasfeo_srowsw(int kmax, struct blasfeo_smat *sA, int ai, int aj, struct blasfeo_smat *sC, int ci, int cj);
+
+/* ---- level 3: include/blasfeo_d_blasfeo_api.h:143 (gemm_nt), :149 (syrk_ln), :222 (trsm_rltn), :186 (trmm_rlnn) ---- */
+void blasfeo_dgemm_nt(int m, int n, int k, double alpha, struct blasfeo_dmat *sA, int ai, int aj,
+	struct blasfeo_dmat *sB, int bi, int bj, double beta, struct blasfeo_dmat *sC, int ci, int cj,
+	struct blasfeo_dmat *sD, int di, int dj);
+void blasfeo_dsyrk_ln(int m, int k, double alpha, struct blasfeo_dmat *sA, int ai, int aj,
+	struct blasfeo_dmat *sB, int bi, int bj, double beta, struct blasfeo_dmat *sC, int ci, int cj,
+	struct blasfeo_dmat *sD, int di, int dj);
+void blasfeo_dtrsm_rltn(int m, int n, double alpha, struct blasfeo_dmat *sA, int ai, int aj,
+	struct blasfeo_dmat *sB, int bi, int bj, struct blasfeo_dmat *sD, int di, int dj);
+void blasfeo_dtrmm_rlnn(int m, int n, double alpha, struct blasfeo_dmat *sA, int ai, int aj,
+	struct blasfeo_dmat *sB, int bi, int bj, struct blasfeo_dmat *sD, int di, int dj);
+/* include/blasfeo_s_blasfeo_api.h (same lines, single precision) */
+void blasfeo_sgemm_nt(int m, int n, int k, float alpha, struct blasfeo_smat *sA, int ai, int aj,
+	struct blasfeo_smat *sB, int bi, int bj, float beta, struct blasfeo_smat *sC, int ci, int cj,
+	struct blasfeo_smat *sD, int di, int dj);
+void blasfeo_ssyrk_ln(int m, int k, float alpha, struct blasfeo_smat *sA, int ai, int aj,
+	struct blasfeo_smat *sB, int bi, int bj, float beta, struct blasfeo_smat *sC, int ci, int cj,
+	struct blasfeo_smat *sD, int di, int dj);
+void blasfeo_strsm_rltn(int m, int n, float alpha, struct blasfeo_smat *sA, int ai, int aj,
+	struct blasfeo_smat *sB, int bi, int bj, struct blasfeo_smat *sD, int di, int dj);
+void blasfeo_strmm_rlnn(int m, int n, float alpha, struct blasfeo_smat *sA, int ai, int aj,
+	struct blasfeo_smat *sB, int bi, int bj, struct blasfeo_smat *sD, int di, int dj);
+
+/* ---- LAPACK: include/blasfeo_d_blasfeo_api.h:280 (potrf_l), :286 (syrk_dpotrf_ln), :291 (getrf_rp), :293-294 (geqrf) ---- */
+void blasfeo_dpotrf_l(int m, struct blasfeo_dmat *sC, int ci, int cj, struct blasfeo_dmat *sD, int di, int dj);
+void blasfeo_dsyrk_dpotrf_ln(int m, int k, struct blasfeo_dmat *sA, int ai, int aj, struct blasfeo_dmat *sB, int bi, int bj,
+	struct blasfeo_dmat *sC, int ci, int cj, struct blasfeo_dmat *sD, int di, int dj);
+/* ipiv: HOST array of min(m,n) ints, as in the reference */
+void blasfeo_dgetrf_rp(int m, int n, struct blasfeo_dmat *sC, int ci, int cj, struct blasfeo_dmat *sD, int di, int dj, int *ipiv);
+int blasfeo_dgeqrf_worksize(int m, int n);
+/* work: unused by the device kernels (may be NULL); kept for the signature */
+void blasfeo_dgeqrf(int m, int n, struct blasfeo_dmat *sC, int ci, int cj, struct blasfeo_dmat *sD, int di, int dj, void *work);
+void blasfeo_spotrf_l(int m, struct blasfeo_smat *sC, int ci, int cj, struct blasfeo_smat *sD, int di, int dj);
+void blasfeo_ssyrk_spotrf_ln(int m, int k, struct blasfeo_smat *sA, int ai, int aj, struct blasfeo_smat *sB, int bi, int bj,
+	struct blasfeo_smat *sC, int ci, int cj, struct blasfeo_smat *sD, int di, int dj);
+void blasfeo_sgetrf_rp(int m, int n, struct blasfeo_smat *sC, int ci, int cj, struct blasfeo_smat *sD, int di, int dj, int *ipiv);
+int blasfeo_sgeqrf_worksize(int m, int n);
+void blasfeo_sgeqrf(int m, int n, struct blasfeo_smat *sC, int ci, int cj, struct blasfeo_smat *sD, int di, int dj, void *work);
+
+/* ---- level 2 used by the solve chains: include/blasfeo_d_blasfeo_api.h:85 (gemv_n), :93 (trsv_lnn), :97 (trsv_ltn) ---- */
+void blasfeo_dgemv_n(int m, int n, double alpha, struct blasfeo_dmat *sA, int ai, int aj, struct blasfeo_dvec *sx, int xi,
+	double beta, struct blasfeo_dvec *sy, int yi, struct blasfeo_dvec *sz, int zi);
+void blasfeo_dtrsv_lnn(int m, struct blasfeo_dmat *sA, int ai, int aj, struct blasfeo_dvec *sx, int xi, struct blasfeo_dvec *sz, int zi);
+void blasfeo_dtrsv_ltn(int m, struct blasfeo_dmat *sA, int ai, int aj, struct blasfeo_dvec *sx, int xi, struct blasfeo_dvec *sz, int zi);
+
+/* ---- uniform batches (no reference counterpart) ---- */
+size_t blasfeo_memsize_dmat_batch(int m, int n, int batch);
+void blasfeo_create_dmat_batch(int m, int n, int batch, struct blasfeo_dmat_batch *sA, void *memory);
+void blasfeo_dmat_batch_instance(struct blasfeo_dmat_batch *sA, int b, struct blasfeo_dmat *out);
+size_t blasfeo_memsize_smat_batch(int m, int n, int batch);
+void blasfeo_create_smat_batch(int m, int n, int batch, struct blasfeo_smat_batch *sA, void *memory);
+void blasfeo_smat_batch_instance(struct blasfeo_smat_batch *sA, int b, struct blasfeo_smat *out);
+
+int blasfeo_dgemm_nt_batch(int batch, int m, int n, int k, double alpha, struct blasfeo_dmat_batch *sA, int ai, int aj,
+	struct blasfeo_dmat_batch *sB, int bi, int bj, double beta, struct blasfeo_dmat_batch *sC, int ci, int cj,
+	struct blasfeo_dmat_batch *sD, int di, int dj, void *stream);
+int blasfeo_dsyrk_ln_batch(int batch, int m, int k, double alpha, struct blasfeo_dmat_batch *sA, int ai, int aj,
+	struct blasfeo_dmat_batch *sB, int bi, int bj, double beta, struct blasfeo_dmat_batch *sC, int ci, int cj,
+	struct blasfeo_dmat_batch *sD, int di, int dj, void *stream);
+int blasfeo_dtrsm_rltn_batch(int batch, int m, int n, double alpha, struct blasfeo_dmat_batch *sA, int ai, int aj,
+	struct blasfeo_dmat_batch *sB, int bi, int bj, struct blasfeo_dmat_batch *sD, int di, int dj, void *stream);
+int blasfeo_dpotrf_l_batch(int batch, int m, struct blasfeo_dmat_batch *sC, int ci, int cj,
+	struct blasfeo_dmat_batch *sD, int di, int dj, int *info, void *stream);
+int blasfeo_dsyrk_dpotrf_ln_batch(int batch, int m, int k, struct blasfeo_dmat_batch *sA, int ai, int aj,
+	struct blasfeo_dmat_batch *sB, int bi, int bj, struct blasfeo_dmat_batch *sC, int ci, int cj,
+	struct blasfeo_dmat_batch *sD, int di, int dj, int *info, void *stream);
+/* ipiv: device array, batch * min(m,n) ints */
+int blasfeo_dgetrf_rp_batch(int batch, int m, int n, struct blasfeo_dmat_batch *sC, int ci, int cj,
+	struct blasfeo_dmat_batch *sD, int di, int dj, int *ipiv, int *info, void *stream);
+int blasfeo_dgeqrf_batch(int batch, int m, int n, struct blasfeo_dmat_batch *sC, int ci, int cj,
+	struct blasfeo_dmat_batch *sD, int di, int dj, void *stream);
+
+int blasfeo_sgemm_nt_batch(int batch, int m, int n, int k, float alpha, struct blasfeo_smat_batch *sA, int ai, int aj,
+	struct blasfeo_smat_batch *sB, int bi, int bj, float beta, struct blasfeo_smat_batch *sC, int ci, int cj,
+	struct blasfeo_smat_batch *sD, int di, int dj, void *stream);
+int blasfeo_ssyrk_ln_batch(int batch, int m, int k, float alpha, struct blasfeo_smat_batch *sA, int ai, int aj,
+	struct blasfeo_smat_batch *sB, int bi, int bj, float beta, struct blasfeo_smat_batch *sC, int ci, int cj,
+	struct blasfeo_smat_batch *sD, int di, int dj, void *stream);
+int blasfeo_strsm_rltn_batch(int batch, int m, int n, float alpha, struct blasfeo_smat_batch *sA, int ai, int aj,
+	struct blasfeo_smat_batch *sB, int bi, int bj, struct blasfeo_smat_batch *sD, int di, int dj, void *stream);
+int blasfeo_spotrf_l_batch(int batch, int m, struct blasfeo_smat_batch *sC, int ci, int cj,
+	struct blasfeo_smat_batch *sD, int di, int dj, int *info, void *stream);
+int blasfeo_ssyrk_spotrf_ln_batch(int batch, int m, int k, struct blasfeo_smat_batch *sA, int ai, int aj,
+	struct blasfeo_smat_batch *sB, int bi, int bj, struct blasfeo_smat_batch *sC, int ci, int cj,
+	struct blasfeo_smat_batch *sD, int di, int dj, int *info, void *stream);
+int blasfeo_sgetrf_rp_batch(int batch, int m, int n, struct blasfeo_smat_batch *sC, int ci, int cj,
+	struct blasfeo_smat_batch *sD, int di, int dj, int *ipiv, int *info, void *stream);
+int blasfeo_sgeqrf_batch(int batch, int m, int n, struct blasfeo_smat_batch *sC, int ci, int cj,
+	struct blasfeo_smat_batch *sD, int di, int dj, void *stream);
+
+/* ---- variable-size batches (no reference counterpart) ----
+ * Size arrays (m, n, k) and descriptor arrays (sA, ...) are DEVICE arrays of
+ * `batch` entries; max_* are upper bounds of the sizes (used for grid and
+ * shared-memory sizing).  All offsets are zero. */
+int blasfeo_dgemm_nt_vbatch(int batch, const int *m, const int *n, const int *k, int max_m, int max_n, int max_k,
+	double alpha, const struct blasfeo_dmat *sA, const struct blasfeo_dmat *sB, double beta,
+	const struct blasfeo_dmat *sC, const struct blasfeo_dmat *sD, void *stream);
+int blasfeo_dpotrf_l_vbatch(int batch, const int *m, int max_m, const struct blasfeo_dmat *sC,
+	const struct blasfeo_dmat *sD, int *info, void *stream);
+/* ipiv: device array, instance b uses ipiv[b*ipiv_stride ...] */
+int blasfeo_dgetrf_rp_vbatch(int batch, const int *m, const int *n, int max_m, int max_n,
+	const struct blasfeo_dmat *sC, const struct blasfeo_dmat *sD, int *ipiv, int ipiv_stride, int *info, void *stream);
+int blasfeo_dgeqrf_vbatch(int batch, const int *m, const int *n, int max_m, int max_n,
+	const struct blasfeo_dmat *sC, const struct blasfeo_dmat *sD, void *stream);
+
+/* ---- fused solvers (no reference counterpart; built from dpotrf_l + dtrsv_lnn + dtrsv_ltn) ----
+ * Solve A x = b for a variable-size batch of SPD systems; A is read from the
+ * lower triangle of each descriptor (full storage, upper part ignored).
+ *   dposv:  plain FP64 factor and solve (x written to sx).
+ *   dsposv: FP32 factor (FP64 diagonal blocks, FP64 pivots), FP64 residual and
+ *           iterative refinement until ||b-Ax||_inf <= tol*||A||_inf*||x||_inf
+ *           or max_iter refinement steps; iters[b] / berr[b] (device, may be NULL)
+ *           receive the step count and final backward error; info[b] = -1 when
+ *           refinement did not reach tol.
+ * work/work_bytes: device workspace (size from blasfeo_dposv_worksize); NULL
+ * uses a library-owned workspace. */
+size_t blasfeo_dposv_worksize(int batch);
+int blasfeo_dposv_l_vbatch(int batch, const int *n, int max_n, const struct blasfeo_dmat *sA,
+	const struct blasfeo_dvec *sb, const struct blasfeo_dvec *sx, int *info,
+	void *work, size_t work_bytes, void *stream);
+int blasfeo_dsposv_l_vbatch(int batch, const int *n, int max_n, const struct blasfeo_dmat *sA,
+	const struct blasfeo_dvec *sb, const struct blasfeo_dvec *sx, int max_iter, double tol,
+	int *iters, double *berr, int *info, void *work, size_t work_bytes, void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* BLASFEO_B200_H_ */
