@@ -1,0 +1,422 @@
+#!/usr/bin/env python
+"""Benchmark: solved instances/s at FP64-level residual, mixed vs plain FP64.
+
+Workload (one "step"): 20,000 independent SPD systems A x = b, n drawn
+uniformly from 4..256 (seeded), A = Q diag(lambda) Q^T with Q from the QR of an
+N(0,1) matrix and log10(lambda) ~ U[0,6], b ~ N(0,1); every system solved to
+||b - A x||_inf <= 1e-12 ||A||_inf ||x||_inf.
+
+  value : mixed-precision path (blasfeo_dsposv_l_vbatch: FP32 factor with FP64
+          diagonal blocks + FP64 iterative refinement), inputs resident in HBM
+  plain : plain FP64 path (blasfeo_dposv_l_vbatch), same inputs
+  e2e   : the mixed path through blasfeo_dsposv_l_vbatch_mapped with every input
+          in pinned host memory (matrices, right-hand sides, sizes,
+          descriptors): the kernels read the lower triangles over the host link
+          and write x back to host memory inside the timed region
+  cpu_baseline / --impl reference : the reference's own CPU path
+          (blasfeo_dpotrf_l + blasfeo_dtrsv_lnn + blasfeo_dtrsv_ltn, BLASFEO
+          compiled from source) on the host cores, threads over instances.
+
+Usage: python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+For N > 1 launch one process per GPU with torch.distributed.run; every rank
+solves its own batch (weak scaling, no data-path collective).
+"""
+import argparse
+import ctypes as C
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "solved instances/s at FP64-level residual, mixed vs plain FP64, same B200"
+UNIT = "systems/s"
+NUM = 20000
+TOL = 1e-12
+MAX_ITER = 30
+WORKLOAD = ("uneven SPD batch: 20,000 systems, n~U{4..256}, A=Q diag(lambda) Q^T, log10(lambda)~U[0,6], "
+            "b~N(0,1), refine to ||r||/(||A|| ||x||) <= 1e-12")
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--num", type=int, default=NUM)
+    ap.add_argument("--cpu-sample", type=int, default=4000)
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    return ap.parse_args()
+
+
+# ---------------------------------------------------------------------------
+# CPU side: the reference (or the oracle port) on the host cores
+# ---------------------------------------------------------------------------
+def _cpu_flags():
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("flags"):
+                    return set(line.split(":", 1)[1].split())
+    except OSError:
+        pass
+    return set()
+
+
+def cpu_library():
+    """(ctypes lib, prefix, kind, name): compiled reference if present, else the oracle port."""
+    from oracle import pyoracle
+    flags = _cpu_flags()
+    for target in (["haswell"] if {"avx2", "fma"} <= flags else []) + ["generic"]:
+        if pyoracle.ref_available(target):
+            return pyoracle.ref_lib(target), "blasfeo_d", "reference", "BLASFEO 0.1.4.2 HP " + target
+    from tests.helpers import ensure_oracle
+    ensure_oracle()
+    return pyoracle.oracle_lib(), "oracle_d_", "port", "oracle restatement (C, scalar loops)"
+
+
+def cpu_sample_systems(num, seed=1):
+    rng = np.random.default_rng(seed)
+    ns = rng.integers(4, 257, size=num)
+    mats, rhs = [], []
+    for n in ns:
+        q, _ = np.linalg.qr(rng.standard_normal((n, n)))
+        lam = 10.0 ** rng.uniform(0, 6, n)
+        a = (q * lam) @ q.T
+        mats.append(0.5 * (a + a.T))
+        rhs.append(rng.standard_normal(n))
+    return ns, mats, rhs
+
+
+class CpuRun:
+    def __init__(self, num, threads=None):
+        from oracle.pyoracle import HostMat, HostVec
+        self.lib, self.prefix, self.kind, self.name = cpu_library()
+        d = os.path.join(ROOT, "oracle")
+        so = os.path.join(d, "libcpu_bench.so")
+        if not os.path.exists(so):
+            subprocess.run(["make", "-s", "-C", d, "cpubench"], check=True)
+        self.drv = C.CDLL(so)
+        self.drv.cpu_posv_batch.restype = C.c_double
+        self.threads = threads or len(os.sched_getaffinity(0))
+        self.ns, mats, self.rhs = cpu_sample_systems(num)
+        self.mats = mats
+        self.hA = [HostMat(int(n), int(n)).set(a) for n, a in zip(self.ns, mats)]
+        self.hb = [HostVec(int(n)).set(b) for n, b in zip(self.ns, self.rhs)]
+        self.hx = [HostVec(int(n)) for n in self.ns]
+        from oracle.pyoracle import DMat, DVec
+        self.A = (DMat * num)(*[h.desc for h in self.hA])
+        self.b = (DVec * num)(*[h.desc for h in self.hb])
+        self.x = (DVec * num)(*[h.desc for h in self.hx])
+        self.n = (C.c_int * num)(*[int(v) for v in self.ns])
+        f = lambda s: C.cast(getattr(self.lib, self.prefix + s), C.c_void_p)
+        self.fp = (f("potrf_l"), f("trsv_lnn"), f("trsv_ltn"))
+        self.num = num
+
+    def run(self):
+        return self.drv.cpu_posv_batch(self.threads, self.num, int(self.ns.max()), self.n, self.A, self.b, self.x,
+                                       *self.fp)
+
+    def check(self, k=8):
+        worst = 0.0
+        for i in range(0, self.num, max(1, self.num // k)):
+            x = self.hx[i].get()
+            a, b = self.mats[i], self.rhs[i]
+            worst = max(worst, np.abs(b - a @ x).max() / (np.abs(a).sum(1).max() * np.abs(x).max()))
+        return worst
+
+
+def cpu_baseline(sample, budget_s=10.0):
+    cr = CpuRun(sample)
+    t = cr.run()
+    reps = max(1, min(20, int(budget_s / max(t, 1e-3))))
+    ts = [cr.run() for _ in range(reps)]
+    t = float(np.median(ts))
+    return {"value": sample / t, "unit": UNIT, "cores": cr.threads, "kind": cr.kind,
+            "sample": "%d systems of the same distribution (seeded), %s, dpotrf_l+dtrsv_lnn+dtrsv_ltn per system, "
+                      "median of %d passes, worst sampled residual %.1e" % (sample, cr.name, reps, cr.check())}
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    cr = CpuRun(args.cpu_sample)
+    for _ in range(args.warmup):
+        cr.run()
+    ts = [cr.run() for _ in range(args.steps)]
+    total = float(np.sum(ts))
+    val = args.cpu_sample * args.steps / total
+    line = {"metric": METRIC, "value": val, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1e3 * total / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic", "impl": "reference",
+            "config": {"workload": WORKLOAD, "sample_systems": args.cpu_sample, "library": cr.name},
+            "cpu_baseline": {"value": val, "unit": UNIT, "cores": cr.threads, "kind": cr.kind,
+                             "sample": "%d systems per step, %s" % (args.cpu_sample, cr.name)},
+            "e2e": {"value": val, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# ---------------------------------------------------------------------------
+# GPU side
+# ---------------------------------------------------------------------------
+class Clocks:
+    """nvidia-smi sampler over the timed region."""
+
+    def __init__(self, index):
+        self.index = index
+        self.samples = []
+        self.proc = None
+
+    def start(self):
+        q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+             "clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), "--query-gpu=" + q,
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.samples.append([x.strip() for x in line.split(",")])
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        mhz = [float(s[0]) for s in self.samples if len(s) >= 7 and s[0].replace(".", "").isdigit()]
+        mx = [float(s[1]) for s in self.samples if len(s) >= 7 and s[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for s in self.samples if len(s) >= 7 for k in range(4) if s[3 + k] == "Active"})
+        return {"sm_mhz": float(np.median(mhz)) if mhz else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.samples)}
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return run_reference(args)
+    import torch
+    import torch.distributed as dist
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300), device_id=torch.device("cuda", local))
+    import blasfeo_b200 as bf
+    from blasfeo_b200.workloads import spd_config3
+    lib = bf.lib
+    P = lambda t: C.c_void_p(t.data_ptr())
+    dev = torch.device("cuda", local)
+    W = spd_config3(args.num, seed=1000 + rank, device=dev)
+    info = torch.zeros(args.num, dtype=torch.int32, device=dev)
+    iters = torch.zeros(args.num, dtype=torch.int32, device=dev)
+    berr = torch.zeros(args.num, dtype=torch.float64, device=dev)
+    stream = torch.cuda.current_stream(dev)
+    sh = C.c_void_p(stream.cuda_stream)
+
+    def mixed():
+        return lib.blasfeo_dsposv_l_vbatch(args.num, P(W.nvec), W.max_n, P(W.desc), P(W.bdesc), P(W.xdesc), MAX_ITER,
+                                           TOL, P(iters), P(berr), P(info), None, 0, sh)
+
+    def plain():
+        return lib.blasfeo_dposv_l_vbatch(args.num, P(W.nvec), W.max_n, P(W.desc), P(W.bdesc), P(W.xdesc), P(info),
+                                          None, 0, sh)
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    def timed(fn, steps, warmup):
+        for _ in range(warmup):
+            bf.check(fn())
+        torch.cuda.synchronize()
+        barrier()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(steps):
+            fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        barrier()
+        ms = e0.elapsed_time(e1) / steps
+        if world > 1:
+            t = torch.tensor([ms], dtype=torch.float64, device=dev)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ms = float(t.item())
+        return ms
+
+    # ---- correctness gate (not timed): every system at FP64-level residual ----
+    bf.check(mixed())
+    torch.cuda.synchronize()
+    inf_ = info.cpu().numpy()
+    be = berr.cpu().numpy()
+    it = iters.cpu().numpy()
+    ok_mixed = bool((inf_ == 0).all() and (be <= TOL).all())
+    rng = np.random.default_rng(rank)
+    worst = 0.0
+    for i in rng.choice(args.num, size=min(16, args.num), replace=False):
+        a, b, x = W.matrix(i), W.rhs[i], W.solution(i)
+        worst = max(worst, np.abs(b - a @ x).max() / (np.abs(a).sum(1).max() * np.abs(x).max()))
+    bf.check(plain())
+    torch.cuda.synchronize()
+    ok_plain = bool((info.cpu().numpy() == 0).all())
+    worst_plain = 0.0
+    for i in rng.choice(args.num, size=min(16, args.num), replace=False):
+        a, b, x = W.matrix(i), W.rhs[i], W.solution(i)
+        worst_plain = max(worst_plain, np.abs(b - a @ x).max() / (np.abs(a).sum(1).max() * np.abs(x).max()))
+    if not ok_mixed or worst > TOL or worst_plain > TOL:
+        print("residual gate failed: mixed ok=%s (max berr %.2e, sampled %.2e), plain ok=%s (sampled %.2e)"
+              % (ok_mixed, be.max(), worst, ok_plain, worst_plain), file=sys.stderr)
+        return 2
+
+    # ---- timed: mixed (headline value) and plain FP64 ----
+    clk = Clocks(local)
+    clk.start()
+    time.sleep(0.3)
+    ms_mixed = timed(mixed, args.steps, args.warmup)
+    ms_plain = timed(plain, args.steps, args.warmup)
+    clocks = clk.stop()
+    nclass = 9  # classify + size classes (upper bound of launches per call)
+    value = world * args.num / (ms_mixed * 1e-3)
+    plain_value = world * args.num / (ms_plain * 1e-3)
+
+    # ---- e2e: everything in pinned host memory, kernels read it over the host link ----
+    e2e = None
+    try:
+        e2e = run_e2e(args, W, lib, torch, dev, stream, barrier, world)
+    except Exception as ex:  # reported, never silently replaced
+        e2e = {"value": None, "unit": UNIT, "error": repr(ex)}
+
+    peak_bw = None
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            peak_bw = float(json.load(f)["hbm_gbs"])
+        peak_src = "measured (MEASURED_PEAKS.json hbm_gbs)"
+    except Exception:
+        peak_bw = 6650.0
+        peak_src = "fallback 6.65 TB/s"
+    fp32_peak = lib.blasfeo_b200_measure_fma_peak(b"s"[0], 4096)
+    fp64_peak = lib.blasfeo_b200_measure_fma_peak(b"d"[0], 2048)
+    bytes_pass = W.lower_bytes()
+    flops = W.chol_flops()
+    achieved = bytes_pass / (ms_mixed * 1e-3) / 1e9
+    roofline = {"bound": "hbm", "achieved": achieved, "peak": peak_bw, "unit": "GB/s", "frac": achieved / peak_bw,
+                "traffic": None, "peak_source": peak_src,
+                "kernel": "k_posv<float,true> (all size classes of one blasfeo_dsposv_l_vbatch call)",
+                "algorithmic_bytes_per_launch": bytes_pass,
+                "fp32_simt": {"achieved_gflops": flops / (ms_mixed * 1e-3) / 1e9, "peak_gflops": fp32_peak,
+                              "frac": flops / (ms_mixed * 1e-3) / 1e9 / fp32_peak if fp32_peak > 0 else None}}
+    plain_roof = {"achieved_gflops": flops / (ms_plain * 1e-3) / 1e9, "fp64_peak_gflops": fp64_peak,
+                  "frac": flops / (ms_plain * 1e-3) / 1e9 / fp64_peak if fp64_peak > 0 else None,
+                  "hbm_frac": bytes_pass / (ms_plain * 1e-3) / 1e9 / peak_bw}
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        try:
+            cpu = cpu_baseline(args.cpu_sample)
+        except Exception as ex:
+            cpu = {"value": None, "error": repr(ex)}
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_mixed, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32 factor + f64 refinement", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "systems_per_gpu": args.num, "max_iter": MAX_ITER, "tol": TOL,
+                       "l2": "inputs larger than L2 (%.2f GB FP64 matrices per GPU vs 126 MB L2)" % (W.total_bytes / 1e9),
+                       "parallelism": "replicas" if world > 1 else "single GPU"},
+            "plain_fp64": {"value": plain_value, "unit": UNIT, "ms_per_step": ms_plain, "roofline": plain_roof},
+            "mixed_vs_plain": value / plain_value,
+            "refinement": {"mean_steps": float(it.mean()), "max_steps": int(it.max()), "max_berr": float(be.max()),
+                           "sampled_host_residual": worst, "sampled_host_residual_plain": worst_plain},
+            "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "clocks": clocks,
+            "gpu_launches": (args.steps * nclass) * 2}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.destroy_process_group()
+    return 0
+
+
+def run_e2e(args, W, lib, torch, dev, stream, barrier, world):
+    """Mixed path with all inputs in pinned host memory (mapped into the GPU's
+    address space): blasfeo_dsposv_l_vbatch_mapped reads the lower triangles
+    over the host link and writes x to host memory."""
+    from blasfeo_b200.workloads import DESC_DTYPE, VDESC_DTYPE
+    P = lambda t: C.c_void_p(t.data_ptr())
+    hslab = torch.empty(W.slab.numel(), dtype=torch.float64, pin_memory=True)
+    hslab.copy_(W.slab)
+    hb = torch.empty(W.b.numel(), dtype=torch.float64, pin_memory=True)
+    hb.copy_(W.b)
+    hx = torch.zeros_like(hb).pin_memory()
+    hn = torch.from_numpy(W.ns.copy()).pin_memory()
+    d = W.desc.cpu().numpy().view(DESC_DTYPE).copy()
+    shift = hslab.data_ptr() - W.slab.data_ptr()
+    for f in ("mem", "pA", "dA"):
+        d[f] = d[f] + np.uint64(shift) if shift >= 0 else d[f] - np.uint64(-shift)
+    hdesc = torch.from_numpy(d.view(np.uint8).copy()).pin_memory()
+
+    def vd(t):
+        v = np.zeros(len(W.ns), dtype=VDESC_DTYPE)
+        v["mem"] = t.data_ptr() + W.voff * 8
+        v["pa"] = t.data_ptr() + W.voff * 8
+        v["m"] = W.ns
+        v["pm"] = W.vlen
+        v["memsize"] = W.vlen * 8
+        return torch.from_numpy(v.view(np.uint8).copy()).pin_memory()
+    hbd, hxd = vd(hb), vd(hx)
+    hinfo = torch.zeros(args.num, dtype=torch.int32).pin_memory()
+    sh = C.c_void_p(stream.cuda_stream)
+
+    def call():
+        return lib.blasfeo_dsposv_l_vbatch_mapped(args.num, P(hn), W.max_n, P(hdesc), P(hbd), P(hxd), MAX_ITER, TOL,
+                                                  None, None, P(hinfo), None, 0, sh)
+    for _ in range(args.warmup):
+        call()
+    torch.cuda.synchronize()
+    if not (hinfo.numpy() == 0).all():
+        raise RuntimeError("mapped solve: %d systems not converged" % int((hinfo.numpy() != 0).sum()))
+    xs = hx.numpy()
+    i = 0
+    a, b = W.matrix(i), W.rhs[i]
+    x = xs[W.voff[i]:W.voff[i] + len(b)]
+    res = np.abs(b - a @ x).max() / (np.abs(a).sum(1).max() * np.abs(x).max())
+    barrier()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    t0 = time.perf_counter()
+    e0.record(stream)
+    for _ in range(args.steps):
+        call()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    wall = (time.perf_counter() - t0) / args.steps
+    ms = e0.elapsed_time(e1) / args.steps
+    barrier()
+    n = W.ns.astype(np.int64)
+    h2d = int((n * (n + 1) // 2 * 8).sum() + W.b.numel() * 8 + hn.numel() * 4 + hdesc.numel() + hbd.numel() * 2)
+    d2h = int(n.sum() * 8)
+    return {"value": world * args.num / (ms * 1e-3), "unit": UNIT, "h2d_bytes_per_step": h2d,
+            "d2h_bytes_per_step": d2h, "ms_per_step": ms, "host_wall_ms_per_step": wall * 1e3,
+            "path": "blasfeo_dsposv_l_vbatch_mapped, all inputs in pinned host memory",
+            "host_link_gbs": (h2d + d2h) / (ms * 1e-3) / 1e9, "residual_system0": float(res)}
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -25,7 +25,7 @@ class BlasfeoError(RuntimeError):
 
 def _load():
     if not os.path.exists(LIB_PATH):
-        raise BlasfeoError("libblasfeo_b200.so not built: run `python -m blasfeo_b200.build` (%s)" % LIB_PATH)
+        raise BlasfeoError("libblasfeo_b200.so not built: run `python blasfeo_b200/build.py` (%s)" % LIB_PATH)
     return C.CDLL(LIB_PATH)
 
 
@@ -95,6 +95,7 @@ _sig("blasfeo_b200_set_stream", None, _vp)
 _sig("blasfeo_b200_get_stream", _vp)
 _sig("blasfeo_b200_set_sync", None, _i)
 _sig("blasfeo_b200_version", _i)
+_sig("blasfeo_b200_measure_fma_peak", _d, C.c_char, _i)
 for p, M, V, R in (("d", _DM, _DV, _d), ("s", _SM, _SV, _f)):
     _sig("blasfeo_memsize_%smat" % p, _sz, _i, _i)
     _sig("blasfeo_memsize_diag_%smat" % p, _sz, _i, _i)
@@ -139,6 +140,7 @@ _sig("blasfeo_dgeqrf_vbatch", _i, _i, _vp, _vp, _i, _i, _vp, _vp, _vp)
 _sig("blasfeo_dposv_worksize", _sz, _i)
 _sig("blasfeo_dposv_l_vbatch", _i, _i, _vp, _i, _vp, _vp, _vp, _vp, _vp, _sz, _vp)
 _sig("blasfeo_dsposv_l_vbatch", _i, _i, _vp, _i, _vp, _vp, _vp, _i, _d, _vp, _vp, _vp, _vp, _sz, _vp)
+_sig("blasfeo_dsposv_l_vbatch_mapped", _i, _i, _vp, _i, _vp, _vp, _vp, _i, _d, _vp, _vp, _vp, _vp, _sz, _vp)
 
 
 def check(status=None):

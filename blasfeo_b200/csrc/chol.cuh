@@ -2,23 +2,30 @@
 // the fused factor+solve kernels.
 //
 // Shared-memory layout ("lower panels"): the lower triangle of an n x n matrix
-// as P = ceil(n/4) row panels; panel p (rows 4p..4p+3) keeps columns
-// 0..4p+3, column-major inside the panel (4 consecutive elements per column),
-// i.e. the BLASFEO panel layout with everything right of the diagonal tile
-// dropped.  Panel p starts at element 8p(p+1); a 4x4 tile and a 4-row column
-// slice are contiguous.  Padding rows/columns (n..4P-1) hold the identity so
-// they factor to the identity and never touch real entries.
+// as P = ceil(n/4) row panels; panel p (rows 4p..4p+3) keeps the 4x4 tiles
+// 0..p, i.e. the BLASFEO panel layout with everything right of the diagonal
+// tile dropped.  Panel p starts at element 8p(p+1); tile (p,q) is 16
+// contiguous elements, column-major inside the tile.  Inside a tile the
+// 16-byte chunks are XOR-swizzled with (p+q): threads that read different
+// tiles of one tile row or one tile column then hit different banks (every
+// tile starts on a 128-byte (FP64) / 64-byte (FP32) boundary, so without the
+// swizzle all of them would collide on the same banks).
+// Padding rows/columns (n..4P-1) hold the identity so they factor to the
+// identity and never touch real entries.
 //
-// Algorithm: right-looking, 16 columns (4 panels) per block step.
-//   1. one warp factors the 16x16 diagonal block in FP64 registers (pivot rule
-//      of kernel/generic/kernel_dgemm_4x4_lib4.c:5700-5710: c>0 -> sqrt(c) and
-//      its reciprocal, else 0 and 0) and forms the explicit inverse of that
-//      block, also in FP64;
-//   2. the panel below is solved as a product with that inverse
-//      (L_IK = A_IK * inv(L_KK)^T), one thread per row;
-//   3. the trailing lower triangle gets the rank-16 update, one 4x4 tile per
-//      thread (loads are 16-byte vectors from the contiguous tiles).
-// Three __syncthreads per 16 columns.
+// Algorithm: right-looking, 16 columns (4 panels) per block step, with
+// look-ahead:
+//   1. panel solve of block column K by substitution, one thread per row,
+//      with the FP64 diagonal block and its reciprocal pivots;
+//   2. rank-16 update of block column K+1 (all threads);
+//   3. warp 0 factors diagonal block K+1 in FP64 (pivot rule of
+//      kernel/generic/kernel_dgemm_4x4_lib4.c:5700-5710: c>0 -> sqrt(c) and its
+//      reciprocal, else 0 and 0) while the other warps apply the rank-16
+//      update to the rest of the trailing matrix (one 4x4 tile per thread).
+// Three __syncthreads per 16 columns; the serial diagonal factorization is
+// hidden behind the trailing update.  Explicit inverses of the diagonal blocks
+// (used by the refinement solves) are formed after the factorization, all
+// blocks in parallel.
 #pragma once
 #include "common.cuh"
 
@@ -29,38 +36,64 @@ __host__ __device__ __forceinline__ int lp_size(int n) {
 	int P = (n + 3) / 4;
 	return 8 * P * (P + 1);
 }
+
+// physical index of element (i,j) (j <= 4*(i/4)+3) in the swizzled lower panels
+template <typename T>
+__device__ __forceinline__ int lp_idx(int i, int j);
+template <>
+__device__ __forceinline__ int lp_idx<double>(int i, int j) {
+	const int p = i >> 2, q = j >> 2;
+	const int e = ((j & 3) << 2) | (i & 3);
+	return lp_off(p) + 16 * q + ((((e >> 1) ^ ((p + q) & 7)) << 1) | (e & 1));
+}
+template <>
+__device__ __forceinline__ int lp_idx<float>(int i, int j) {
+	const int p = i >> 2, q = j >> 2;
+	return lp_off(p) + 16 * q + ((((j & 3) ^ ((p + q) & 3)) << 2) | (i & 3));
+}
 template <typename T>
 __device__ __forceinline__ T &lp_at(T *S, int i, int j) {
-	return S[lp_off(i >> 2) + 4 * j + (i & 3)];
-}
-
-// 4-element vector type per precision
-template <typename T> struct V4;
-template <> struct V4<float> { typedef float4 type; };
-template <> struct V4<double> { typedef double4 type; };
-
-template <typename T>
-__device__ __forceinline__ void ld4(const T *p, T &a, T &b, T &c, T &d);
-template <>
-__device__ __forceinline__ void ld4<float>(const float *p, float &a, float &b, float &c, float &d) {
-	float4 v = *(const float4 *)p;
-	a = v.x; b = v.y; c = v.z; d = v.w;
-}
-template <>
-__device__ __forceinline__ void ld4<double>(const double *p, double &a, double &b, double &c, double &d) {
-	double2 v0 = *(const double2 *)p, v1 = *(const double2 *)(p + 2);
-	a = v0.x; b = v0.y; c = v1.x; d = v1.y;
+	return S[lp_idx<T>(i, j)];
 }
 template <typename T>
-__device__ __forceinline__ void st4(T *p, T a, T b, T c, T d);
+__device__ __forceinline__ const T &lp_at(const T *S, int i, int j) {
+	return S[lp_idx<T>(i, j)];
+}
+
+// column c (0..3) of tile (p,q): the 4 rows as a, b, c, d
+template <typename T>
+__device__ __forceinline__ void tile_col_ld(const T *S, int p, int q, int c, T &a0, T &a1, T &a2, T &a3);
 template <>
-__device__ __forceinline__ void st4<float>(float *p, float a, float b, float c, float d) {
-	*(float4 *)p = make_float4(a, b, c, d);
+__device__ __forceinline__ void tile_col_ld<double>(const double *S, int p, int q, int c, double &a0, double &a1,
+                                                    double &a2, double &a3) {
+	const double *t = S + lp_off(p) + 16 * q;
+	const int s = (p + q) & 7;
+	double2 v0 = *(const double2 *)(t + (((2 * c) ^ s) << 1));
+	double2 v1 = *(const double2 *)(t + (((2 * c + 1) ^ s) << 1));
+	a0 = v0.x; a1 = v0.y; a2 = v1.x; a3 = v1.y;
 }
 template <>
-__device__ __forceinline__ void st4<double>(double *p, double a, double b, double c, double d) {
-	*(double2 *)p = make_double2(a, b);
-	*(double2 *)(p + 2) = make_double2(c, d);
+__device__ __forceinline__ void tile_col_ld<float>(const float *S, int p, int q, int c, float &a0, float &a1,
+                                                   float &a2, float &a3) {
+	const float *t = S + lp_off(p) + 16 * q;
+	float4 v = *(const float4 *)(t + ((c ^ ((p + q) & 3)) << 2));
+	a0 = v.x; a1 = v.y; a2 = v.z; a3 = v.w;
+}
+template <typename T>
+__device__ __forceinline__ void tile_col_st(T *S, int p, int q, int c, T a0, T a1, T a2, T a3);
+template <>
+__device__ __forceinline__ void tile_col_st<double>(double *S, int p, int q, int c, double a0, double a1, double a2,
+                                                    double a3) {
+	double *t = S + lp_off(p) + 16 * q;
+	const int s = (p + q) & 7;
+	*(double2 *)(t + (((2 * c) ^ s) << 1)) = make_double2(a0, a1);
+	*(double2 *)(t + (((2 * c + 1) ^ s) << 1)) = make_double2(a2, a3);
+}
+template <>
+__device__ __forceinline__ void tile_col_st<float>(float *S, int p, int q, int c, float a0, float a1, float a2,
+                                                   float a3) {
+	float *t = S + lp_off(p) + 16 * q;
+	*(float4 *)(t + ((c ^ ((p + q) & 3)) << 2)) = make_float4(a0, a1, a2, a3);
 }
 
 // map a linear index over the lower-triangular tile set {(ti,tj): 0<=tj<=ti<R}
@@ -72,14 +105,25 @@ __device__ __forceinline__ void tri_index(int t, int &ti, int &tj) {
 	tj = t - r * (r + 1) / 2;
 }
 
-// Factor the 16x16 diagonal block at column c0 (nbk <= 16 real columns) with
-// warp 0.  Writes L_KK back into S (type T), 1/L_jj into dinv[c0+j] (FP64 in
-// shared memory), the explicit inverse of L_KK (row-major 16x16, FP64 math,
-// stored as T) into invL, and the first bad pivot (j+1) into *bad.
+// Cholesky pivot through one reciprocal square root: inv = 1/sqrt(c),
+// d = c*inv (= sqrt(c)); non-positive c -> 0, 0.
+__device__ __forceinline__ void chol_pivot_rsqrt(double c, double &d, double &inv) {
+	if (c > 0.0) {
+		inv = rsqrt(c);
+		d = c * inv;
+	} else {
+		d = 0.0;
+		inv = 0.0;
+	}
+}
+
+// Factor the diagonal block at column c0 (nbk <= 16 real columns) with one
+// warp (lane i owns row c0+i, FP64).  Writes L_KK back into S, the FP64 block
+// into Ld (16x17 row-major), 1/L_jj into dinv[c0+j], the first bad pivot
+// (j+1) into *bad.
 template <typename T>
-__device__ void chol_diag_block(T *S, int c0, int nbk, double *dinv, T *invL, double *scratch, int *bad) {
+__device__ void chol_diag_factor(T *S, int c0, int nbk, double *dinv, double *Ld, int *bad) {
 	const int lane = threadIdx.x & 31;
-	// lane i (< 16) holds row c0+i of the block in FP64
 	double v[CHOL_NB];
 #pragma unroll
 	for (int l = 0; l < CHOL_NB; l++) {
@@ -95,117 +139,283 @@ __device__ void chol_diag_block(T *S, int c0, int nbk, double *dinv, T *invL, do
 #pragma unroll
 	for (int j = 0; j < CHOL_NB; j++) {
 		double d = 0.0, inv = 0.0;
+		const double cj = __shfl_sync(0xffffffffu, v[j], j);
+		chol_pivot_rsqrt(cj, d, inv);
 		if (lane == j) {
-			chol_pivot(v[j], d, inv);
-			if (!(v[j] > 0.0) && j < nbk && *bad == 0) *bad = c0 + j + 1;
 			v[j] = d;
+			if (!(cj > 0.0) && j < nbk && *bad == 0) *bad = c0 + j + 1;
+			if (j < nbk) dinv[c0 + j] = inv;
 		}
-		inv = __shfl_sync(0xffffffffu, inv, j);
 		if (lane > j) v[j] *= inv;
-		if (lane == j && j < nbk) dinv[c0 + j] = inv;
 #pragma unroll
 		for (int l = j + 1; l < CHOL_NB; l++) {
 			double t = __shfl_sync(0xffffffffu, v[j], l);
 			if (lane >= l) v[l] = fma(-v[j], t, v[l]);
 		}
 	}
-	// L_KK -> scratch (FP64, row-major 16x17, column 16 = inverse pivot) and back into S
 	if (lane < CHOL_NB) {
-		double dd = 0.0;
 #pragma unroll
-		for (int l = 0; l < CHOL_NB; l++)
-			if (l == lane) dd = v[l];
-		scratch[lane * 17 + 16] = (dd != 0.0) ? 1.0 / dd : 0.0;
-#pragma unroll
-		for (int l = 0; l < CHOL_NB; l++) scratch[lane * 17 + l] = (l <= lane) ? v[l] : 0.0;
+		for (int l = 0; l < CHOL_NB; l++) Ld[lane * 17 + l] = (l <= lane) ? v[l] : 0.0;
 		if (lane < nbk) {
 #pragma unroll
 			for (int l = 0; l < CHOL_NB; l++)
 				if (l <= lane && l < nbk) lp_at(S, c0 + lane, c0 + l) = (T)v[l];
 		}
 	}
-	__syncwarp();
-	// explicit inverse: lane c computes column c of inv(L_KK) by forward substitution
-	if (lane < CHOL_NB) {
-		const int c = lane;
-		double x[CHOL_NB];
+}
+
+// panel solve of block column c0: rows r in [c0+16, rend):
+// L[r][c0+c] = (A[r][c0+c] - sum_{l<c} L[r][c0+l] L_KK[c][l]) * inv_c
+template <typename T>
+__device__ __forceinline__ void chol_panel_rows(T *S, int c0, int rbeg, int rend, int tid0, int nthr,
+                                                const double *Ld, const double *dinv) {
+	const int kb = c0 >> 2;
+	for (int r = rbeg + tid0; r < rend; r += nthr) {
+		const int p = r >> 2, ri = r & 3;
+		T *row = S + lp_off(p) + 16 * kb;
+		int idx[CHOL_NB];
 #pragma unroll
-		for (int i = 0; i < CHOL_NB; i++) {
-			double s = (i == c) ? 1.0 : 0.0;
+		for (int l = 0; l < CHOL_NB; l++) {
+			const int qq = l >> 2, e = ((l & 3) << 2) | ri;
+			idx[l] = 16 * qq + (sizeof(T) == 4 ? ((((l & 3) ^ ((p + kb + qq) & 3)) << 2) | ri)
+			                                   : ((((e >> 1) ^ ((p + kb + qq) & 7)) << 1) | (e & 1)));
+		}
+		T a[CHOL_NB];
 #pragma unroll
-			for (int l = 0; l < i; l++) s = fma(-scratch[i * 17 + l], x[l], s);
-			x[i] = (i < c) ? 0.0 : s * scratch[i * 17 + 16];
+		for (int l = 0; l < CHOL_NB; l++) a[l] = row[idx[l]];
+#pragma unroll
+		for (int c = 0; c < CHOL_NB; c++) {
+			T s = a[c];
+#pragma unroll
+			for (int l = 0; l < c; l++) s = fma(-a[l], (T)Ld[c * 17 + l], s);
+			a[c] = s * (T)dinv[c0 + c];
 		}
 #pragma unroll
-		for (int i = 0; i < CHOL_NB; i++) invL[i * CHOL_NB + c] = (T)x[i];
+		for (int l = 0; l < CHOL_NB; l++) row[idx[l]] = a[l];
 	}
 }
 
-// Full factorization of the n x n lower-panel matrix S by the whole CTA.
-// dinv: FP64 shared array of >= 4P entries; invL_all: per block step 256
-// entries (row-major inverse of each diagonal block; pass stride 0 to reuse
-// one 256-entry buffer); scratch: 16*17 doubles; bad: shared int (0 on entry).
+// rank-16 update of tile (ti,tj) with the panel at block column c0
 template <typename T>
-__device__ void chol_smem(T *S, int n, double *dinv, T *invL_all, int invL_stride, double *scratch, int *bad) {
+__device__ __forceinline__ void chol_tile_update(T *S, int ti, int tj, int c0) {
+	T acc[16];
+	const int kb = c0 >> 2;
+#pragma unroll
+	for (int q = 0; q < 4; q++) tile_col_ld<T>(S, ti, tj, q, acc[4 * q], acc[4 * q + 1], acc[4 * q + 2], acc[4 * q + 3]);
+	const T *pa = S + lp_off(ti) + 16 * kb;
+	const T *pb = S + lp_off(tj) + 16 * kb;
+#pragma unroll
+	for (int qq = 0; qq < 4; qq++) {
+		// tile kb+qq of row panels ti and tj; column slices with the tile swizzle
+		const T *ta = pa + 16 * qq, *tb = pb + 16 * qq;
+		const int sa = ti + kb + qq, sb = tj + kb + qq;
+#pragma unroll
+		for (int c = 0; c < 4; c++) {
+			T a0, a1, a2, a3, b0, b1, b2, b3;
+			if (sizeof(T) == 4) {
+				float4 va = *(const float4 *)(ta + ((c ^ (sa & 3)) << 2));
+				float4 vb = *(const float4 *)(tb + ((c ^ (sb & 3)) << 2));
+				a0 = (T)va.x; a1 = (T)va.y; a2 = (T)va.z; a3 = (T)va.w;
+				b0 = (T)vb.x; b1 = (T)vb.y; b2 = (T)vb.z; b3 = (T)vb.w;
+			} else {
+				double2 va0 = *(const double2 *)(ta + (((2 * c) ^ (sa & 7)) << 1));
+				double2 va1 = *(const double2 *)(ta + (((2 * c + 1) ^ (sa & 7)) << 1));
+				double2 vb0 = *(const double2 *)(tb + (((2 * c) ^ (sb & 7)) << 1));
+				double2 vb1 = *(const double2 *)(tb + (((2 * c + 1) ^ (sb & 7)) << 1));
+				a0 = (T)va0.x; a1 = (T)va0.y; a2 = (T)va1.x; a3 = (T)va1.y;
+				b0 = (T)vb0.x; b1 = (T)vb0.y; b2 = (T)vb1.x; b3 = (T)vb1.y;
+			}
+			// acc[4*q + r] is element (row r of ti, column q of tj)
+			acc[0] = fma(-a0, b0, acc[0]); acc[1] = fma(-a1, b0, acc[1]);
+			acc[2] = fma(-a2, b0, acc[2]); acc[3] = fma(-a3, b0, acc[3]);
+			acc[4] = fma(-a0, b1, acc[4]); acc[5] = fma(-a1, b1, acc[5]);
+			acc[6] = fma(-a2, b1, acc[6]); acc[7] = fma(-a3, b1, acc[7]);
+			acc[8] = fma(-a0, b2, acc[8]); acc[9] = fma(-a1, b2, acc[9]);
+			acc[10] = fma(-a2, b2, acc[10]); acc[11] = fma(-a3, b2, acc[11]);
+			acc[12] = fma(-a0, b3, acc[12]); acc[13] = fma(-a1, b3, acc[13]);
+			acc[14] = fma(-a2, b3, acc[14]); acc[15] = fma(-a3, b3, acc[15]);
+		}
+	}
+#pragma unroll
+	for (int q = 0; q < 4; q++) tile_col_st<T>(S, ti, tj, q, acc[4 * q], acc[4 * q + 1], acc[4 * q + 2], acc[4 * q + 3]);
+}
+
+// Explicit inverse of diagonal block K (row-major 16x16, stored as T) from
+// the factor in S and the FP64 reciprocal pivots; one lane per column.
+template <typename T>
+__device__ void chol_block_inverse(const T *S, int n, int K, const double *dinv, T *invL, int lane) {
+	const int c0 = 16 * K;
+	const int nbk = min(CHOL_NB, n - c0);
+	const int c = lane;
+	if (c >= CHOL_NB) return;
+	double x[CHOL_NB];
+#pragma unroll
+	for (int i = 0; i < CHOL_NB; i++) {
+		double s = (i == c) ? 1.0 : 0.0;
+#pragma unroll
+		for (int l = 0; l < i; l++) {
+			double lil = (i < nbk && l < nbk) ? (double)lp_at(S, c0 + i, c0 + l) : 0.0;
+			s = fma(-lil, x[l], s);
+		}
+		double di = (i < nbk) ? dinv[c0 + i] : 1.0;
+		x[i] = (i < c) ? 0.0 : s * di;
+	}
+#pragma unroll
+	for (int i = 0; i < CHOL_NB; i++) invL[i * CHOL_NB + c] = (T)x[i];
+}
+
+// Full factorization of the n x n lower-panel matrix S by the whole CTA
+// (blockDim.x >= 64).  dinv: FP64 shared array of >= 4P entries; Ld: 16*17
+// FP64 scratch; bad: shared int (0 on entry).  If invL_all is non-null the
+// explicit inverses of all diagonal blocks are formed at the end (256 entries
+// per block).
+template <typename T>
+__device__ void chol_smem(T *S, int n, double *dinv, double *Ld, int *bad, T *invL_all) {
 	const int P = (n + 3) >> 2;
+	const int NB = (n + 15) >> 4;
 	const int tid = threadIdx.x, nt = blockDim.x;
-	for (int k0 = 0; k0 < P; k0 += 4) {
-		const int c0 = 4 * k0;
-		const int nbk = min(CHOL_NB, n - c0);
-		T *invL = invL_all + (size_t)(k0 >> 2) * invL_stride;
-		if (tid < 32) chol_diag_block<T>(S, c0, nbk, dinv, invL, scratch, bad);
+	const int warp = tid >> 5;
+	if (warp == 0) chol_diag_factor<T>(S, 0, min(CHOL_NB, n), dinv, Ld, bad);
+	__syncthreads();
+	for (int K = 0; K < NB; K++) {
+		const int c0 = 16 * K, k0 = 4 * K;
+		// 1. panel rows below the diagonal block
+		chol_panel_rows<T>(S, c0, c0 + CHOL_NB, 4 * P, tid, nt, Ld, dinv);
 		__syncthreads();
-		// panel: rows r in [c0+16, 4P) : L[r][c0..c0+15] = A[r][c0..] * invL^T
-		const int r0 = c0 + CHOL_NB;
-		const int nrow = 4 * P - r0;
-		for (int t = tid; t < nrow; t += nt) {
-			const int r = r0 + t;
-			T a[CHOL_NB];
-#pragma unroll
-			for (int l = 0; l < CHOL_NB; l++) a[l] = lp_at(S, r, c0 + l);
-#pragma unroll
-			for (int c = 0; c < CHOL_NB; c++) {
-				T s = T(0);
-#pragma unroll
-				for (int l = 0; l <= c; l++) s = fma(a[l], invL[c * CHOL_NB + l], s);
-				lp_at(S, r, c0 + c) = s;
+		if (K + 1 >= NB) break;
+		// 2. look-ahead: tiles of block column K+1 (tj in [k0+4, k0+8), ti >= tj)
+		{
+			const int rows = P - (k0 + 4);
+			const int cols = min(4, P - (k0 + 4));
+			for (int t = tid; t < rows * cols; t += nt) {
+				const int tj = k0 + 4 + t % cols, ti = k0 + 4 + t / cols;
+				if (ti >= tj) chol_tile_update<T>(S, ti, tj, c0);
 			}
 		}
 		__syncthreads();
-		// trailing update of tiles (ti,tj), k0+4 <= tj <= ti < P
-		const int R = P - (k0 + 4);
-		if (R > 0) {
-			const int ntiles = R * (R + 1) / 2;
-			for (int t = tid; t < ntiles; t += nt) {
-				int ti, tj;
-				tri_index(t, ti, tj);
-				ti += k0 + 4;
-				tj += k0 + 4;
-				T *tile = S + lp_off(ti) + 16 * tj;
-				T acc[16];
-#pragma unroll
-				for (int q = 0; q < 4; q++) ld4<T>(tile + 4 * q, acc[4 * q], acc[4 * q + 1], acc[4 * q + 2], acc[4 * q + 3]);
-				const T *li = S + lp_off(ti) + 4 * c0;
-				const T *lj = S + lp_off(tj) + 4 * c0;
-#pragma unroll 4
-				for (int c = 0; c < CHOL_NB; c++) {
-					T a0, a1, a2, a3, b0, b1, b2, b3;
-					ld4<T>(li + 4 * c, a0, a1, a2, a3);
-					ld4<T>(lj + 4 * c, b0, b1, b2, b3);
-					// acc[4*q + r] is element (row r of ti, column q of tj)
-					acc[0] = fma(-a0, b0, acc[0]); acc[1] = fma(-a1, b0, acc[1]);
-					acc[2] = fma(-a2, b0, acc[2]); acc[3] = fma(-a3, b0, acc[3]);
-					acc[4] = fma(-a0, b1, acc[4]); acc[5] = fma(-a1, b1, acc[5]);
-					acc[6] = fma(-a2, b1, acc[6]); acc[7] = fma(-a3, b1, acc[7]);
-					acc[8] = fma(-a0, b2, acc[8]); acc[9] = fma(-a1, b2, acc[9]);
-					acc[10] = fma(-a2, b2, acc[10]); acc[11] = fma(-a3, b2, acc[11]);
-					acc[12] = fma(-a0, b3, acc[12]); acc[13] = fma(-a1, b3, acc[13]);
-					acc[14] = fma(-a2, b3, acc[14]); acc[15] = fma(-a3, b3, acc[15]);
+		// 3. warp 0: diagonal block K+1 ; other warps: remaining trailing tiles
+		if (warp == 0) {
+			chol_diag_factor<T>(S, c0 + CHOL_NB, min(CHOL_NB, n - c0 - CHOL_NB), dinv, Ld, bad);
+		} else {
+			const int R = P - (k0 + 8);
+			if (R > 0) {
+				const int ntiles = R * (R + 1) / 2;
+				for (int t = tid - 32; t < ntiles; t += nt - 32) {
+					int ti, tj;
+					tri_index(t, ti, tj);
+					chol_tile_update<T>(S, ti + k0 + 8, tj + k0 + 8, c0);
 				}
-#pragma unroll
-				for (int q = 0; q < 4; q++) st4<T>(tile + 4 * q, acc[4 * q], acc[4 * q + 1], acc[4 * q + 2], acc[4 * q + 3]);
 			}
 		}
 		__syncthreads();
+	}
+	if (invL_all) {
+		const int lane = tid & 31, nw = nt >> 5;
+		for (int K = warp; K < NB; K += nw) chol_block_inverse<T>(S, n, K, dinv, invL_all + (size_t)K * 256, lane);
+		__syncthreads();
+	}
+}
+
+// Panel index of 4-element chunk ch of the lower panels (panel p holds
+// 4(p+1) chunks; chunks before panel p: 2p(p+1)).
+__device__ __forceinline__ int lp_chunk_panel(int ch) {
+	int p = (int)((sqrtf(2.0f * (float)ch + 1.0f) - 1.0f) * 0.5f);
+	while (2 * (p + 1) * (p + 2) <= ch) p++;
+	while (2 * p * (p + 1) > ch) p--;
+	return p;
+}
+
+// Load the lower triangle of an n x n panel-major matrix (row offset a
+// multiple of 4: panel p of the lower triangle is the contiguous run
+// src[4p*cn .. 4p*cn + 16(p+1)) ) into swizzled lower panels of type TD,
+// identity in the padding.  Each thread moves 4-element column slices,
+// UNR of them in flight.  slot (optional): unswizzled FP64 copy.
+template <typename TD, typename TS, int UNR>
+__device__ void load_lp_vec(TD *S, int n, const TS *__restrict__ src, int cn, double *slot) {
+	const int P = (n + 3) >> 2;
+	const int nch = 2 * P * (P + 1);
+	const int tid = threadIdx.x, nt = blockDim.x;
+	for (int base = tid; base < nch; base += UNR * nt) {
+		TS v[UNR][4];
+		int pp[UNR], cc[UNR];
+#pragma unroll
+		for (int u = 0; u < UNR; u++) {
+			const int ch = base + u * nt;
+			pp[u] = -1;
+			if (ch < nch) {
+				const int p = lp_chunk_panel(ch);
+				const int col = ch - 2 * p * (p + 1);
+				pp[u] = p;
+				cc[u] = col;
+				const TS *g = src + (size_t)(4 * p) * cn + 4 * col;
+				if (sizeof(TS) == 8) {
+					double2 x0 = __ldg((const double2 *)g), x1 = __ldg((const double2 *)g + 1);
+					v[u][0] = (TS)x0.x; v[u][1] = (TS)x0.y; v[u][2] = (TS)x1.x; v[u][3] = (TS)x1.y;
+				} else {
+					float4 x = __ldg((const float4 *)g);
+					v[u][0] = (TS)x.x; v[u][1] = (TS)x.y; v[u][2] = (TS)x.z; v[u][3] = (TS)x.w;
+				}
+			}
+		}
+#pragma unroll
+		for (int u = 0; u < UNR; u++) {
+			const int p = pp[u];
+			if (p < 0) continue;
+			const int j = cc[u];
+			TD o[4];
+			double d[4];
+#pragma unroll
+			for (int r = 0; r < 4; r++) {
+				const int i = 4 * p + r;
+				double x;
+				if (i < n && j < n)
+					x = (j <= i) ? (double)v[u][r] : 0.0;
+				else
+					x = (i == j) ? 1.0 : 0.0;
+				d[r] = x;
+				o[r] = (TD)x;
+			}
+			tile_col_st<TD>(S, p, j >> 2, j & 3, o[0], o[1], o[2], o[3]);
+			if (slot) {
+				double *sd = slot + lp_off(p) + 4 * j;
+				*(double2 *)sd = make_double2(d[0], d[1]);
+				*(double2 *)(sd + 2) = make_double2(d[2], d[3]);
+			}
+		}
+	}
+}
+
+// Store the lower triangle (j <= i < n) of swizzled lower panels into a
+// panel-major matrix with panel-aligned row offset (see load_lp_vec).
+template <typename T, int UNR>
+__device__ void store_lp_vec(const T *S, int n, T *dst, int cn) {
+	const int P = (n + 3) >> 2;
+	const int nch = 2 * P * (P + 1);
+	const int tid = threadIdx.x, nt = blockDim.x;
+	for (int base = tid; base < nch; base += UNR * nt) {
+#pragma unroll
+		for (int u = 0; u < UNR; u++) {
+			const int ch = base + u * nt;
+			if (ch >= nch) continue;
+			const int p = lp_chunk_panel(ch);
+			const int j = ch - 2 * p * (p + 1);
+			if (j >= n) continue;
+			T o0, o1, o2, o3;
+			tile_col_ld<T>(S, p, j >> 2, j & 3, o0, o1, o2, o3);
+			T *g = dst + (size_t)(4 * p) * cn + 4 * j;
+			if (j < 4 * p && 4 * p + 3 < n) {
+				if (sizeof(T) == 8) {
+					*(double2 *)g = make_double2((double)o0, (double)o1);
+					*((double2 *)g + 1) = make_double2((double)o2, (double)o3);
+				} else {
+					*(float4 *)g = make_float4((float)o0, (float)o1, (float)o2, (float)o3);
+				}
+			} else {
+				const T o[4] = {o0, o1, o2, o3};
+#pragma unroll
+				for (int r = 0; r < 4; r++)
+					if (4 * p + r < n && j <= 4 * p + r) g[r] = o[r];
+			}
+		}
 	}
 }

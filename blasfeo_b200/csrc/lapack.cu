@@ -41,7 +41,7 @@ __host__ __device__ inline PotrfSmem potrf_smem_plan(int max_n) {
 	p.s_bytes = align16((size_t)lp_size(max_n) * sizeof(T));
 	p.dinv_off = p.s_bytes;
 	p.invl_off = p.dinv_off + align16((size_t)4 * P * sizeof(double));
-	p.scratch_off = p.invl_off + align16(256 * sizeof(T));
+	p.scratch_off = p.invl_off;
 	p.bad_off = p.scratch_off + align16(16 * 17 * sizeof(double));
 	p.total = p.bad_off + 16;
 	return p;
@@ -54,7 +54,6 @@ __device__ void load_lower_panels(T *S, int n, const PMat<T> &c) {
 	const int P = (n + 3) >> 2;
 	const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
 	for (int p = warp; p < P; p += nw) {
-		T *dst = S + lp_off(p);
 		const int cnt = 16 * (p + 1);
 		for (int e = lane; e < cnt; e += 32) {
 			int i = 4 * p + (e & 3), j = e >> 2;
@@ -63,7 +62,7 @@ __device__ void load_lower_panels(T *S, int n, const PMat<T> &c) {
 				v = (j <= i) ? c.at(i, j) : T(0);
 			else
 				v = (i == j) ? T(1) : T(0);
-			dst[e] = v;
+			S[lp_idx<T>(i, j)] = v;
 		}
 	}
 }
@@ -74,17 +73,16 @@ __device__ void store_lower_panels(const T *S, int n, const PMat<T> &d) {
 	const int P = (n + 3) >> 2;
 	const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
 	for (int p = warp; p < P; p += nw) {
-		const T *src = S + lp_off(p);
 		const int cnt = 16 * (p + 1);
 		for (int e = lane; e < cnt; e += 32) {
 			int i = 4 * p + (e & 3), j = e >> 2;
-			if (i < n && j <= i) d.at(i, j) = src[e];
+			if (i < n && j <= i) d.at(i, j) = S[lp_idx<T>(i, j)];
 		}
 	}
 }
 
-template <typename T>
-__global__ void __launch_bounds__(256) k_potrf_smem(SizeArg sz, MatArg<T> C, MatArg<T> D, int *info, int max_n) {
+template <typename T, int NT, int MINB>
+__global__ void __launch_bounds__(NT, MINB) k_potrf_smem(SizeArg sz, MatArg<T> C, MatArg<T> D, int *info, int max_n) {
 	extern __shared__ __align__(16) unsigned char smem[];
 	const int b = blockIdx.x;
 	const int n = sz.M(b);
@@ -92,15 +90,20 @@ __global__ void __launch_bounds__(256) k_potrf_smem(SizeArg sz, MatArg<T> C, Mat
 	PotrfSmem pl = potrf_smem_plan<T>(max_n);
 	T *S = (T *)smem;
 	double *dinv = (double *)(smem + pl.dinv_off);
-	T *invL = (T *)(smem + pl.invl_off);
 	double *scratch = (double *)(smem + pl.scratch_off);
 	int *bad = (int *)(smem + pl.bad_off);
 	const PMat<T> c = C.get(b), d = D.get(b);
 	if (threadIdx.x == 0) *bad = 0;
-	load_lower_panels<T>(S, n, c);
+	if ((c.ri & 3) == 0)
+		load_lp_vec<T, T, 4>(S, n, c.p + (size_t)c.ri * c.cn + 4 * c.cj, c.cn, nullptr);
+	else
+		load_lower_panels<T>(S, n, c);
 	__syncthreads();
-	chol_smem<T>(S, n, dinv, invL, 0, scratch, bad);
-	store_lower_panels<T>(S, n, d);
+	chol_smem<T>(S, n, dinv, scratch, bad, (T *)nullptr);
+	if ((d.ri & 3) == 0)
+		store_lp_vec<T, 4>(S, n, d.p + (size_t)d.ri * d.cn + 4 * d.cj, d.cn);
+	else
+		store_lower_panels<T>(S, n, d);
 	for (int j = threadIdx.x; j < n; j += blockDim.x) d.d[j] = (T)dinv[j];
 	if (info && threadIdx.x == 0) info[b] = *bad;
 }
@@ -115,10 +118,9 @@ __global__ void __launch_bounds__(256) k_potrf_global(SizeArg sz, MatArg<T> C, M
 	if (n <= 0) return;
 	const PMat<T> c = C.get(b), d = D.get(b);
 	const int tid = threadIdx.x, nt = blockDim.x;
-	for (long long e = tid; e < (long long)n * n; e += nt) {
-		int i = (int)(e % n), j = (int)(e / n);
-		if (j <= i) d.at(i, j) = c.at(i, j);
-	}
+	const int warp = tid >> 5, lane = tid & 31, nw = nt >> 5;
+	for (int j = warp; j < n; j += nw)
+		for (int i = j + lane; i < n; i += 32) d.at(i, j) = c.at(i, j);
 	if (tid == 0) s_bad = 0;
 	__syncthreads();
 	for (int j = 0; j < n; j++) {
@@ -135,10 +137,9 @@ __global__ void __launch_bounds__(256) k_potrf_global(SizeArg sz, MatArg<T> C, M
 		const T inv = (T)s_inv;
 		for (int i = j + 1 + tid; i < n; i += nt) d.at(i, j) *= inv;
 		__syncthreads();
-		const int r = n - j - 1;
-		for (long long e = tid; e < (long long)r * r; e += nt) {
-			int i = j + 1 + (int)(e % r), l = j + 1 + (int)(e / r);
-			if (l <= i) d.at(i, l) = fma(-d.at(i, j), d.at(l, j), d.at(i, l));
+		for (int l = j + 1 + warp; l < n; l += nw) {
+			const T djl = d.at(l, j);
+			for (int i = l + lane; i < n; i += 32) d.at(i, l) = fma(-d.at(i, j), djl, d.at(i, l));
 		}
 		__syncthreads();
 	}
@@ -191,10 +192,9 @@ __global__ void __launch_bounds__(256) k_getrf_global(SizeArg sz, MatArg<T> C, M
 	const PMat<T> c = C.get(b), d = D.get(b);
 	const int tid = threadIdx.x, nt = blockDim.x;
 	int *piv = ipiv + ipiv_stride * b;
-	for (long long e = tid; e < (long long)m * n; e += nt) {
-		int i = (int)(e % m), j = (int)(e / m);
-		d.at(i, j) = c.at(i, j);
-	}
+	const int warp = tid >> 5, lane = tid & 31, nw = nt >> 5;
+	for (int j = warp; j < n; j += nw)
+		for (int i = lane; i < m; i += 32) d.at(i, j) = c.at(i, j);
 	if (tid == 0) s_bad = 0;
 	__syncthreads();
 	const int mn = m < n ? m : n;
@@ -226,10 +226,9 @@ __global__ void __launch_bounds__(256) k_getrf_global(SizeArg sz, MatArg<T> C, M
 		}
 		for (int i = j + 1 + tid; i < m; i += nt) d.at(i, j) *= inv;
 		__syncthreads();
-		const int rm = m - j - 1, rn = n - j - 1;
-		for (long long e = tid; e < (long long)rm * rn; e += nt) {
-			int i = j + 1 + (int)(e % rm), l = j + 1 + (int)(e / rm);
-			d.at(i, l) = fma(-d.at(i, j), d.at(j, l), d.at(i, l));
+		for (int l = j + 1 + warp; l < n; l += nw) {
+			const T ujl = d.at(j, l);
+			for (int i = j + 1 + lane; i < m; i += 32) d.at(i, l) = fma(-d.at(i, j), ujl, d.at(i, l));
 		}
 		__syncthreads();
 	}
@@ -264,9 +263,10 @@ __global__ void __launch_bounds__(256) k_geqrf_global(SizeArg sz, MatArg<T> C, M
 	const PMat<T> c = C.get(b), d = D.get(b);
 	T *tau = d.d + d.ri;
 	const int tid = threadIdx.x, nt = blockDim.x;
-	for (long long e = tid; e < (long long)m * n; e += nt) {
-		int i = (int)(e % m), j = (int)(e / m);
-		d.at(i, j) = c.at(i, j);
+	{
+		const int warp = tid >> 5, lane = tid & 31, nw = nt >> 5;
+		for (int j = warp; j < n; j += nw)
+			for (int i = lane; i < m; i += 32) d.at(i, j) = c.at(i, j);
 	}
 	__syncthreads();
 	const int kmax = m < n ? m : n;
@@ -312,6 +312,16 @@ __global__ void __launch_bounds__(256) k_geqrf_global(SizeArg sz, MatArg<T> C, M
 
 }  // namespace
 
+namespace {
+template <typename T, int NT, int MINB>
+void launch_potrf_smem(int batch, SizeArg sz, int max_m, size_t smem, MatArg<T> C, MatArg<T> D, int *info,
+                       cudaStream_t s) {
+	auto kern = k_potrf_smem<T, NT, MINB>;
+	if (smem > 48 * 1024) cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+	kern<<<batch, NT, smem, s>>>(sz, C, D, info, max_m);
+}
+}  // namespace
+
 namespace bf {
 
 template <typename T>
@@ -319,10 +329,12 @@ int potrf_launch(int batch, SizeArg sz, int max_m, MatArg<T> C, MatArg<T> D, int
 	if (batch <= 0 || max_m <= 0) return BLASFEO_B200_OK;
 	PotrfSmem pl = potrf_smem_plan<T>(max_m);
 	if (pl.total <= max_smem_optin()) {
-		if (pl.total > 48 * 1024)
-			cudaFuncSetAttribute(k_potrf_smem<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pl.total);
-		int threads = max_m <= 32 ? 64 : (max_m <= 96 ? 128 : 256);
-		k_potrf_smem<T><<<batch, threads, pl.total, s>>>(sz, C, D, info, max_m);
+		if (max_m <= 64)
+			launch_potrf_smem<T, 64, 8>(batch, sz, max_m, pl.total, C, D, info, s);
+		else if (max_m <= 128)
+			launch_potrf_smem<T, 128, 4>(batch, sz, max_m, pl.total, C, D, info, s);
+		else
+			launch_potrf_smem<T, 512, 1>(batch, sz, max_m, pl.total, C, D, info, s);
 	} else {
 		k_potrf_global<T><<<batch, 256, 0, s>>>(sz, C, D, info);
 	}

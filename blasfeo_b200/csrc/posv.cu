@@ -25,7 +25,7 @@
 
 namespace {
 
-constexpr int POSV_MAX_CLASSES = 8;
+constexpr int POSV_MAX_CLASSES = 10;
 
 struct ClassTable {
 	int nclass;
@@ -92,7 +92,7 @@ __global__ void k_posv_classify(int batch, const int *__restrict__ nvec, int max
 
 // shared-memory plan of the posv kernel
 struct PosvPlan {
-	size_t S_off, inv_off, dinv_off, scr_off, w_off, x_off, r_off, ybuf_off, misc_off, total;
+	size_t S_off, inv_off, dinv_off, scr_off, w_off, x_off, r_off, ybuf_off, asum_off, misc_off, total;
 };
 template <typename T, bool MIXED>
 __host__ __device__ inline PosvPlan posv_plan(int max_n) {
@@ -108,7 +108,8 @@ __host__ __device__ inline PosvPlan posv_plan(int max_n) {
 	p.x_off = p.w_off + a16((size_t)nv * sizeof(T));
 	p.r_off = p.x_off + (MIXED ? a16((size_t)nv * sizeof(double)) : 0);
 	p.ybuf_off = p.r_off + (MIXED ? a16((size_t)nv * sizeof(double)) : 0);
-	p.misc_off = p.ybuf_off + a16(16 * sizeof(T));
+	p.asum_off = p.ybuf_off + a16(16 * sizeof(T));
+	p.misc_off = p.asum_off + (MIXED ? a16((size_t)nv * sizeof(double)) : 0);
 	p.total = p.misc_off + 64 * sizeof(double);
 	return p;
 }
@@ -138,16 +139,15 @@ __device__ void trsv_fwd(const T *S, int n, const T *invL_all, const double *din
 			for (int k = 0; k < nbk; k++) {
 				T yk = __shfl_sync(0xffffffffu, v, k) * (T)dinv[c0 + k];
 				if (lane == k) v = yk;
-				if (lane > k && lane < nbk) v = fma(-S[lp_off((c0 + lane) >> 2) + 4 * (c0 + k) + ((c0 + lane) & 3)], yk, v);
+				if (lane > k && lane < nbk) v = fma(-lp_at(S, c0 + lane, c0 + k), yk, v);
 			}
 			if (lane < 16) ybuf[lane] = (lane < nbk) ? v : T(0);
 		}
 		__syncthreads();
 		for (int r = c0 + 16 + tid; r < n; r += nt) {
-			const T *row = S + lp_off(r >> 2) + 4 * c0 + (r & 3);
 			T s = w[r];
 #pragma unroll
-			for (int l = 0; l < 16; l++) s = fma(-row[4 * l], ybuf[l], s);
+			for (int l = 0; l < 16; l++) s = fma(-lp_at(S, r, c0 + l), ybuf[l], s);
 			w[r] = s;
 		}
 		if (tid < nbk) w[c0 + tid] = ybuf[tid];
@@ -178,7 +178,7 @@ __device__ void trsv_bwd(const T *S, int n, const T *invL_all, const double *din
 			for (int k = nbk - 1; k >= 0; k--) {
 				T xk = __shfl_sync(0xffffffffu, v, k) * (T)dinv[c0 + k];
 				if (lane == k) v = xk;
-				if (lane < k) v = fma(-S[lp_off((c0 + k) >> 2) + 4 * (c0 + lane) + ((c0 + k) & 3)], xk, v);
+				if (lane < k) v = fma(-lp_at(S, c0 + k, c0 + lane), xk, v);
 			}
 			if (lane < 16) ybuf[lane] = (lane < nbk) ? v : T(0);
 		}
@@ -187,7 +187,7 @@ __device__ void trsv_bwd(const T *S, int n, const T *invL_all, const double *din
 			T s = w[j];
 			for (int k = 0; k < nbk; k++) {
 				const int r = c0 + k;
-				s = fma(-S[lp_off(r >> 2) + 4 * j + (r & 3)], ybuf[k], s);
+				s = fma(-lp_at(S, r, j), ybuf[k], s);
 			}
 			w[j] = s;
 		}
@@ -214,120 +214,112 @@ __device__ double block_max(double v, double *red) {
 	return r;
 }
 
-// r = b - A x (FP64), A symmetric given by its lower triangle in global
-// memory; one warp per 4-row tile row, lanes over 4x4 tiles (128-byte
-// contiguous loads), transposed contributions accumulated with shared
-// atomics.  Also returns the row sums of |A| in asum when want_norm.
-__device__ void sym_residual(const PMat<double> &a, int n, const double *b, const double *x, double *r,
+// r = b - A x (FP64), A symmetric given by its lower triangle.
+// LP = false: A in BLASFEO panel-major storage (tile (ti,tj) at base + 4*ti*cn + 16*tj);
+// LP = true: A in lower panels (tile at base + lp_off(ti) + 16*tj).
+// Two deterministic passes, no atomics: pass 1 gives every 4-row tile row to
+// one warp (row part A(i,j<=i) x_j, lanes over the tiles of the row, 128-byte
+// tile loads, warp reduction); pass 2 gives every tile column to one warp
+// (column part sum_{i>j} A(i,j) x_i for the rows of that column).  With
+// want_norm the row sums of |A| are accumulated the same way into asum.
+template <bool LP>
+__device__ __forceinline__ const double *res_tile(const double *base, int cn, int ti, int tj) {
+	return LP ? base + lp_off(ti) + 16 * tj : base + (size_t)(4 * ti) * cn + 16 * tj;
+}
+
+template <bool LP>
+__device__ void sym_residual(const double *base, int cn, int n, const double *b, const double *x, double *r,
                              double *asum, bool want_norm) {
 	const int tid = threadIdx.x, nt = blockDim.x;
 	const int lane = tid & 31, warp = tid >> 5, nw = nt >> 5;
 	const int P = (n + 3) >> 2;
-	for (int i = tid; i < 4 * P; i += nt) {
-		r[i] = (i < n) ? b[i] : 0.0;
-		if (want_norm) asum[i] = 0.0;
-	}
-	__syncthreads();
-	for (int ti = warp; ti < P; ti += nw) {
-		double acc0 = 0.0, acc1 = 0.0, acc2 = 0.0, acc3 = 0.0;
-		double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
-		const double xi0 = x[4 * ti], xi1 = x[4 * ti + 1], xi2 = x[4 * ti + 2], xi3 = x[4 * ti + 3];
-		const double *prow = a.p + (size_t)(4 * ti) * a.cn;
-		for (int tj = lane; tj <= ti; tj += 32) {
-			const double *t = prow + 16 * tj;
-			double e[16];
+	for (int pass = 0; pass < 2; pass++) {
+		for (int t0 = warp; t0 < P; t0 += nw) {
+			double acc[4] = {0.0, 0.0, 0.0, 0.0}, sa[4] = {0.0, 0.0, 0.0, 0.0};
+			// pass 0: tiles (t0, t1), t1 <= t0 (row part); pass 1: tiles (t1, t0), t1 > t0 (column part)
+			const int lo = pass == 0 ? 0 : t0 + 1, hi = pass == 0 ? t0 : P - 1;
+			for (int t1 = lo + lane; t1 <= hi; t1 += 32) {
+				const int ti = pass == 0 ? t0 : t1, tj = pass == 0 ? t1 : t0;
+				const double *t = res_tile<LP>(base, cn, ti, tj);
+				double e[16];
 #pragma unroll
-			for (int q = 0; q < 8; q++) {
-				double2 v = __ldg((const double2 *)(t + 2 * q));
-				e[2 * q] = v.x;
-				e[2 * q + 1] = v.y;
+				for (int q = 0; q < 8; q++) {
+					double2 v = __ldg((const double2 *)(t + 2 * q));
+					e[2 * q] = v.x;
+					e[2 * q + 1] = v.y;
+				}
+#pragma unroll
+				for (int q = 0; q < 4; q++)
+#pragma unroll
+					for (int rr = 0; rr < 4; rr++) {
+						int gi = 4 * ti + rr, gj = 4 * tj + q;
+						if (!(gi < n && gj < n && (tj < ti || gj <= gi))) e[4 * q + rr] = 0.0;
+					}
+				if (pass == 0) {
+					const double x0 = x[4 * tj], x1 = x[4 * tj + 1], x2 = x[4 * tj + 2], x3 = x[4 * tj + 3];
+#pragma unroll
+					for (int rr = 0; rr < 4; rr++) {
+						acc[rr] = fma(e[rr], x0, fma(e[4 + rr], x1, fma(e[8 + rr], x2, fma(e[12 + rr], x3, acc[rr]))));
+						if (want_norm) sa[rr] += fabs(e[rr]) + fabs(e[4 + rr]) + fabs(e[8 + rr]) + fabs(e[12 + rr]);
+					}
+					if (tj == ti) {
+						// strictly-upper part of the diagonal tile mirrors the lower part
+						acc[0] = fma(e[1], x1, fma(e[2], x2, fma(e[3], x3, acc[0])));
+						acc[1] = fma(e[6], x2, fma(e[7], x3, acc[1]));
+						acc[2] = fma(e[11], x3, acc[2]);
+						if (want_norm) {
+							sa[0] += fabs(e[1]) + fabs(e[2]) + fabs(e[3]);
+							sa[1] += fabs(e[6]) + fabs(e[7]);
+							sa[2] += fabs(e[11]);
+						}
+					}
+				} else {
+					const double x0 = x[4 * ti], x1 = x[4 * ti + 1], x2 = x[4 * ti + 2], x3 = x[4 * ti + 3];
+#pragma unroll
+					for (int q = 0; q < 4; q++) {
+						acc[q] = fma(e[4 * q], x0, fma(e[4 * q + 1], x1, fma(e[4 * q + 2], x2, fma(e[4 * q + 3], x3, acc[q]))));
+						if (want_norm)
+							sa[q] += fabs(e[4 * q]) + fabs(e[4 * q + 1]) + fabs(e[4 * q + 2]) + fabs(e[4 * q + 3]);
+					}
+				}
 			}
-			// mask entries outside the matrix (padding rows/cols may hold anything)
 #pragma unroll
-			for (int q = 0; q < 4; q++)
+			for (int off = 16; off > 0; off >>= 1)
 #pragma unroll
 				for (int rr = 0; rr < 4; rr++) {
-					int gi = 4 * ti + rr, gj = 4 * tj + q;
-					bool ok = gi < n && gj < n && (tj < ti || gj <= gi);
-					if (!ok) e[4 * q + rr] = 0.0;
+					acc[rr] += __shfl_down_sync(0xffffffffu, acc[rr], off);
+					if (want_norm) sa[rr] += __shfl_down_sync(0xffffffffu, sa[rr], off);
 				}
-			const double xj0 = x[4 * tj], xj1 = x[4 * tj + 1], xj2 = x[4 * tj + 2], xj3 = x[4 * tj + 3];
-			// rows of ti: A_tile * x_tj
-			acc0 = fma(e[0], xj0, fma(e[4], xj1, fma(e[8], xj2, fma(e[12], xj3, acc0))));
-			acc1 = fma(e[1], xj0, fma(e[5], xj1, fma(e[9], xj2, fma(e[13], xj3, acc1))));
-			acc2 = fma(e[2], xj0, fma(e[6], xj1, fma(e[10], xj2, fma(e[14], xj3, acc2))));
-			acc3 = fma(e[3], xj0, fma(e[7], xj1, fma(e[11], xj2, fma(e[15], xj3, acc3))));
-			if (want_norm) {
-				s0 += fabs(e[0]) + fabs(e[4]) + fabs(e[8]) + fabs(e[12]);
-				s1 += fabs(e[1]) + fabs(e[5]) + fabs(e[9]) + fabs(e[13]);
-				s2 += fabs(e[2]) + fabs(e[6]) + fabs(e[10]) + fabs(e[14]);
-				s3 += fabs(e[3]) + fabs(e[7]) + fabs(e[11]) + fabs(e[15]);
-			}
-			if (tj < ti) {
-				// transposed part: rows of tj get A_tile^T * x_ti
-				double c0 = fma(e[0], xi0, fma(e[1], xi1, fma(e[2], xi2, e[3] * xi3)));
-				double c1 = fma(e[4], xi0, fma(e[5], xi1, fma(e[6], xi2, e[7] * xi3)));
-				double c2 = fma(e[8], xi0, fma(e[9], xi1, fma(e[10], xi2, e[11] * xi3)));
-				double c3 = fma(e[12], xi0, fma(e[13], xi1, fma(e[14], xi2, e[15] * xi3)));
-				atomicAdd(&r[4 * tj], -c0);
-				atomicAdd(&r[4 * tj + 1], -c1);
-				atomicAdd(&r[4 * tj + 2], -c2);
-				atomicAdd(&r[4 * tj + 3], -c3);
-				if (want_norm) {
-					atomicAdd(&asum[4 * tj], fabs(e[0]) + fabs(e[1]) + fabs(e[2]) + fabs(e[3]));
-					atomicAdd(&asum[4 * tj + 1], fabs(e[4]) + fabs(e[5]) + fabs(e[6]) + fabs(e[7]));
-					atomicAdd(&asum[4 * tj + 2], fabs(e[8]) + fabs(e[9]) + fabs(e[10]) + fabs(e[11]));
-					atomicAdd(&asum[4 * tj + 3], fabs(e[12]) + fabs(e[13]) + fabs(e[14]) + fabs(e[15]));
-				}
-			} else {
-				// diagonal tile: the strictly-upper part is the mirror of the lower part
-				acc0 = fma(e[1], xi1, fma(e[2], xi2, fma(e[3], xi3, acc0)));
-				acc1 = fma(e[6], xi2, fma(e[7], xi3, acc1));
-				acc2 = fma(e[11], xi3, acc2);
-				if (want_norm) {
-					s0 += fabs(e[1]) + fabs(e[2]) + fabs(e[3]);
-					s1 += fabs(e[6]) + fabs(e[7]);
-					s2 += fabs(e[11]);
-				}
-			}
-		}
+			if (lane == 0) {
 #pragma unroll
-		for (int off = 16; off > 0; off >>= 1) {
-			acc0 += __shfl_down_sync(0xffffffffu, acc0, off);
-			acc1 += __shfl_down_sync(0xffffffffu, acc1, off);
-			acc2 += __shfl_down_sync(0xffffffffu, acc2, off);
-			acc3 += __shfl_down_sync(0xffffffffu, acc3, off);
-			if (want_norm) {
-				s0 += __shfl_down_sync(0xffffffffu, s0, off);
-				s1 += __shfl_down_sync(0xffffffffu, s1, off);
-				s2 += __shfl_down_sync(0xffffffffu, s2, off);
-				s3 += __shfl_down_sync(0xffffffffu, s3, off);
+				for (int rr = 0; rr < 4; rr++) {
+					const int i = 4 * t0 + rr;
+					if (pass == 0) {
+						r[i] = (i < n ? b[i] : 0.0) - acc[rr];
+						if (want_norm) asum[i] = sa[rr];
+					} else {
+						r[i] -= acc[rr];
+						if (want_norm) asum[i] += sa[rr];
+					}
+				}
 			}
 		}
-		if (lane == 0) {
-			atomicAdd(&r[4 * ti], -acc0);
-			atomicAdd(&r[4 * ti + 1], -acc1);
-			atomicAdd(&r[4 * ti + 2], -acc2);
-			atomicAdd(&r[4 * ti + 3], -acc3);
-			if (want_norm) {
-				atomicAdd(&asum[4 * ti], s0);
-				atomicAdd(&asum[4 * ti + 1], s1);
-				atomicAdd(&asum[4 * ti + 2], s2);
-				atomicAdd(&asum[4 * ti + 3], s3);
-			}
-		}
+		__syncthreads();
 	}
-	__syncthreads();
 }
 
-template <typename T, bool MIXED>
-__global__ void __launch_bounds__(256) k_posv(int cls, int max_n, PosvWs ws, const int *__restrict__ nvec,
+template <typename T, bool MIXED, int NT, int MINB>
+__global__ void __launch_bounds__(NT, MINB) k_posv(int cls, int max_n, PosvWs ws, const int *__restrict__ nvec,
                                               const DevDesc<double> *__restrict__ sA,
                                               const DevVec<double> *__restrict__ sb,
                                               const DevVec<double> *__restrict__ sx, int max_iter, double tol,
-                                              int *iters, double *berr, int *info) {
+                                              int *iters, double *berr, int *info, double *slots) {
 	extern __shared__ __align__(16) unsigned char smem[];
 	const PosvPlan pl = posv_plan<T, MIXED>(max_n);
+	// per-CTA FP64 copy of the lower panels (refinement residuals read it from
+	// L2 instead of the caller's matrix, which may sit in host memory)
+	double *slot = slots ? slots + (size_t)blockIdx.x * lp_size(max_n) : nullptr;
+	double *asum = (double *)(smem + pl.asum_off);
 	T *S = (T *)(smem + pl.S_off);
 	T *invL = (T *)(smem + pl.inv_off);
 	double *dinv = (double *)(smem + pl.dinv_off);
@@ -371,32 +363,14 @@ __global__ void __launch_bounds__(256) k_posv(int cls, int max_n, PosvWs ws, con
 		const int P = (n + 3) >> 2;
 		const int nv = ((n + 15) >> 4) * 16;
 
-		// lower triangle -> lower panels (converted to T), identity padding
-		{
-			const int warp = tid >> 5, lane = tid & 31, nw = nt >> 5;
-			for (int p = warp; p < P; p += nw) {
-				T *dst = S + lp_off(p);
-				const double *src = a.p + (size_t)(4 * p) * a.cn;
-				const int cnt = 16 * (p + 1);
-				for (int e = 2 * lane; e < cnt; e += 64) {
-					double2 v = __ldg((const double2 *)(src + e));
-					int i0 = 4 * p + (e & 3), j0 = e >> 2;
-					T v0, v1;
-					// e is even: elements e, e+1 are rows i0, i0+1 of column j0
-					if (i0 < n && j0 < n) v0 = (j0 <= i0) ? (T)v.x : T(0);
-					else v0 = (i0 == j0) ? T(1) : T(0);
-					if (i0 + 1 < n && j0 < n) v1 = (j0 <= i0 + 1) ? (T)v.y : T(0);
-					else v1 = (i0 + 1 == j0) ? T(1) : T(0);
-					dst[e] = v0;
-					dst[e + 1] = v1;
-				}
-			}
-			for (int i = tid; i < nv; i += nt) w[i] = (i < n) ? (T)bg[i] : T(0);
-			if (MIXED)
-				for (int i = tid; i < nv; i += nt) xs[i] = 0.0;
-		}
+		// lower triangle -> lower panels (converted to T), identity padding; the
+		// mixed path with refinement slots also keeps an FP64 copy there
+		load_lp_vec<T, double, 2>(S, n, a.p, a.cn, MIXED ? slot : nullptr);
+		for (int i = tid; i < nv; i += nt) w[i] = (i < n) ? (T)bg[i] : T(0);
+		if (MIXED)
+			for (int i = tid; i < nv; i += nt) xs[i] = 0.0;
 		__syncthreads();
-		chol_smem<T>(S, n, dinv, invL, MIXED ? 256 : 0, scratch, s_bad);
+		chol_smem<T>(S, n, dinv, scratch, s_bad, MIXED ? invL : (T *)nullptr);
 
 		if (!MIXED) {
 			trsv_fwd<T>(S, n, nullptr, dinv, w, ybuf);
@@ -428,7 +402,10 @@ __global__ void __launch_bounds__(256) k_posv(int cls, int max_n, PosvWs ws, con
 			trsv_bwd<T>(S, n, invL, dinv, w, ybuf);
 			for (int i = tid; i < n; i += nt) xs[i] += (double)w[i] / scale;
 			__syncthreads();
-			sym_residual(a, n, bg, xs, rs, nullptr, false);
+			if (slot)
+				sym_residual<true>(slot, 0, n, bg, xs, rs, asum, it == 0);
+			else
+				sym_residual<false>(a.p, a.cn, n, bg, xs, rs, asum, it == 0);
 			// norms
 			double rm = 0.0, xm = 0.0;
 			for (int i = tid; i < n; i += nt) {
@@ -438,14 +415,9 @@ __global__ void __launch_bounds__(256) k_posv(int cls, int max_n, PosvWs ws, con
 			rm = block_max<T>(rm, misc);
 			xm = block_max<T>(xm, misc);
 			if (it == 0) {
-				// ||A||_inf from the lower triangle: row i sums row part + column part
+				// ||A||_inf: row sums of |A| accumulated by the first residual pass
 				double am = 0.0;
-				for (int i = tid; i < n; i += nt) {
-					double s = 0.0;
-					for (int j = 0; j <= i; j++) s += fabs(a.at(i, j));
-					for (int j = i + 1; j < n; j++) s += fabs(a.at(j, i));
-					am = fmax(am, s);
-				}
+				for (int i = tid; i < n; i += nt) am = fmax(am, asum[i]);
 				anorm = block_max<T>(am, misc);
 			}
 			it++;
@@ -504,9 +476,10 @@ __global__ void __launch_bounds__(256) k_posv_global(int cls, int max_n, PosvWs 
 		a.p = sA[sys].pA;
 		a.cn = sA[sys].cn;
 		a.ri = a.cj = 0;
-		for (long long e = tid; e < (long long)n * n; e += nt) {
-			int i = (int)(e % n), j = (int)(e / n);
-			if (j <= i) L[e] = a.at(i, j);
+		{
+			const int warp = tid >> 5, lane = tid & 31, nw = nt >> 5;
+			for (int j = warp; j < n; j += nw)
+				for (int i = j + lane; i < n; i += 32) L[(size_t)j * n + i] = a.at(i, j);
 		}
 		__syncthreads();
 		for (int j = 0; j < n; j++) {
@@ -522,10 +495,14 @@ __global__ void __launch_bounds__(256) k_posv_global(int cls, int max_n, PosvWs 
 			__syncthreads();
 			for (int i = j + 1 + tid; i < n; i += nt) L[(size_t)j * n + i] *= s_inv;
 			__syncthreads();
-			const int r = n - j - 1;
-			for (long long e = tid; e < (long long)r * r; e += nt) {
-				int i = j + 1 + (int)(e % r), l = j + 1 + (int)(e / r);
-				if (l <= i) L[(size_t)l * n + i] = fma(-L[(size_t)j * n + i], L[(size_t)j * n + l], L[(size_t)l * n + i]);
+			{
+				const int warp = tid >> 5, lane = tid & 31, nw = nt >> 5;
+				const double *lj = L + (size_t)j * n;
+				for (int l = j + 1 + warp; l < n; l += nw) {
+					const double ljl = lj[l];
+					double *col = L + (size_t)l * n;
+					for (int i = l + lane; i < n; i += 32) col[i] = fma(-lj[i], ljl, col[i]);
+				}
 			}
 			__syncthreads();
 		}
@@ -561,9 +538,27 @@ struct PosvClassCfg {
 	int threads;
 };
 
+template <typename T, bool MIXED, int NT, int MINB>
+int launch_posv(int c, int upper, size_t smem, int batch, int rslots, PosvWs ws, const int *n, const void *sA,
+                const void *sb, const void *sx, int max_iter, double tol, int *iters, double *berr, int *info,
+                double *rs, cudaStream_t s) {
+	auto kern = k_posv<T, MIXED, NT, MINB>;
+	if (smem > 48 * 1024) cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+	int per_sm = 0;
+	cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, NT, smem);
+	if (per_sm < 1) per_sm = 1;
+	int grid = bf::num_sms() * per_sm;
+	if (grid > batch) grid = batch;
+	if (rslots && grid > rslots) grid = rslots;
+	kern<<<grid, NT, smem, s>>>(c, upper, ws, n, (const DevDesc<double> *)sA, (const DevVec<double> *)sb,
+	                            (const DevVec<double> *)sx, max_iter, tol, iters, berr, info, rs);
+	return bf::check_launch();
+}
+
 template <typename T, bool MIXED>
 int posv_run(int batch, const int *n, int max_n, const void *sA, const void *sb, const void *sx, int max_iter,
-             double tol, int *iters, double *berr, int *info, void *work, size_t work_bytes, cudaStream_t s) {
+             double tol, int *iters, double *berr, int *info, void *work, size_t work_bytes, cudaStream_t s,
+             bool use_slots) {
 	if (batch < 0 || !n || !sA || !sb || !sx || max_n < 0) return BLASFEO_B200_EINVAL;
 	if (batch == 0 || max_n == 0) return BLASFEO_B200_OK;
 	// size classes: shared memory and CTA size follow the largest member
@@ -580,7 +575,7 @@ int posv_run(int batch, const int *n, int max_n, const void *sA, const void *sb,
 		int uu = u < smem_limit_n ? u : smem_limit_n;
 		if (nc > 0 && uu <= cfg[nc - 1].upper) continue;
 		cfg[nc].upper = uu;
-		cfg[nc].threads = uu <= 32 ? 64 : (uu <= 96 ? 128 : 256);
+		cfg[nc].threads = uu <= 64 ? 64 : (uu <= 128 ? 128 : (uu <= 192 ? 256 : 512));
 		nc++;
 		if (uu >= max_n) break;
 	}
@@ -599,6 +594,14 @@ int posv_run(int batch, const int *n, int max_n, const void *sA, const void *sb,
 	size_t slot_bytes = ((size_t)max_n * max_n + 2 * (size_t)max_n) * sizeof(double);
 	size_t slots_off = need;
 	need += (size_t)gslots * slot_bytes;
+	// refinement slots of the mixed kernel: one per resident CTA of the largest class
+	size_t rslots_off = a16(need);
+	int rslots = 0;
+	if (MIXED && use_slots) {
+		const int per_sm = 16;  // upper bound of resident CTAs per SM over all classes
+		rslots = bf::num_sms() * per_sm;
+		need = rslots_off + (size_t)rslots * lp_size(max_n) * sizeof(double);
+	}
 	char *wsp = (char *)work;
 	if (!wsp) {
 		wsp = (char *)bf::workspace(need, s);
@@ -627,17 +630,21 @@ int posv_run(int batch, const int *n, int max_n, const void *sA, const void *sb,
 			                                     (double *)(wsp + slots_off), info);
 		} else {
 			PosvPlan pl = posv_plan<T, MIXED>(cfg[c].upper);
-			if (pl.total > 48 * 1024)
-				cudaFuncSetAttribute(k_posv<T, MIXED>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pl.total);
-			int per_sm = 0;
-			cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_posv<T, MIXED>, cfg[c].threads, pl.total);
-			if (per_sm < 1) per_sm = 1;
-			int grid = sms * per_sm;
-			if (grid > batch) grid = batch;
-			k_posv<T, MIXED><<<grid, cfg[c].threads, pl.total, s>>>(c, cfg[c].upper, ws, n, (const DevDesc<double> *)sA,
-			                                                        (const DevVec<double> *)sb,
-			                                                        (const DevVec<double> *)sx, max_iter, tol, iters,
-			                                                        berr, info);
+			double *rs = rslots ? (double *)(wsp + rslots_off) : nullptr;
+			int st;
+			if (cfg[c].upper <= 64)
+				st = launch_posv<T, MIXED, 64, 8>(c, cfg[c].upper, pl.total, batch, rslots, ws, n, sA, sb, sx, max_iter,
+				                                  tol, iters, berr, info, rs, s);
+			else if (cfg[c].upper <= 128)
+				st = launch_posv<T, MIXED, 128, 4>(c, cfg[c].upper, pl.total, batch, rslots, ws, n, sA, sb, sx,
+				                                   max_iter, tol, iters, berr, info, rs, s);
+			else if (cfg[c].upper <= 192)
+				st = launch_posv<T, MIXED, 256, 2>(c, cfg[c].upper, pl.total, batch, rslots, ws, n, sA, sb, sx,
+				                                   max_iter, tol, iters, berr, info, rs, s);
+			else
+				st = launch_posv<T, MIXED, 512, 1>(c, cfg[c].upper, pl.total, batch, rslots, ws, n, sA, sb, sx,
+				                                   max_iter, tol, iters, berr, info, rs, s);
+			if (st) return st;
 		}
 		if (bf::check_launch()) return BLASFEO_B200_ECUDA;
 	}
@@ -658,14 +665,22 @@ int blasfeo_dposv_l_vbatch(int batch, const int *n, int max_n, const struct blas
                            const struct blasfeo_dvec *sb, const struct blasfeo_dvec *sx, int *info, void *work,
                            size_t work_bytes, void *stream) {
 	return posv_run<double, false>(batch, n, max_n, sA, sb, sx, 0, 0.0, nullptr, nullptr, info, work, work_bytes,
-	                               (cudaStream_t)stream);
+	                               (cudaStream_t)stream, false);
 }
 
 int blasfeo_dsposv_l_vbatch(int batch, const int *n, int max_n, const struct blasfeo_dmat *sA,
                             const struct blasfeo_dvec *sb, const struct blasfeo_dvec *sx, int max_iter, double tol,
                             int *iters, double *berr, int *info, void *work, size_t work_bytes, void *stream) {
 	return posv_run<float, true>(batch, n, max_n, sA, sb, sx, max_iter, tol, iters, berr, info, work, work_bytes,
-	                             (cudaStream_t)stream);
+	                             (cudaStream_t)stream, false);
+}
+
+int blasfeo_dsposv_l_vbatch_mapped(int batch, const int *n, int max_n, const struct blasfeo_dmat *sA,
+                                   const struct blasfeo_dvec *sb, const struct blasfeo_dvec *sx, int max_iter,
+                                   double tol, int *iters, double *berr, int *info, void *work, size_t work_bytes,
+                                   void *stream) {
+	return posv_run<float, true>(batch, n, max_n, sA, sb, sx, max_iter, tol, iters, berr, info, work, work_bytes,
+	                             (cudaStream_t)stream, true);
 }
 
 }  // extern "C"

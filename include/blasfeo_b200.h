@@ -99,6 +99,9 @@ void blasfeo_b200_set_stream(void *stream);         /* stream of the single-inst
 void *blasfeo_b200_get_stream(void);
 void blasfeo_b200_set_sync(int sync);               /* 1 (default): single-instance calls synchronise before return */
 int blasfeo_b200_version(void);
+/* measured FMA throughput (GFLOP/s) of the current device, prec 'd' or 's';
+ * the roofline denominator of the SIMT kernels (no reference counterpart) */
+double blasfeo_b200_measure_fma_peak(char prec, int iters);
 
 /* ---- storage: auxiliary/d_aux_lib4.c:1519,1548,1575,1588 / include/blasfeo_d_aux.h ---- */
 size_t blasfeo_memsize_dmat(int m, int n);
@@ -250,6 +253,15 @@ int blasfeo_dposv_l_vbatch(int batch, const int *n, int max_n, const struct blas
 	const struct blasfeo_dvec *sb, const struct blasfeo_dvec *sx, int *info,
 	void *work, size_t work_bytes, void *stream);
 int blasfeo_dsposv_l_vbatch(int batch, const int *n, int max_n, const struct blasfeo_dmat *sA,
+	const struct blasfeo_dvec *sb, const struct blasfeo_dvec *sx, int max_iter, double tol,
+	int *iters, double *berr, int *info, void *work, size_t work_bytes, void *stream);
+
+/* Same as blasfeo_dsposv_l_vbatch, for callers whose matrices, vectors, sizes
+ * and descriptors live in mapped (cudaHostAlloc / cudaHostRegister) host
+ * memory: the kernels read the lower triangles straight over the host link
+ * (only the lower triangle crosses it) and keep a per-CTA FP64 copy in device
+ * memory for the refinement residuals; x is written back to host memory. */
+int blasfeo_dsposv_l_vbatch_mapped(int batch, const int *n, int max_n, const struct blasfeo_dmat *sA,
 	const struct blasfeo_dvec *sb, const struct blasfeo_dvec *sx, int max_iter, double tol,
 	int *iters, double *berr, int *info, void *work, size_t work_bytes, void *stream);
 

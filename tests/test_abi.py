@@ -1,0 +1,93 @@
+"""CPU tests of the C-ABI boundary: the shared library loads, exports every
+function declared in include/blasfeo_b200.h, keeps the reference's descriptor
+layout and storage sizes, and rejects bad arguments before touching a GPU."""
+import ctypes as C
+import os
+import re
+
+import numpy as np
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+HEADER = os.path.join(ROOT, "include", "blasfeo_b200.h")
+
+
+def declared_functions():
+    src = open(HEADER).read()
+    src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+    names = re.findall(r"^\s*(?:[A-Za-z_][\w\s\*]*?)\b(blasfeo_\w+)\s*\(", src, flags=re.M)
+    return sorted(set(names))
+
+
+def test_header_declares_hot_path():
+    names = declared_functions()
+    for r in ["blasfeo_dgemm_nt", "blasfeo_dsyrk_ln", "blasfeo_dtrsm_rltn", "blasfeo_dpotrf_l", "blasfeo_dgetrf_rp",
+              "blasfeo_dgeqrf", "blasfeo_dgeqrf_worksize", "blasfeo_dsyrk_dpotrf_ln", "blasfeo_sgemm_nt",
+              "blasfeo_ssyrk_ln", "blasfeo_strsm_rltn", "blasfeo_spotrf_l", "blasfeo_sgetrf_rp", "blasfeo_sgeqrf",
+              "blasfeo_memsize_dmat", "blasfeo_create_dmat", "blasfeo_pack_dmat", "blasfeo_unpack_dmat"]:
+        assert r in names, r
+
+
+def test_library_exports_every_declared_symbol():
+    import blasfeo_b200
+    missing = [n for n in declared_functions() if not hasattr(blasfeo_b200.lib, n)]
+    assert not missing, missing
+
+
+def test_descriptor_layout():
+    import blasfeo_b200 as bf
+    assert C.sizeof(bf.dmat) == 48 and C.sizeof(bf.dvec) == 32
+    assert [f for f, _ in bf.dmat._fields_] == ["mem", "pA", "dA", "m", "n", "pm", "cn", "use_dA", "memsize"]
+
+
+@pytest.mark.parametrize("mn", [(64, 64), (16, 16), (16, 32), (5, 3), (1, 1), (257, 13), (13, 257)])
+def test_memsize_and_create_match_reference(mn):
+    import blasfeo_b200 as bf
+    m, n = mn
+    pm, cn = (m + 3) // 4 * 4, (n + 3) // 4 * 4
+    dl = (min(m, n) + 15) // 16 * 16
+    want = ((pm * cn + dl) * 8 + 63) // 64 * 64
+    assert bf.lib.blasfeo_memsize_dmat(m, n) == want
+    s = bf.dmat()
+    base = 0x10000
+    bf.lib.blasfeo_create_dmat(m, n, C.byref(s), C.c_void_p(base))
+    assert (s.m, s.n, s.pm, s.cn, s.use_dA) == (m, n, pm, cn, 0)
+    assert s.pA == base and s.dA == base + pm * cn * 8 and s.memsize == want
+    from oracle.pyoracle import ref_available, ref_lib
+    if ref_available("generic"):
+        r = ref_lib("generic")
+        r.blasfeo_memsize_dmat.restype = C.c_size_t
+        assert r.blasfeo_memsize_dmat(m, n) == want
+        r.blasfeo_memsize_smat.restype = C.c_size_t
+        assert r.blasfeo_memsize_smat(m, n) == bf.lib.blasfeo_memsize_smat(m, n)
+
+
+def test_batch_slab_layout():
+    import blasfeo_b200 as bf
+    s = bf.dmat_batch()
+    bf.lib.blasfeo_create_dmat_batch(16, 16, 100, C.byref(s), C.c_void_p(0x1000))
+    assert s.stride * 8 == bf.lib.blasfeo_memsize_dmat(16, 16)
+    assert s.memsize == 100 * bf.lib.blasfeo_memsize_dmat(16, 16)
+    inst = bf.dmat()
+    bf.lib.blasfeo_dmat_batch_instance(C.byref(s), 7, C.byref(inst))
+    assert inst.pA == 0x1000 + 7 * s.stride * 8
+
+
+def test_bad_arguments_rejected_without_gpu():
+    import blasfeo_b200 as bf
+    lib = bf.lib
+    EINVAL = 1
+    s = bf.dmat_batch()
+    assert lib.blasfeo_dgemm_nt_batch(-1, 4, 4, 4, 1.0, None, 0, 0, None, 0, 0, 0.0, None, 0, 0, None, 0, 0, None) == EINVAL
+    assert lib.blasfeo_dpotrf_l_batch(4, 4, None, 0, 0, C.byref(s), 0, 0, None, None) == EINVAL
+    assert lib.blasfeo_dposv_l_vbatch(-1, None, 4, None, None, None, None, None, 0, None) == EINVAL
+    assert lib.blasfeo_dsposv_l_vbatch(3, None, 4, None, None, None, 10, 1e-12, None, None, None, None, 0, None) == EINVAL
+    # zero-size calls are no-ops that succeed
+    assert lib.blasfeo_dpotrf_l_batch(0, 4, C.byref(s), 0, 0, C.byref(s), 0, 0, None, None) == 0
+    assert lib.blasfeo_dgeqrf_worksize(12, 8) == 4 * (12 + 8) * 8
+
+
+def test_error_strings():
+    import blasfeo_b200 as bf
+    assert bf.lib.blasfeo_b200_error_string(0) == b"ok"
+    assert b"invalid" in bf.lib.blasfeo_b200_error_string(1)

@@ -1,0 +1,197 @@
+"""CPU tests of the oracle: pinned against the golden fixtures generated from
+the compiled reference (tests/golden/make_golden.py) and, where the compiled
+reference is present (oracle/_ref), against the reference itself on random
+inputs with row/column offsets (the sweep structure of the reference's
+tests/test_x.c)."""
+import hashlib
+import json
+import os
+
+import numpy as np
+import pytest
+
+from tests.helpers import oracle_api, relfro
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+GOLD = os.path.join(HERE, "golden")
+NP = {"d": np.float64, "s": np.float32}
+TOL = {"d": 1e-13, "s": 2e-6}
+
+
+@pytest.fixture(scope="module")
+def orc():
+    return oracle_api()
+
+
+def gold(name):
+    return np.load(os.path.join(GOLD, name))
+
+
+def host(m, n, prec="d", data=None):
+    from oracle.pyoracle import HostMat
+    h = HostMat(m, n, NP[prec])
+    if data is not None:
+        h.set(data)
+    return h
+
+
+def test_manifest_hashes():
+    man = json.load(open(os.path.join(GOLD, "manifest.json")))
+    for name, sha in man["files"].items():
+        assert hashlib.sha256(open(os.path.join(GOLD, name), "rb").read()).hexdigest() == sha, name
+
+
+@pytest.mark.parametrize("prec", ["d", "s"])
+def test_oracle_vs_golden_testx(orc, prec):
+    import sys
+    sys.path.insert(0, GOLD)
+    from make_golden import run_testx
+    g = gold("testx_%s.npz" % prec)
+    out = run_testx(orc, prec)
+    for k in g.files:
+        if k.endswith("ipiv"):
+            assert np.array_equal(out[k], g[k]), k
+        else:
+            assert relfro(out[k], g[k]) <= TOL[prec] * (10 if prec == "d" else 100), (k, relfro(out[k], g[k]))
+
+
+def test_oracle_vs_golden_cfg1(orc):
+    g = gold("cfg1.npz")
+    n = 64
+    hA, hB, hC, hD = host(n, n, data=g["A"]), host(n, n, data=g["B"]), host(n, n), host(n, n)
+    orc.gemm_nt("d", n, n, n, 1.0, hA, 0, 0, hB, 0, 0, 0.0, hC, 0, 0, hD, 0, 0)
+    assert relfro(hD.get(), g["D"]) <= 1e-13
+    hS, hL = host(n, n, data=g["S"]), host(n, n)
+    orc.potrf_l("d", n, hS, 0, 0, hL, 0, 0)
+    assert relfro(np.tril(hL.get()), g["L"]) <= 1e-13
+    assert relfro(hL.diag(n), g["L_dA"]) <= 1e-13
+    hR, hX = host(n, n, data=g["R"]), host(n, n)
+    orc.trsm_rltn("d", n, n, 1.0, hL, 0, 0, hR, 0, 0, hX, 0, 0)
+    assert relfro(hX.get(), g["X"]) <= 1e-13
+
+
+def test_oracle_vs_golden_cfg3(orc):
+    from oracle.pyoracle import HostVec
+    g = gold("cfg3.npz")
+    for i, n in enumerate(g["ns"]):
+        n = int(n)
+        hA, hL = host(n, n, data=g["A%d" % i]), host(n, n)
+        orc.potrf_l("d", n, hA, 0, 0, hL, 0, 0)
+        assert relfro(np.tril(hL.get()), g["L%d" % i]) <= 1e-13
+        hb, hy, hx = HostVec(n).set(g["b%d" % i]), HostVec(n), HostVec(n)
+        orc.trsv_lnn("d", n, hL, 0, 0, hb, 0, hy, 0)
+        orc.trsv_ltn("d", n, hL, 0, 0, hy, 0, hx, 0)
+        # cond up to 1e6: solutions of two FP64 solvers agree to ~cond*eps
+        assert relfro(hx.get(), g["x%d" % i]) <= 1e-9
+
+
+def test_oracle_vs_golden_cfg4(orc):
+    import sys
+    sys.path.insert(0, GOLD)
+    from make_golden import riccati_ref
+    g = gold("cfg4.npz")
+    for p in range(2):
+        Ls = riccati_ref(orc, g["A%d" % p], g["B%d" % p])
+        for k, L in enumerate(Ls):
+            ref = g["L%d" % p][k][: L.shape[0], : L.shape[1]]
+            assert relfro(L, ref) <= 1e-13, (p, k)
+
+
+def test_oracle_vs_golden_cfg5(orc):
+    g = gold("cfg5.npz")
+    for i, n in enumerate([5, 11, 27, 64]):
+        hM, hD = host(n, n, data=g["lu_in%d" % i]), host(n, n)
+        piv = orc.getrf_rp("d", n, n, hM, 0, 0, hD, 0, 0)
+        assert np.array_equal(piv, g["lu_ipiv%d" % i])
+        assert relfro(hD.get(), g["lu%d" % i]) <= 1e-13
+    for i, n in enumerate([3, 8, 21, 40]):
+        hM, hD = host(2 * n, n, data=g["qr_in%d" % i]), host(2 * n, n)
+        orc.geqrf("d", 2 * n, n, hM, 0, 0, hD, 0, 0)
+        assert relfro(hD.get(), g["qr%d" % i]) <= 1e-13
+        assert relfro(hD.diag(n), g["qr_tau%d" % i]) <= 1e-13
+
+
+def test_oracle_vs_golden_cfg2(orc):
+    g = gold("cfg2.npz")
+    m, k = 16, 32
+    for b in range(g["A"].shape[0]):
+        hA, hS = host(m, k, data=g["A"][b]), host(m, m)
+        orc.syrk_ln("d", m, k, 1.0, hA, 0, 0, hA, 0, 0, 0.0, hS, 0, 0, hS, 0, 0)
+        import ctypes as C
+        orc.lib.oracle_d_diare(m, C.c_double(16.0), hS.ref, 0, 0)
+        hL = host(m, m)
+        orc.potrf_l("d", m, hS, 0, 0, hL, 0, 0)
+        hR, hX = host(m, m, data=g["R"][b]), host(m, m)
+        orc.trsm_rltn("d", m, m, 1.0, hL, 0, 0, hR, 0, 0, hX, 0, 0)
+        hC, hG, hD = host(m, m, data=g["C"][b]), host(m, m, data=g["G"][b]), host(m, m)
+        orc.gemm_nt("d", m, m, m, -1.0, hX, 0, 0, hG, 0, 0, 1.0, hC, 0, 0, hD, 0, 0)
+        assert relfro(np.tril(hL.get()), g["L"][b]) <= 1e-13
+        assert relfro(hD.get(), g["D"][b]) <= 1e-13
+
+
+# ---- against the compiled reference itself (when built here) ----
+
+def _ref_or_skip(target="generic"):
+    from oracle.pyoracle import Api, ref_available
+    if not ref_available(target):
+        pytest.skip("compiled reference not built (make -C oracle generic)")
+    return Api("hp", target), Api("ref", target)
+
+
+@pytest.mark.parametrize("prec", ["d", "s"])
+@pytest.mark.parametrize("case", [(7, 5, 3, 1, 2, 3, 0), (16, 16, 16, 0, 0, 0, 0), (33, 19, 40, 2, 1, 0, 3)])
+def test_oracle_vs_reference_gemm_offsets(orc, prec, case):
+    hp, _ = _ref_or_skip()
+    m, n, k, ai, bi, ci, di = case
+    rng = np.random.default_rng(m + n + k)
+    A, B = rng.standard_normal((m + ai, k + 2)), rng.standard_normal((n + bi, k + 2))
+    Cm, D0 = rng.standard_normal((m + ci, n + 1)), rng.standard_normal((m + di, n + 1))
+    outs = []
+    for api in (orc, hp):
+        hA, hB, hC, hD = host(m + ai, k + 2, prec, A), host(n + bi, k + 2, prec, B), host(m + ci, n + 1, prec, Cm), host(m + di, n + 1, prec, D0)
+        api.gemm_nt(prec, m, n, k, -0.75, hA, ai, 2, hB, bi, 1, 1.25, hC, ci, 1, hD, di, 0)
+        outs.append(hD.get())
+    assert relfro(outs[0], outs[1]) <= TOL[prec] * 10
+
+
+@pytest.mark.parametrize("prec", ["d", "s"])
+@pytest.mark.parametrize("n", [1, 3, 4, 9, 21, 60])
+def test_oracle_vs_reference_factorizations(orc, prec, n):
+    hp, ref = _ref_or_skip()
+    rng = np.random.default_rng(n)
+    g = rng.standard_normal((n, n))
+    S = g @ g.T + n * np.eye(n)
+    M = rng.standard_normal((n, n))
+    T = rng.standard_normal((2 * n, n))
+    res = {}
+    for name, api in (("o", orc), ("hp", hp), ("ref", ref)):
+        hS, hL = host(n, n, prec, S), host(n, n, prec)
+        api.potrf_l(prec, n, hS, 0, 0, hL, 0, 0)
+        hX, hY = host(n + 2, n, prec, rng.standard_normal((n + 2, n)) if name == "o" else res["o"]["X"]), host(n + 2, n, prec)
+        api.trsm_rltn(prec, n + 2, n, 1.0, hL, 0, 0, hX, 0, 0, hY, 0, 0)
+        hM, hLU = host(n, n, prec, M), host(n, n, prec)
+        piv = api.getrf_rp(prec, n, n, hM, 0, 0, hLU, 0, 0)
+        hT, hQ = host(2 * n, n, prec, T), host(2 * n, n, prec)
+        api.geqrf(prec, 2 * n, n, hT, 0, 0, hQ, 0, 0)
+        res[name] = {"L": np.tril(hL.get()), "X": hX.get(), "Y": hY.get(), "LU": hLU.get(), "piv": piv,
+                     "QR": hQ.get(), "tau": hQ.diag(n)}
+    for other in ("hp", "ref"):
+        for k in ("L", "Y", "LU", "QR", "tau"):
+            assert relfro(res["o"][k], res[other][k]) <= TOL[prec] * 100, (other, k)
+        assert np.array_equal(res["o"]["piv"], res[other]["piv"])
+
+
+def test_memsize_matches_reference_layout():
+    from oracle.pyoracle import oracle_lib
+    import ctypes as C
+    lib = oracle_lib()
+    lib.oracle_d_memsize_mat.restype = C.c_size_t
+    for m, n in [(64, 64), (16, 16), (16, 32), (5, 3), (1, 1), (257, 13)]:
+        pm, cn = (m + 3) // 4 * 4, (n + 3) // 4 * 4
+        dl = (min(m, n) + 15) // 16 * 16
+        want = ((pm * cn + dl) * 8 + 63) // 64 * 64
+        assert lib.oracle_d_memsize_mat(m, n) == want
+    # the figures quoted for the configurations: 64x64 -> 33,280 B, 16x16 -> 2,176 B, 16x32 -> 4,224 B
+    assert lib.oracle_d_memsize_mat(64, 64) == 33280
+    assert lib.oracle_d_memsize_mat(16, 16) == 2176
+    assert lib.oracle_d_memsize_mat(16, 32) == 4224
