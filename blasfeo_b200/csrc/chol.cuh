@@ -13,19 +13,19 @@
 // Padding rows/columns (n..4P-1) hold the identity so they factor to the
 // identity and never touch real entries.
 //
-// Algorithm: right-looking, 16 columns (4 panels) per block step, with
-// look-ahead:
-//   1. panel solve of block column K by substitution, one thread per row,
-//      with the FP64 diagonal block and its reciprocal pivots;
-//   2. rank-16 update of block column K+1 (all threads);
-//   3. warp 0 factors diagonal block K+1 in FP64 (pivot rule of
+// Algorithm: right-looking, 16 columns (4 panels) per block step, two
+// __syncthreads per step:
+//   A. all threads: panel of block column K as a product with the explicit
+//      inverse of the diagonal block, L_IK = A_IK inv(L_KK)^T (no sequential
+//      dependence inside a row);
+//   B. warp 0 (critical path): rank-16 update of the 16x16 diagonal block K+1,
+//      its factorization in FP64 registers (pivot rule of
 //      kernel/generic/kernel_dgemm_4x4_lib4.c:5700-5710: c>0 -> sqrt(c) and its
-//      reciprocal, else 0 and 0) while the other warps apply the rank-16
-//      update to the rest of the trailing matrix (one 4x4 tile per thread).
-// Three __syncthreads per 16 columns; the serial diagonal factorization is
-// hidden behind the trailing update.  Explicit inverses of the diagonal blocks
-// (used by the refinement solves) are formed after the factorization, all
-// blocks in parallel.
+//      reciprocal, else 0 and 0) and its explicit inverse in FP64;
+//      all other warps: rank-16 update of the rest of the trailing matrix
+//      (one 4x4 tile per thread), which hides the serial diagonal work.
+// The inverses of the diagonal blocks are kept (invL_all) for the triangular
+// solves of the refinement loop.
 #pragma once
 #include "common.cuh"
 
@@ -117,14 +117,44 @@ __device__ __forceinline__ void chol_pivot_rsqrt(double c, double &d, double &in
 	}
 }
 
-// Factor the diagonal block at column c0 (nbk <= 16 real columns) with one
-// warp (lane i owns row c0+i, FP64).  Writes L_KK back into S, the FP64 block
-// into Ld (16x17 row-major), 1/L_jj into dinv[c0+j], the first bad pivot
-// (j+1) into *bad.
+// One column J of the 16x16 diagonal-block factorization; lane i holds row i
+// of the block in r[] (compile-time indices only, so r stays in registers).
+// The pivot is broadcast by a shuffle and every lane computes the reciprocal
+// square root itself; column J reaches the other rows by shuffles.
+template <int J>
+struct DiagCol {
+	static __device__ __forceinline__ void run(double (&r)[CHOL_NB], int lane, int nbk, int c0, double *dinv,
+	                                           int *bad) {
+		const double cj = __shfl_sync(0xffffffffu, r[J], J);
+		double d, inv;
+		chol_pivot_rsqrt(cj, d, inv);
+		r[J] = (lane == J) ? d : r[J] * inv;
+		if (lane == J && J < nbk) {
+			dinv[c0 + J] = inv;
+			if (!(cj > 0.0) && *bad == 0) *bad = c0 + J + 1;
+		}
+#pragma unroll
+		for (int l = J + 1; l < CHOL_NB; l++) {
+			const double t = __shfl_sync(0xffffffffu, r[J], l);
+			if (lane >= l) r[l] = fma(-r[J], t, r[l]);
+		}
+		DiagCol<J + 1>::run(r, lane, nbk, c0, dinv, bad);
+	}
+};
+template <>
+struct DiagCol<CHOL_NB> {
+	static __device__ __forceinline__ void run(double (&)[CHOL_NB], int, int, int, double *, int *) {}
+};
+
+// Warp 0: factor the diagonal block at column c0 (nbk <= 16 real columns; the
+// padding is the identity) in FP64 registers; write L_KK back into S, 1/L_jj
+// into dinv[c0+j] (FP64), the first bad pivot (j+1) into *bad, and for the
+// panel solve a row-major 16x17 copy Lt of L_KK in the working precision with
+// the reciprocal pivots in column 16.
 template <typename T>
-__device__ void chol_diag_factor(T *S, int c0, int nbk, double *dinv, double *Ld, int *bad) {
+__device__ void chol_diag_factor(T *S, int c0, int nbk, double *dinv, T *Lt, int *bad) {
 	const int lane = threadIdx.x & 31;
-	double v[CHOL_NB];
+	double r[CHOL_NB];
 #pragma unroll
 	for (int l = 0; l < CHOL_NB; l++) {
 		double x = 0.0;
@@ -134,41 +164,30 @@ __device__ void chol_diag_factor(T *S, int c0, int nbk, double *dinv, double *Ld
 			else if (l == lane)
 				x = 1.0;
 		}
-		v[l] = x;
+		r[l] = x;
 	}
-#pragma unroll
-	for (int j = 0; j < CHOL_NB; j++) {
-		double d = 0.0, inv = 0.0;
-		const double cj = __shfl_sync(0xffffffffu, v[j], j);
-		chol_pivot_rsqrt(cj, d, inv);
-		if (lane == j) {
-			v[j] = d;
-			if (!(cj > 0.0) && j < nbk && *bad == 0) *bad = c0 + j + 1;
-			if (j < nbk) dinv[c0 + j] = inv;
-		}
-		if (lane > j) v[j] *= inv;
-#pragma unroll
-		for (int l = j + 1; l < CHOL_NB; l++) {
-			double t = __shfl_sync(0xffffffffu, v[j], l);
-			if (lane >= l) v[l] = fma(-v[j], t, v[l]);
-		}
-	}
+	DiagCol<0>::run(r, lane, nbk, c0, dinv, bad);
 	if (lane < CHOL_NB) {
+		double dd = 1.0;
 #pragma unroll
-		for (int l = 0; l < CHOL_NB; l++) Ld[lane * 17 + l] = (l <= lane) ? v[l] : 0.0;
+		for (int l = 0; l < CHOL_NB; l++) {
+			Lt[lane * 17 + l] = (l <= lane) ? (T)r[l] : T(0);
+			if (l == lane) dd = r[l];
+		}
+		Lt[lane * 17 + 16] = (dd != 0.0) ? (T)(1.0 / dd) : T(0);
 		if (lane < nbk) {
 #pragma unroll
 			for (int l = 0; l < CHOL_NB; l++)
-				if (l <= lane && l < nbk) lp_at(S, c0 + lane, c0 + l) = (T)v[l];
+				if (l <= lane) lp_at(S, c0 + lane, c0 + l) = (T)r[l];
 		}
 	}
+	__syncwarp();
 }
 
-// panel solve of block column c0: rows r in [c0+16, rend):
-// L[r][c0+c] = (A[r][c0+c] - sum_{l<c} L[r][c0+l] L_KK[c][l]) * inv_c
+// panel of block column c0, rows r in [rbeg, rend): substitution with the
+// diagonal block, L[r][c0+c] = (A[r][c0+c] - sum_{l<c} L[r][c0+l] L_KK[c][l]) * inv_c
 template <typename T>
-__device__ __forceinline__ void chol_panel_rows(T *S, int c0, int rbeg, int rend, int tid0, int nthr,
-                                                const double *Ld, const double *dinv) {
+__device__ __forceinline__ void chol_panel_rows(T *S, int c0, int rbeg, int rend, int tid0, int nthr, const T *Lt) {
 	const int kb = c0 >> 2;
 	for (int r = rbeg + tid0; r < rend; r += nthr) {
 		const int p = r >> 2, ri = r & 3;
@@ -187,12 +206,36 @@ __device__ __forceinline__ void chol_panel_rows(T *S, int c0, int rbeg, int rend
 		for (int c = 0; c < CHOL_NB; c++) {
 			T s = a[c];
 #pragma unroll
-			for (int l = 0; l < c; l++) s = fma(-a[l], (T)Ld[c * 17 + l], s);
-			a[c] = s * (T)dinv[c0 + c];
+			for (int l = 0; l < c; l++) s = fma(-a[l], Lt[c * 17 + l], s);
+			a[c] = s * Lt[c * 17 + 16];
 		}
 #pragma unroll
 		for (int l = 0; l < CHOL_NB; l++) row[idx[l]] = a[l];
 	}
+}
+
+// Explicit inverse of diagonal block K (row-major 16x16, stored as T) from the
+// factor in S and the FP64 reciprocal pivots; lane c computes column c.
+template <typename T>
+__device__ void chol_block_inverse(const T *S, int n, int K, const double *dinv, T *invL, int lane) {
+	const int c0 = 16 * K;
+	const int nbk = min(CHOL_NB, n - c0);
+	const int c = lane;
+	if (c >= CHOL_NB) return;
+	double x[CHOL_NB];
+#pragma unroll
+	for (int i = 0; i < CHOL_NB; i++) {
+		double s = (i == c) ? 1.0 : 0.0;
+#pragma unroll
+		for (int l = 0; l < i; l++) {
+			const double lil = (i < nbk && l < nbk) ? (double)lp_at(S, c0 + i, c0 + l) : 0.0;
+			s = fma(-lil, x[l], s);
+		}
+		const double di = (i < nbk) ? dinv[c0 + i] : 1.0;
+		x[i] = (i < c) ? 0.0 : s * di;
+	}
+#pragma unroll
+	for (int i = 0; i < CHOL_NB; i++) invL[i * CHOL_NB + c] = (T)x[i];
 }
 
 // rank-16 update of tile (ti,tj) with the panel at block column c0
@@ -240,77 +283,49 @@ __device__ __forceinline__ void chol_tile_update(T *S, int ti, int tj, int c0) {
 	for (int q = 0; q < 4; q++) tile_col_st<T>(S, ti, tj, q, acc[4 * q], acc[4 * q + 1], acc[4 * q + 2], acc[4 * q + 3]);
 }
 
-// Explicit inverse of diagonal block K (row-major 16x16, stored as T) from
-// the factor in S and the FP64 reciprocal pivots; one lane per column.
-template <typename T>
-__device__ void chol_block_inverse(const T *S, int n, int K, const double *dinv, T *invL, int lane) {
-	const int c0 = 16 * K;
-	const int nbk = min(CHOL_NB, n - c0);
-	const int c = lane;
-	if (c >= CHOL_NB) return;
-	double x[CHOL_NB];
-#pragma unroll
-	for (int i = 0; i < CHOL_NB; i++) {
-		double s = (i == c) ? 1.0 : 0.0;
-#pragma unroll
-		for (int l = 0; l < i; l++) {
-			double lil = (i < nbk && l < nbk) ? (double)lp_at(S, c0 + i, c0 + l) : 0.0;
-			s = fma(-lil, x[l], s);
-		}
-		double di = (i < nbk) ? dinv[c0 + i] : 1.0;
-		x[i] = (i < c) ? 0.0 : s * di;
-	}
-#pragma unroll
-	for (int i = 0; i < CHOL_NB; i++) invL[i * CHOL_NB + c] = (T)x[i];
-}
-
 // Full factorization of the n x n lower-panel matrix S by the whole CTA
-// (blockDim.x >= 64).  dinv: FP64 shared array of >= 4P entries; Ld: 16*17
-// FP64 scratch; bad: shared int (0 on entry).  If invL_all is non-null the
-// explicit inverses of all diagonal blocks are formed at the end (256 entries
-// per block).
+// (blockDim.x >= 64).  dinv: FP64 shared array of >= 4P entries; Lt: 16*17
+// entries of T; bad: shared int (0 on entry).  If invL_all is non-null the
+// explicit inverses of all diagonal blocks (256 entries each, row-major) are
+// formed at the end, all blocks in parallel.
 template <typename T>
-__device__ void chol_smem(T *S, int n, double *dinv, double *Ld, int *bad, T *invL_all) {
+__device__ void chol_smem(T *S, int n, double *dinv, T *Lt, int *bad, T *invL_all) {
 	const int P = (n + 3) >> 2;
 	const int NB = (n + 15) >> 4;
 	const int tid = threadIdx.x, nt = blockDim.x;
-	const int warp = tid >> 5;
-	if (warp == 0) chol_diag_factor<T>(S, 0, min(CHOL_NB, n), dinv, Ld, bad);
+	const int warp = tid >> 5, lane = tid & 31;
+	if (warp == 0) chol_diag_factor<T>(S, 0, min(CHOL_NB, n), dinv, Lt, bad);
 	__syncthreads();
 	for (int K = 0; K < NB; K++) {
 		const int c0 = 16 * K, k0 = 4 * K;
-		// 1. panel rows below the diagonal block
-		chol_panel_rows<T>(S, c0, c0 + CHOL_NB, 4 * P, tid, nt, Ld, dinv);
+		// A. panel rows below the diagonal block
+		chol_panel_rows<T>(S, c0, c0 + CHOL_NB, 4 * P, tid, nt, Lt);
 		__syncthreads();
 		if (K + 1 >= NB) break;
-		// 2. look-ahead: tiles of block column K+1 (tj in [k0+4, k0+8), ti >= tj)
-		{
-			const int rows = P - (k0 + 4);
-			const int cols = min(4, P - (k0 + 4));
-			for (int t = tid; t < rows * cols; t += nt) {
-				const int tj = k0 + 4 + t % cols, ti = k0 + 4 + t / cols;
-				if (ti >= tj) chol_tile_update<T>(S, ti, tj, c0);
-			}
-		}
-		__syncthreads();
-		// 3. warp 0: diagonal block K+1 ; other warps: remaining trailing tiles
+		// B. trailing tiles (ti,tj), k0+4 <= tj <= ti < P; the first 10 (the
+		// diagonal block K+1) belong to warp 0, which then factors that block
+		const int R = P - (k0 + 4);
+		const int ntiles = R * (R + 1) / 2;
+		const int ndiag = ntiles < 10 ? ntiles : 10;
 		if (warp == 0) {
-			chol_diag_factor<T>(S, c0 + CHOL_NB, min(CHOL_NB, n - c0 - CHOL_NB), dinv, Ld, bad);
+			if (lane < ndiag) {
+				int ti, tj;
+				tri_index(lane, ti, tj);
+				chol_tile_update<T>(S, ti + k0 + 4, tj + k0 + 4, c0);
+			}
+			__syncwarp();
+			chol_diag_factor<T>(S, c0 + CHOL_NB, min(CHOL_NB, n - c0 - CHOL_NB), dinv, Lt, bad);
 		} else {
-			const int R = P - (k0 + 8);
-			if (R > 0) {
-				const int ntiles = R * (R + 1) / 2;
-				for (int t = tid - 32; t < ntiles; t += nt - 32) {
-					int ti, tj;
-					tri_index(t, ti, tj);
-					chol_tile_update<T>(S, ti + k0 + 8, tj + k0 + 8, c0);
-				}
+			for (int t = ndiag + tid - 32; t < ntiles; t += nt - 32) {
+				int ti, tj;
+				tri_index(t, ti, tj);
+				chol_tile_update<T>(S, ti + k0 + 4, tj + k0 + 4, c0);
 			}
 		}
 		__syncthreads();
 	}
 	if (invL_all) {
-		const int lane = tid & 31, nw = nt >> 5;
+		const int nw = nt >> 5;
 		for (int K = warp; K < NB; K += nw) chol_block_inverse<T>(S, n, K, dinv, invL_all + (size_t)K * 256, lane);
 		__syncthreads();
 	}

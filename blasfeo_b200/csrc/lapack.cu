@@ -41,8 +41,8 @@ __host__ __device__ inline PotrfSmem potrf_smem_plan(int max_n) {
 	p.s_bytes = align16((size_t)lp_size(max_n) * sizeof(T));
 	p.dinv_off = p.s_bytes;
 	p.invl_off = p.dinv_off + align16((size_t)4 * P * sizeof(double));
-	p.scratch_off = p.invl_off;
-	p.bad_off = p.scratch_off + align16(16 * 17 * sizeof(double));
+	p.scratch_off = p.invl_off + align16(16 * 17 * sizeof(T));
+	p.bad_off = p.scratch_off + align16((16 * 17 + 64) * sizeof(double));
 	p.total = p.bad_off + 16;
 	return p;
 }
@@ -90,6 +90,7 @@ __global__ void __launch_bounds__(NT, MINB) k_potrf_smem(SizeArg sz, MatArg<T> C
 	PotrfSmem pl = potrf_smem_plan<T>(max_n);
 	T *S = (T *)smem;
 	double *dinv = (double *)(smem + pl.dinv_off);
+	T *invL = (T *)(smem + pl.invl_off);
 	double *scratch = (double *)(smem + pl.scratch_off);
 	int *bad = (int *)(smem + pl.bad_off);
 	const PMat<T> c = C.get(b), d = D.get(b);
@@ -99,7 +100,7 @@ __global__ void __launch_bounds__(NT, MINB) k_potrf_smem(SizeArg sz, MatArg<T> C
 	else
 		load_lower_panels<T>(S, n, c);
 	__syncthreads();
-	chol_smem<T>(S, n, dinv, scratch, bad, (T *)nullptr);
+	chol_smem<T>(S, n, dinv, invL, bad, (T *)nullptr);
 	if ((d.ri & 3) == 0)
 		store_lp_vec<T, 4>(S, n, d.p + (size_t)d.ri * d.cn + 4 * d.cj, d.cn);
 	else

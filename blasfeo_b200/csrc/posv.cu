@@ -104,7 +104,7 @@ __host__ __device__ inline PosvPlan posv_plan(int max_n) {
 	p.inv_off = p.S_off + a16((size_t)lp_size(max_n) * sizeof(T));
 	p.dinv_off = p.inv_off + a16((size_t)(MIXED ? NB : 1) * 256 * sizeof(T));
 	p.scr_off = p.dinv_off + a16((size_t)4 * P * sizeof(double));
-	p.w_off = p.scr_off + a16(16 * 17 * sizeof(double));
+	p.w_off = p.scr_off + a16((16 * 17 + 64) * sizeof(double));
 	p.x_off = p.w_off + a16((size_t)nv * sizeof(T));
 	p.r_off = p.x_off + (MIXED ? a16((size_t)nv * sizeof(double)) : 0);
 	p.ybuf_off = p.r_off + (MIXED ? a16((size_t)nv * sizeof(double)) : 0);
@@ -370,7 +370,7 @@ __global__ void __launch_bounds__(NT, MINB) k_posv(int cls, int max_n, PosvWs ws
 		if (MIXED)
 			for (int i = tid; i < nv; i += nt) xs[i] = 0.0;
 		__syncthreads();
-		chol_smem<T>(S, n, dinv, scratch, s_bad, MIXED ? invL : (T *)nullptr);
+		chol_smem<T>(S, n, dinv, (T *)scratch, s_bad, MIXED ? invL : (T *)nullptr);
 
 		if (!MIXED) {
 			trsv_fwd<T>(S, n, nullptr, dinv, w, ybuf);
