@@ -265,6 +265,24 @@ int blasfeo_dsposv_l_vbatch_mapped(int batch, const int *n, int max_n, const str
 	const struct blasfeo_dvec *sb, const struct blasfeo_dvec *sx, int max_iter, double tol,
 	int *iters, double *berr, int *info, void *work, size_t work_bytes, void *stream);
 
+/* Allocation-free variant of blasfeo_dsposv_l_vbatch (no counterpart in the
+ * reference, which has no batched or GPU solver).  For callers that must not
+ * allocate device memory while they run (embedded and real-time solvers that
+ * fix their memory at start-up, or code that cannot afford the device-wide
+ * synchronisation of cudaMalloc) and that do not pass a workspace: the scratch
+ * is a static device array owned by the library (blasfeo_dsposv_noalloc_scratch_bytes()
+ * bytes, resident on every GPU that uses the library until the process exits).
+ * At most BLASFEO_B200_NOALLOC_MAX_BATCH systems per call and n <= 256, else
+ * BLASFEO_B200_ENOTSUP.  All calls share the array: calls that overlap on the
+ * GPU race and must be serialised by the caller.  The first call on a device
+ * looks up the array's device address and caches it; make that first call
+ * before any stream capture. */
+#define BLASFEO_B200_NOALLOC_MAX_BATCH 65536
+size_t blasfeo_dsposv_noalloc_scratch_bytes(void);
+int blasfeo_dsposv_l_vbatch_noalloc(int batch, const int *n, int max_n, const struct blasfeo_dmat *sA,
+	const struct blasfeo_dvec *sb, const struct blasfeo_dvec *sx, int max_iter, double tol,
+	int *iters, double *berr, int *info, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -1,0 +1,64 @@
+"""GPU test of blasfeo_dsposv_l_vbatch_noalloc, the allocation-free entry point.
+
+It exists for callers that cannot allocate device memory while they run
+(embedded / real-time solvers whose memory is fixed at start-up, code that
+cannot take cudaMalloc's device-wide synchronisation) and that pass no
+workspace: its scratch is a static device array owned by the library.  The
+test calls it through the C ABI twice in a row and checks both results
+against the allocating entry point on the same inputs.  The file name sorts
+last so that a run stopping at the first failure has run every other test."""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def _inputs(num, seed):
+    from blasfeo_b200.workloads import spd_config3
+    return spd_config3(num, seed=seed)
+
+
+def test_noalloc_matches_allocating_entry_point_twice():
+    import torch
+    import blasfeo_b200 as bf
+    lib = bf.lib
+    P = lambda t: C.c_void_p(t.data_ptr())
+    num = 300
+    W = _inputs(num, seed=11)
+    info = torch.full((num,), -9, dtype=torch.int32, device="cuda")
+    berr = torch.zeros(num, dtype=torch.float64, device="cuda")
+    st = lib.blasfeo_dsposv_l_vbatch(num, P(W.nvec), W.max_n, P(W.desc), P(W.bdesc), P(W.xdesc), 30, 1e-12, None,
+                                     P(berr), P(info), None, 0, None)
+    torch.cuda.synchronize()
+    assert st == 0 and (info.cpu().numpy() == 0).all()
+    x_ref = W.x.clone()
+    for call in range(2):
+        W.x.zero_()
+        info.fill_(-9)
+        berr.zero_()
+        st = lib.blasfeo_dsposv_l_vbatch_noalloc(num, P(W.nvec), W.max_n, P(W.desc), P(W.bdesc), P(W.xdesc), 30,
+                                                 1e-12, None, P(berr), P(info), None)
+        torch.cuda.synchronize()
+        assert st == 0, (call, st)
+        assert (info.cpu().numpy() == 0).all(), call
+        assert (berr.cpu().numpy() <= 1e-12).all(), call
+        diff = (W.x - x_ref).norm().item() / x_ref.norm().item()
+        assert diff <= 1e-12, (call, diff)
+    # spot check against the host: backward error of the largest system
+    i = int(np.argmax(W.ns))
+    a, b, x = W.matrix(i), W.rhs[i], W.solution(i)
+    assert np.abs(b - a @ x).max() / (np.abs(a).sum(1).max() * np.abs(x).max()) <= 1e-12
+
+
+def test_noalloc_rejects_oversize_requests():
+    import blasfeo_b200 as bf
+    lib = bf.lib
+    ENOTSUP = 4
+    big = 65536 + 1
+    assert lib.blasfeo_dsposv_l_vbatch_noalloc(big, None, 16, None, None, None, 30, 1e-12, None, None, None,
+                                               None) == ENOTSUP
+    assert lib.blasfeo_dsposv_l_vbatch_noalloc(10, None, 257, None, None, None, 30, 1e-12, None, None, None,
+                                               None) == ENOTSUP
+    assert lib.blasfeo_dsposv_noalloc_scratch_bytes() == 65536 * 4 + 4 * 48
