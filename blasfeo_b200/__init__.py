@@ -141,6 +141,7 @@ _sig("blasfeo_dposv_worksize", _sz, _i)
 _sig("blasfeo_dposv_l_vbatch", _i, _i, _vp, _i, _vp, _vp, _vp, _vp, _vp, _sz, _vp)
 _sig("blasfeo_dsposv_l_vbatch", _i, _i, _vp, _i, _vp, _vp, _vp, _i, _d, _vp, _vp, _vp, _vp, _sz, _vp)
 _sig("blasfeo_dsposv_l_vbatch_mapped", _i, _i, _vp, _i, _vp, _vp, _vp, _i, _d, _vp, _vp, _vp, _vp, _sz, _vp)
+_sig("blasfeo_dsyrk_dpotrf_dtrsm_dgemm_batch", _i, _i, _i, _i, _d, _DB, _DB, _DB, _DB, _DB, _DB, _DB, _vp, _vp)
 _sig("blasfeo_dsposv_noalloc_scratch_bytes", _sz)
 _sig("blasfeo_dsposv_l_vbatch_noalloc", _i, _i, _vp, _i, _vp, _vp, _vp, _i, _d, _vp, _vp, _vp, _vp)
 

@@ -256,6 +256,19 @@ int blasfeo_dsposv_l_vbatch(int batch, const int *n, int max_n, const struct bla
 	const struct blasfeo_dvec *sb, const struct blasfeo_dvec *sx, int max_iter, double tol,
 	int *iters, double *berr, int *info, void *work, size_t work_bytes, void *stream);
 
+/* Fused per-instance chain on a uniform batch (m = 16, 1 <= k <= 64; all
+ * slabs from blasfeo_create_dmat_batch, zero offsets), replacing the sequence
+ * blasfeo_dsyrk_ln (d_blas3_lib4.c:5400) + blasfeo_ddiare + blasfeo_dpotrf_l
+ * (d_lapack_lib4.c:918) + blasfeo_dtrsm_rltn (d_blas3_lib4.c:4123) +
+ * blasfeo_dgemm_nt (d_blas3_lib4.c:727):
+ *   S = A A^T + shift*I,  L = chol(S) (lower, inverse diagonal in L's dA),
+ *   X = R L^{-T},  D = C - X G^T.
+ * One launch; info[b] as for dpotrf_l (-3: a bulk copy timed out). */
+int blasfeo_dsyrk_dpotrf_dtrsm_dgemm_batch(int batch, int m, int k, double shift, struct blasfeo_dmat_batch *sA,
+	struct blasfeo_dmat_batch *sR, struct blasfeo_dmat_batch *sC, struct blasfeo_dmat_batch *sG,
+	struct blasfeo_dmat_batch *sL, struct blasfeo_dmat_batch *sX, struct blasfeo_dmat_batch *sD, int *info,
+	void *stream);
+
 /* Same as blasfeo_dsposv_l_vbatch, for callers whose matrices, vectors, sizes
  * and descriptors live in mapped (cudaHostAlloc / cudaHostRegister) host
  * memory: the kernels read the lower triangles straight over the host link
