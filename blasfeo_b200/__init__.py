@@ -142,6 +142,8 @@ _sig("blasfeo_dposv_l_vbatch", _i, _i, _vp, _i, _vp, _vp, _vp, _vp, _vp, _sz, _v
 _sig("blasfeo_dsposv_l_vbatch", _i, _i, _vp, _i, _vp, _vp, _vp, _i, _d, _vp, _vp, _vp, _vp, _sz, _vp)
 _sig("blasfeo_dsposv_l_vbatch_mapped", _i, _i, _vp, _i, _vp, _vp, _vp, _i, _d, _vp, _vp, _vp, _vp, _sz, _vp)
 _sig("blasfeo_dsyrk_dpotrf_dtrsm_dgemm_batch", _i, _i, _i, _i, _d, _DB, _DB, _DB, _DB, _DB, _DB, _DB, _vp, _vp)
+_sig("blasfeo_dric_trf_batch", _i, _i, _i, _i, _i, _DB, _DB, _DB, _vp, _vp)
+_sig("blasfeo_sric_trf_batch", _i, _i, _i, _i, _i, _SB, _SB, _SB, _vp, _vp)
 _sig("blasfeo_dsposv_noalloc_scratch_bytes", _sz)
 _sig("blasfeo_dsposv_l_vbatch_noalloc", _i, _i, _vp, _i, _vp, _vp, _vp, _i, _d, _vp, _vp, _vp, _vp)
 

@@ -269,6 +269,21 @@ int blasfeo_dsyrk_dpotrf_dtrsm_dgemm_batch(int batch, int m, int k, double shift
 	struct blasfeo_dmat_batch *sL, struct blasfeo_dmat_batch *sX, struct blasfeo_dmat_batch *sD, int *info,
 	void *stream);
 
+/* Batched Riccati factorization (LQR backward pass), the recursion of
+ * examples/example_d_riccati_recursion.c:115-143 (blasfeo_dpotrf_l, then per
+ * stage blasfeo_dtrmm_rlnn + blasfeo_dsyrk_dpotrf_ln) for `batch` independent
+ * problems with horizon N, nx states, nu inputs, nu + nx <= 16, in one launch.
+ * Slabs (zero offsets): sBAbt batch*N instances of 16 x nx (problem b, stage k
+ * at b*N + k; rows 0..nu-1 = B_k^T, rows nu.. = A_k^T), sRSQ and sL
+ * batch*(N+1) instances of 16 x 16 (problem b, stage k at b*(N+1) + k; stage N
+ * holds Q_N / L_N in its top-left nx x nx block).  Outputs: L_k (lower
+ * triangle) and its inverse diagonal in sL's dA; info[b] = 16*(N-k) + j + 1
+ * for the first non-positive pivot j of stage k, -3 on a copy timeout. */
+int blasfeo_dric_trf_batch(int batch, int N, int nx, int nu, struct blasfeo_dmat_batch *sBAbt,
+	struct blasfeo_dmat_batch *sRSQ, struct blasfeo_dmat_batch *sL, int *info, void *stream);
+int blasfeo_sric_trf_batch(int batch, int N, int nx, int nu, struct blasfeo_smat_batch *sBAbt,
+	struct blasfeo_smat_batch *sRSQ, struct blasfeo_smat_batch *sL, int *info, void *stream);
+
 /* Same as blasfeo_dsposv_l_vbatch, for callers whose matrices, vectors, sizes
  * and descriptors live in mapped (cudaHostAlloc / cudaHostRegister) host
  * memory: the kernels read the lower triangles straight over the host link
