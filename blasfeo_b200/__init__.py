@@ -137,6 +137,11 @@ _sig("blasfeo_dgemm_nt_vbatch", _i, _i, _vp, _vp, _vp, _i, _i, _i, _d, _vp, _vp,
 _sig("blasfeo_dpotrf_l_vbatch", _i, _i, _vp, _i, _vp, _vp, _vp, _vp)
 _sig("blasfeo_dgetrf_rp_vbatch", _i, _i, _vp, _vp, _i, _i, _vp, _vp, _vp, _i, _vp, _vp)
 _sig("blasfeo_dgeqrf_vbatch", _i, _i, _vp, _vp, _i, _i, _vp, _vp, _vp)
+_sig("blasfeo_b200_num_variants", _i, _i)
+_sig("blasfeo_dgemm_nt_vbatch_variant", _i, _i, _vp, _vp, _vp, _i, _i, _i, _d, _vp, _vp, _d, _vp, _vp, _i, _vp)
+_sig("blasfeo_dpotrf_l_vbatch_variant", _i, _i, _vp, _i, _vp, _vp, _vp, _i, _vp)
+_sig("blasfeo_dgetrf_rp_vbatch_variant", _i, _i, _vp, _vp, _i, _i, _vp, _vp, _vp, _i, _vp, _i, _vp)
+_sig("blasfeo_dgeqrf_vbatch_variant", _i, _i, _vp, _vp, _i, _i, _vp, _vp, _i, _vp)
 _sig("blasfeo_dposv_worksize", _sz, _i)
 _sig("blasfeo_dposv_l_vbatch", _i, _i, _vp, _i, _vp, _vp, _vp, _vp, _vp, _sz, _vp)
 _sig("blasfeo_dsposv_l_vbatch", _i, _i, _vp, _i, _vp, _vp, _vp, _i, _d, _vp, _vp, _vp, _vp, _sz, _vp)
@@ -144,6 +149,11 @@ _sig("blasfeo_dsposv_l_vbatch_mapped", _i, _i, _vp, _i, _vp, _vp, _vp, _i, _d, _
 _sig("blasfeo_dsyrk_dpotrf_dtrsm_dgemm_batch", _i, _i, _i, _i, _d, _DB, _DB, _DB, _DB, _DB, _DB, _DB, _vp, _vp)
 _sig("blasfeo_dric_trf_batch", _i, _i, _i, _i, _i, _DB, _DB, _DB, _vp, _vp)
 _sig("blasfeo_sric_trf_batch", _i, _i, _i, _i, _i, _SB, _SB, _SB, _vp, _vp)
+_sig("blasfeo_b200_mlp_param_count", _i, _i, _i)
+_sig("blasfeo_b200_mlp_work_bytes", _sz, _i, _i)
+_sig("blasfeo_b200_mlp_forward", _i, _i, _i, _vp, _i, _vp, _vp, _vp, _vp)
+_sig("blasfeo_b200_mlp_grad", _i, _i, _i, _vp, _i, _vp, _vp, _vp, _vp, _vp, _vp)
+_sig("blasfeo_b200_mlp_adam", _i, _i, _vp, _vp, _vp, _vp, _i, _f, _vp)
 _sig("blasfeo_dsposv_noalloc_scratch_bytes", _sz)
 _sig("blasfeo_dsposv_l_vbatch_noalloc", _i, _i, _vp, _i, _vp, _vp, _vp, _i, _d, _vp, _vp, _vp, _vp)
 

@@ -383,13 +383,33 @@ int blasfeo_strsm_rltn_batch(int batch, int m, int n, float alpha, struct blasfe
 	return trsm_batch<float>(batch, m, n, alpha, sA, ai, aj, sB, bi, bj, sD, di, dj, stream);
 }
 
+int blasfeo_dgemm_nt_vbatch_variant(int batch, const int *m, const int *n, const int *k, int max_m, int max_n,
+                                    int max_k, double alpha, const struct blasfeo_dmat *sA, const struct blasfeo_dmat *sB,
+                                    double beta, const struct blasfeo_dmat *sC, const struct blasfeo_dmat *sD,
+                                    int variant, void *stream) {
+	if (batch < 0 || !m || !n || !k || !sA || !sB || !sC || !sD) return BLASFEO_B200_EINVAL;
+	if (variant > 3) return BLASFEO_B200_EINVAL;
+	return bf::gemm_nt_launch<double, false>(batch, var_sizes(m, n, k), max_m, max_n, max_k, alpha,
+	                                         vbatch_arg<double>(sA), vbatch_arg<double>(sB), beta,
+	                                         vbatch_arg<double>(sC), vbatch_arg<double>(sD), (cudaStream_t)stream,
+	                                         variant);
+}
 int blasfeo_dgemm_nt_vbatch(int batch, const int *m, const int *n, const int *k, int max_m, int max_n, int max_k,
                             double alpha, const struct blasfeo_dmat *sA, const struct blasfeo_dmat *sB, double beta,
                             const struct blasfeo_dmat *sC, const struct blasfeo_dmat *sD, void *stream) {
-	if (batch < 0 || !m || !n || !k || !sA || !sB || !sC || !sD) return BLASFEO_B200_EINVAL;
-	return bf::gemm_nt_launch<double, false>(batch, var_sizes(m, n, k), max_m, max_n, max_k, alpha,
-	                                         vbatch_arg<double>(sA), vbatch_arg<double>(sB), beta,
-	                                         vbatch_arg<double>(sC), vbatch_arg<double>(sD), (cudaStream_t)stream, -1);
+	return blasfeo_dgemm_nt_vbatch_variant(batch, m, n, k, max_m, max_n, max_k, alpha, sA, sB, beta, sC, sD, -1,
+	                                       stream);
+}
+
+/* number of kernel variants of a routine: op 0 gemm_nt, 1 potrf_l, 2 getrf_rp, 3 geqrf */
+int blasfeo_b200_num_variants(int op) {
+	switch (op) {
+	case 0: return 4;
+	case 1: return 5;
+	case 2: return 6;
+	case 3: return 6;
+	default: return 0;
+	}
 }
 
 }  // extern "C"

@@ -11,6 +11,7 @@ int gemm_nt_launch(int batch, SizeArg sz, int max_m, int max_n, int max_k, T alp
 
 // D = chol(C) lower, inverse diagonal into D's dA, info (device, may be null)
 template <typename T>
-int potrf_launch(int batch, SizeArg sz, int max_m, MatArg<T> C, MatArg<T> D, int *info, cudaStream_t s);
+int potrf_launch(int batch, SizeArg sz, int max_m, MatArg<T> C, MatArg<T> D, int *info, cudaStream_t s,
+                 int variant);
 
 }  // namespace bf

@@ -81,12 +81,14 @@ __device__ void store_lower_panels(const T *S, int n, const PMat<T> &d) {
 	}
 }
 
+// Instances with n <= max_n are factored here; larger ones of a
+// variable-size batch are left to the global-memory kernel.
 template <typename T, int NT, int MINB>
 __global__ void __launch_bounds__(NT, MINB) k_potrf_smem(SizeArg sz, MatArg<T> C, MatArg<T> D, int *info, int max_n) {
 	extern __shared__ __align__(16) unsigned char smem[];
 	const int b = blockIdx.x;
 	const int n = sz.M(b);
-	if (n <= 0) return;
+	if (n <= 0 || n > max_n) return;
 	PotrfSmem pl = potrf_smem_plan<T>(max_n);
 	T *S = (T *)smem;
 	double *dinv = (double *)(smem + pl.dinv_off);
@@ -111,12 +113,12 @@ __global__ void __launch_bounds__(NT, MINB) k_potrf_smem(SizeArg sz, MatArg<T> C
 
 // unblocked right-looking Cholesky in global memory (any size)
 template <typename T>
-__global__ void __launch_bounds__(256) k_potrf_global(SizeArg sz, MatArg<T> C, MatArg<T> D, int *info) {
+__global__ void __launch_bounds__(256) k_potrf_global(SizeArg sz, MatArg<T> C, MatArg<T> D, int *info, int min_n) {
 	__shared__ double s_inv;
 	__shared__ int s_bad;
 	const int b = blockIdx.x;
 	const int n = sz.M(b);
-	if (n <= 0) return;
+	if (n <= 0 || n <= min_n) return;
 	const PMat<T> c = C.get(b), d = D.get(b);
 	const int tid = threadIdx.x, nt = blockDim.x;
 	const int warp = tid >> 5, lane = tid & 31, nw = nt >> 5;
@@ -181,19 +183,33 @@ __device__ int block_argmax_first(T v, int idx, int *s_idx, T *s_val) {
 	return r;
 }
 
-template <typename T>
-__global__ void __launch_bounds__(256) k_getrf_global(SizeArg sz, MatArg<T> C, MatArg<T> D, int *ipiv,
-                                                       long long ipiv_stride, int *info) {
+// LU with row pivoting of one instance per CTA.  SMEM: the instance's m x n
+// block is copied into shared memory (panel-major), factored there and
+// copied back; only instances whose block fits in smem_cap bytes are taken.
+// Global: factored in place in D; with smem_cap >= 0 only the instances that
+// do not fit are taken (the other kernel of the launch has the rest).
+template <typename T, int NT, bool SMEM>
+__global__ void __launch_bounds__(NT) k_getrf(SizeArg sz, MatArg<T> C, MatArg<T> D, int *ipiv, long long ipiv_stride,
+                                               int *info, int smem_cap) {
+	extern __shared__ __align__(16) unsigned char smem_raw[];
 	__shared__ int s_idx[33];
 	__shared__ T s_val[32];
 	__shared__ int s_bad;
 	const int b = blockIdx.x;
 	const int m = sz.M(b), n = sz.N(b);
 	if (m <= 0 || n <= 0) return;
-	const PMat<T> c = C.get(b), d = D.get(b);
-	const int tid = threadIdx.x, nt = blockDim.x;
+	const bool fits = (size_t)((m + 3) / 4 * 4) * ((n + 3) / 4 * 4) * sizeof(T) <= (size_t)(smem_cap < 0 ? 0 : smem_cap);
+	if (SMEM ? !fits : (smem_cap >= 0 && fits)) return;
+	const PMat<T> c = C.get(b), dg = D.get(b);
+	PMat<T> d = dg;
+	if (SMEM) {
+		d.p = (T *)smem_raw;
+		d.cn = (n + 3) / 4 * 4;
+		d.ri = d.cj = 0;
+	}
+	const int tid = threadIdx.x;
 	int *piv = ipiv + ipiv_stride * b;
-	const int warp = tid >> 5, lane = tid & 31, nw = nt >> 5;
+	const int warp = tid >> 5, lane = tid & 31, nw = NT >> 5;
 	for (int j = warp; j < n; j += nw)
 		for (int i = lane; i < m; i += 32) d.at(i, j) = c.at(i, j);
 	if (tid == 0) s_bad = 0;
@@ -203,7 +219,7 @@ __global__ void __launch_bounds__(256) k_getrf_global(SizeArg sz, MatArg<T> C, M
 		// pivot search over rows j..m-1
 		T best = T(-1);
 		int bi = INT_MAX;
-		for (int i = j + tid; i < m; i += nt) {
+		for (int i = j + tid; i < m; i += NT) {
 			T a = dev_abs(d.at(i, j));
 			if (a > best) {
 				best = a;
@@ -212,7 +228,7 @@ __global__ void __launch_bounds__(256) k_getrf_global(SizeArg sz, MatArg<T> C, M
 		}
 		const int ip = block_argmax_first<T>(best, bi, s_idx, s_val);
 		if (ip != j)
-			for (int l = tid; l < n; l += nt) {
+			for (int l = tid; l < n; l += NT) {
 				T t = d.at(j, l);
 				d.at(j, l) = d.at(ip, l);
 				d.at(ip, l) = t;
@@ -222,16 +238,20 @@ __global__ void __launch_bounds__(256) k_getrf_global(SizeArg sz, MatArg<T> C, M
 		const T inv = (p != T(0)) ? T(1) / p : T(0);
 		if (tid == 0) {
 			piv[j] = ip;
-			d.d[j] = inv;
+			dg.d[j] = inv;
 			if (p == T(0) && s_bad == 0) s_bad = j + 1;
 		}
-		for (int i = j + 1 + tid; i < m; i += nt) d.at(i, j) *= inv;
+		for (int i = j + 1 + tid; i < m; i += NT) d.at(i, j) *= inv;
 		__syncthreads();
 		for (int l = j + 1 + warp; l < n; l += nw) {
 			const T ujl = d.at(j, l);
 			for (int i = j + 1 + lane; i < m; i += 32) d.at(i, l) = fma(-d.at(i, j), ujl, d.at(i, l));
 		}
 		__syncthreads();
+	}
+	if (SMEM) {
+		for (int j = warp; j < n; j += nw)
+			for (int i = lane; i < m; i += 32) dg.at(i, j) = d.at(i, j);
 	}
 	if (info && tid == 0) info[b] = s_bad;
 }
@@ -254,26 +274,34 @@ __device__ T block_sum(T v, T *s_red) {
 	return r;
 }
 
-template <typename T>
-__global__ void __launch_bounds__(256) k_geqrf_global(SizeArg sz, MatArg<T> C, MatArg<T> D) {
+// Householder QR of one instance per CTA (shared or global memory, as k_getrf).
+template <typename T, int NT, bool SMEM>
+__global__ void __launch_bounds__(NT) k_geqrf(SizeArg sz, MatArg<T> C, MatArg<T> D, int smem_cap) {
+	extern __shared__ __align__(16) unsigned char smem_raw[];
 	__shared__ T s_red[33];
 	__shared__ T s_tau, s_sc, s_beta;
 	const int b = blockIdx.x;
 	const int m = sz.M(b), n = sz.N(b);
 	if (m <= 0 || n <= 0) return;
-	const PMat<T> c = C.get(b), d = D.get(b);
-	T *tau = d.d + d.ri;
-	const int tid = threadIdx.x, nt = blockDim.x;
-	{
-		const int warp = tid >> 5, lane = tid & 31, nw = nt >> 5;
-		for (int j = warp; j < n; j += nw)
-			for (int i = lane; i < m; i += 32) d.at(i, j) = c.at(i, j);
+	const bool fits = (size_t)((m + 3) / 4 * 4) * ((n + 3) / 4 * 4) * sizeof(T) <= (size_t)(smem_cap < 0 ? 0 : smem_cap);
+	if (SMEM ? !fits : (smem_cap >= 0 && fits)) return;
+	const PMat<T> c = C.get(b), dg = D.get(b);
+	PMat<T> d = dg;
+	if (SMEM) {
+		d.p = (T *)smem_raw;
+		d.cn = (n + 3) / 4 * 4;
+		d.ri = d.cj = 0;
 	}
+	T *tau = dg.d + dg.ri;
+	const int tid = threadIdx.x;
+	const int warp = tid >> 5, lane = tid & 31, nw = NT >> 5;
+	for (int j = warp; j < n; j += nw)
+		for (int i = lane; i < m; i += 32) d.at(i, j) = c.at(i, j);
 	__syncthreads();
 	const int kmax = m < n ? m : n;
 	for (int j = 0; j < kmax; j++) {
 		T part = T(0);
-		for (int i = j + 1 + tid; i < m; i += nt) {
+		for (int i = j + 1 + tid; i < m; i += NT) {
 			T x = d.at(i, j);
 			part = fma(x, x, part);
 		}
@@ -296,18 +324,26 @@ __global__ void __launch_bounds__(256) k_geqrf_global(SizeArg sz, MatArg<T> C, M
 		__syncthreads();
 		const T t = s_tau;
 		if (s != T(0)) {
-			for (int i = j + 1 + tid; i < m; i += nt) d.at(i, j) *= s_sc;
+			for (int i = j + 1 + tid; i < m; i += NT) d.at(i, j) *= s_sc;
 			if (tid == 0) d.at(j, j) = s_beta;
 		}
 		__syncthreads();
-		for (int col = j + 1 + tid; col < n; col += nt) {
-			T w = d.at(j, col);
-			for (int i = j + 1; i < m; i++) w = fma(d.at(i, j), d.at(i, col), w);
-			w = -t * w;
-			d.at(j, col) += w;
-			for (int i = j + 1; i < m; i++) d.at(i, col) = fma(w, d.at(i, j), d.at(i, col));
+		// apply the reflector: one warp per trailing column, lanes over rows
+		for (int col = j + 1 + warp; col < n; col += nw) {
+			T w = T(0);
+			for (int i = j + 1 + lane; i < m; i += 32) w = fma(d.at(i, j), d.at(i, col), w);
+#pragma unroll
+			for (int off = 16; off > 0; off >>= 1) w += __shfl_xor_sync(0xffffffffu, w, off);
+			w = -t * (w + d.at(j, col));
+			for (int i = j + 1 + lane; i < m; i += 32) d.at(i, col) = fma(w, d.at(i, j), d.at(i, col));
+			__syncwarp();
+			if (lane == 0) d.at(j, col) += w;
 		}
 		__syncthreads();
+	}
+	if (SMEM) {
+		for (int j = warp; j < n; j += nw)
+			for (int i = lane; i < m; i += 32) dg.at(i, j) = d.at(i, j);
 	}
 }
 
@@ -325,24 +361,32 @@ void launch_potrf_smem(int batch, SizeArg sz, int max_m, size_t smem, MatArg<T> 
 
 namespace bf {
 
+// variant: -1 auto; 0..3: shared memory with 64/128/256/512 threads for the
+// instances that fit (the others in global memory, a second launch);
+// 4: everything in global memory.
 template <typename T>
-int potrf_launch(int batch, SizeArg sz, int max_m, MatArg<T> C, MatArg<T> D, int *info, cudaStream_t s) {
+int potrf_launch(int batch, SizeArg sz, int max_m, MatArg<T> C, MatArg<T> D, int *info, cudaStream_t s, int variant) {
 	if (batch <= 0 || max_m <= 0) return BLASFEO_B200_OK;
-	PotrfSmem pl = potrf_smem_plan<T>(max_m);
-	if (pl.total <= max_smem_optin()) {
-		if (max_m <= 64)
-			launch_potrf_smem<T, 64, 8>(batch, sz, max_m, pl.total, C, D, info, s);
-		else if (max_m <= 128)
-			launch_potrf_smem<T, 128, 4>(batch, sz, max_m, pl.total, C, D, info, s);
-		else
-			launch_potrf_smem<T, 512, 1>(batch, sz, max_m, pl.total, C, D, info, s);
-	} else {
-		k_potrf_global<T><<<batch, 256, 0, s>>>(sz, C, D, info);
+	static int limit_cache[2] = {0, 0};
+	int &lim = limit_cache[sizeof(T) == 8];
+	if (!lim)
+		for (int v = 4; v <= 1024; v += 4)
+			if (potrf_smem_plan<T>(v).total <= max_smem_optin()) lim = v;
+	const int smax = max_m < lim ? max_m : lim;
+	PotrfSmem pl = potrf_smem_plan<T>(smax);
+	if (variant < 0) variant = smax <= 64 ? 0 : (smax <= 128 ? 1 : 3);
+	switch (variant) {
+	case 0: launch_potrf_smem<T, 64, 8>(batch, sz, smax, pl.total, C, D, info, s); break;
+	case 1: launch_potrf_smem<T, 128, 4>(batch, sz, smax, pl.total, C, D, info, s); break;
+	case 2: launch_potrf_smem<T, 256, 2>(batch, sz, smax, pl.total, C, D, info, s); break;
+	case 3: launch_potrf_smem<T, 512, 1>(batch, sz, smax, pl.total, C, D, info, s); break;
+	default: break;
 	}
+	if (variant >= 4 || max_m > smax) k_potrf_global<T><<<batch, 256, 0, s>>>(sz, C, D, info, variant >= 4 ? 0 : smax);
 	return check_launch();
 }
-template int potrf_launch<double>(int, SizeArg, int, MatArg<double>, MatArg<double>, int *, cudaStream_t);
-template int potrf_launch<float>(int, SizeArg, int, MatArg<float>, MatArg<float>, int *, cudaStream_t);
+template int potrf_launch<double>(int, SizeArg, int, MatArg<double>, MatArg<double>, int *, cudaStream_t, int);
+template int potrf_launch<float>(int, SizeArg, int, MatArg<float>, MatArg<float>, int *, cudaStream_t, int);
 
 }  // namespace bf
 
@@ -353,7 +397,7 @@ void potrf_single(int m, S *sC, int ci, int cj, S *sD, int di, int dj) {
 	if (m <= 0) return;
 	sD->use_dA = (di == 0 && dj == 0) ? m : 0;
 	bf::potrf_launch<T>(1, uniform_sizes(m, m, 0), m, single_arg<T>(sC, ci, cj), single_arg<T>(sD, di, dj), nullptr,
-	                    bf::cur_stream());
+	                    bf::cur_stream(), -1);
 	bf::finish_single();
 }
 
@@ -363,7 +407,7 @@ int potrf_batch(int batch, int m, BT *sC, int ci, int cj, BT *sD, int di, int dj
 	if (m <= 0 || batch == 0) return BLASFEO_B200_OK;
 	sD->use_dA = (di == 0 && dj == 0) ? m : 0;
 	return bf::potrf_launch<T>(batch, uniform_sizes(m, m, 0), m, batch_arg<T>(sC, ci, cj), batch_arg<T>(sD, di, dj),
-	                           info, (cudaStream_t)stream);
+	                           info, (cudaStream_t)stream, -1);
 }
 
 template <typename T, typename S>
@@ -375,7 +419,7 @@ void syrk_potrf_single(int m, int k, S *sA, int ai, int aj, S *sB, int bi, int b
 	bf::gemm_nt_launch<T, true>(1, uniform_sizes(m, m, k), m, m, k, T(1), single_arg<T>(sA, ai, aj),
 	                            single_arg<T>(sB, bi, bj), T(1), single_arg<T>(sC, ci, cj), D, s, -1);
 	sD->use_dA = (di == 0 && dj == 0) ? m : 0;
-	bf::potrf_launch<T>(1, uniform_sizes(m, m, 0), m, D, D, nullptr, s);
+	bf::potrf_launch<T>(1, uniform_sizes(m, m, 0), m, D, D, nullptr, s, -1);
 	bf::finish_single();
 }
 
@@ -390,13 +434,75 @@ int syrk_potrf_batch(int batch, int m, int k, BT *sA, int ai, int aj, BT *sB, in
 	                                     batch_arg<T>(sB, bi, bj), T(1), batch_arg<T>(sC, ci, cj), D, s, -1);
 	if (st) return st;
 	sD->use_dA = (di == 0 && dj == 0) ? m : 0;
-	return bf::potrf_launch<T>(batch, uniform_sizes(m, m, 0), m, D, D, info, s);
+	return bf::potrf_launch<T>(batch, uniform_sizes(m, m, 0), m, D, D, info, s, -1);
+}
+
+// variant: -1 auto; 0..2: global memory only, 128/256/512 threads; 3..5: the
+// instances whose block fits in shared memory there (128/256/512 threads),
+// the others in global memory (a second launch, 512 threads).
+template <typename T, int NT, bool SMEM>
+void launch_getrf(int batch, SizeArg sz, int cap, size_t smem, MatArg<T> C, MatArg<T> D, int *ipiv,
+                  long long ipiv_stride, int *info, cudaStream_t s) {
+	auto kern = k_getrf<T, NT, SMEM>;
+	if (smem > 48 * 1024) cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+	kern<<<batch, NT, smem, s>>>(sz, C, D, ipiv, ipiv_stride, info, cap);
+}
+template <typename T, int NT, bool SMEM>
+void launch_geqrf(int batch, SizeArg sz, int cap, size_t smem, MatArg<T> C, MatArg<T> D, cudaStream_t s) {
+	auto kern = k_geqrf<T, NT, SMEM>;
+	if (smem > 48 * 1024) cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+	kern<<<batch, NT, smem, s>>>(sz, C, D, cap);
+}
+
+inline size_t lu_smem_bytes(int max_m, int max_n, size_t esz) {
+	return (size_t)((max_m + 3) / 4 * 4) * ((max_n + 3) / 4 * 4) * esz;
+}
+
+inline int pick_lu_variant(int variant, int max_m, int max_n) {
+	if (variant < 0) {
+		const int mx = max_m > max_n ? max_m : max_n;
+		variant = mx <= 64 ? 3 : (mx <= 160 ? 4 : 5);
+	}
+	return variant;
 }
 
 template <typename T>
 int getrf_launch(int batch, SizeArg sz, MatArg<T> C, MatArg<T> D, int *ipiv, long long ipiv_stride, int *info,
-                 cudaStream_t s) {
-	k_getrf_global<T><<<batch, 256, 0, s>>>(sz, C, D, ipiv, ipiv_stride, info);
+                 cudaStream_t s, int max_m, int max_n, int variant = -1) {
+	const size_t cap_full = bf::max_smem_optin() - 1024;
+	const size_t need = lu_smem_bytes(max_m, max_n, sizeof(T));
+	const size_t smem = need < cap_full ? need : cap_full;
+	const int cap = (int)smem;
+	variant = pick_lu_variant(variant, max_m, max_n);
+	switch (variant) {
+	case 0: launch_getrf<T, 128, false>(batch, sz, -1, 0, C, D, ipiv, ipiv_stride, info, s); break;
+	case 1: launch_getrf<T, 256, false>(batch, sz, -1, 0, C, D, ipiv, ipiv_stride, info, s); break;
+	case 2: launch_getrf<T, 512, false>(batch, sz, -1, 0, C, D, ipiv, ipiv_stride, info, s); break;
+	case 3: launch_getrf<T, 128, true>(batch, sz, cap, smem, C, D, ipiv, ipiv_stride, info, s); break;
+	case 4: launch_getrf<T, 256, true>(batch, sz, cap, smem, C, D, ipiv, ipiv_stride, info, s); break;
+	default: launch_getrf<T, 512, true>(batch, sz, cap, smem, C, D, ipiv, ipiv_stride, info, s); break;
+	}
+	if (variant >= 3 && need > smem) launch_getrf<T, 512, false>(batch, sz, cap, 0, C, D, ipiv, ipiv_stride, info, s);
+	return bf::check_launch();
+}
+
+template <typename T>
+int geqrf_launch(int batch, SizeArg sz, MatArg<T> C, MatArg<T> D, cudaStream_t s, int max_m, int max_n,
+                 int variant = -1) {
+	const size_t cap_full = bf::max_smem_optin() - 1024;
+	const size_t need = lu_smem_bytes(max_m, max_n, sizeof(T));
+	const size_t smem = need < cap_full ? need : cap_full;
+	const int cap = (int)smem;
+	variant = pick_lu_variant(variant, max_m, max_n);
+	switch (variant) {
+	case 0: launch_geqrf<T, 128, false>(batch, sz, -1, 0, C, D, s); break;
+	case 1: launch_geqrf<T, 256, false>(batch, sz, -1, 0, C, D, s); break;
+	case 2: launch_geqrf<T, 512, false>(batch, sz, -1, 0, C, D, s); break;
+	case 3: launch_geqrf<T, 128, true>(batch, sz, cap, smem, C, D, s); break;
+	case 4: launch_geqrf<T, 256, true>(batch, sz, cap, smem, C, D, s); break;
+	default: launch_geqrf<T, 512, true>(batch, sz, cap, smem, C, D, s); break;
+	}
+	if (variant >= 3 && need > smem) launch_geqrf<T, 512, false>(batch, sz, cap, 0, C, D, s);
 	return bf::check_launch();
 }
 
@@ -415,7 +521,8 @@ void getrf_single(int m, int n, S *sC, int ci, int cj, S *sD, int di, int dj, in
 		bf::set_error(BLASFEO_B200_ENOMEM);
 		return;
 	}
-	getrf_launch<T>(1, uniform_sizes(m, n, 0), single_arg<T>(sC, ci, cj), single_arg<T>(sD, di, dj), dpiv, 0, nullptr, s);
+	getrf_launch<T>(1, uniform_sizes(m, n, 0), single_arg<T>(sC, ci, cj), single_arg<T>(sD, di, dj), dpiv, 0, nullptr, s,
+	                m, n);
 	if (bf::check_launch() != BLASFEO_B200_OK) return;
 	// the pivot vector is a host array in the reference API: always complete the copy
 	if (cudaMemcpyAsync(ipiv, dpiv, mn * sizeof(int), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
@@ -431,15 +538,15 @@ int getrf_batch(int batch, int m, int n, BT *sC, int ci, int cj, BT *sD, int di,
 	sD->use_dA = (di == 0 && dj == 0) ? 1 : 0;
 	int mn = m < n ? m : n;
 	return getrf_launch<T>(batch, uniform_sizes(m, n, 0), batch_arg<T>(sC, ci, cj), batch_arg<T>(sD, di, dj), ipiv, mn,
-	                       info, (cudaStream_t)stream);
+	                       info, (cudaStream_t)stream, m, n);
 }
 
 template <typename T, typename S>
 void geqrf_single(int m, int n, S *sC, int ci, int cj, S *sD, int di, int dj) {
 	if (m <= 0 || n <= 0) return;
 	sD->use_dA = 0;
-	k_geqrf_global<T><<<1, 256, 0, bf::cur_stream()>>>(uniform_sizes(m, n, 0), single_arg<T>(sC, ci, cj),
-	                                                   single_arg<T>(sD, di, dj));
+	geqrf_launch<T>(1, uniform_sizes(m, n, 0), single_arg<T>(sC, ci, cj), single_arg<T>(sD, di, dj), bf::cur_stream(), m,
+	                n);
 	bf::finish_single();
 }
 
@@ -448,9 +555,8 @@ int geqrf_batch(int batch, int m, int n, BT *sC, int ci, int cj, BT *sD, int di,
 	if (batch < 0 || !sC || !sD) return BLASFEO_B200_EINVAL;
 	if (m <= 0 || n <= 0 || batch == 0) return BLASFEO_B200_OK;
 	sD->use_dA = 0;
-	k_geqrf_global<T><<<batch, 256, 0, (cudaStream_t)stream>>>(uniform_sizes(m, n, 0), batch_arg<T>(sC, ci, cj),
-	                                                             batch_arg<T>(sD, di, dj));
-	return bf::check_launch();
+	return geqrf_launch<T>(batch, uniform_sizes(m, n, 0), batch_arg<T>(sC, ci, cj), batch_arg<T>(sD, di, dj),
+	                       (cudaStream_t)stream, m, n);
 }
 
 // geqrf work size of the HP reference (blasfeo_hp_pm/d_lapack_lib4.c:3433-3440)
@@ -535,31 +641,41 @@ int blasfeo_sgeqrf_batch(int batch, int m, int n, struct blasfeo_smat_batch *sC,
 	return geqrf_batch<float>(batch, m, n, sC, ci, cj, sD, di, dj, stream);
 }
 
+int blasfeo_dpotrf_l_vbatch_variant(int batch, const int *m, int max_m, const struct blasfeo_dmat *sC,
+                                    const struct blasfeo_dmat *sD, int *info, int variant, void *stream) {
+	if (batch < 0 || !m || !sC || !sD || max_m < 0 || variant > 4) return BLASFEO_B200_EINVAL;
+	if (batch == 0 || max_m == 0) return BLASFEO_B200_OK;
+	return bf::potrf_launch<double>(batch, var_sizes(m, m, nullptr), max_m, vbatch_arg<double>(sC),
+	                                vbatch_arg<double>(sD), info, (cudaStream_t)stream, variant);
+}
 int blasfeo_dpotrf_l_vbatch(int batch, const int *m, int max_m, const struct blasfeo_dmat *sC,
                             const struct blasfeo_dmat *sD, int *info, void *stream) {
-	if (batch < 0 || !m || !sC || !sD) return BLASFEO_B200_EINVAL;
-	return bf::potrf_launch<double>(batch, var_sizes(m, m, nullptr), max_m, vbatch_arg<double>(sC),
-	                                vbatch_arg<double>(sD), info, (cudaStream_t)stream);
+	return blasfeo_dpotrf_l_vbatch_variant(batch, m, max_m, sC, sD, info, -1, stream);
+}
+int blasfeo_dgetrf_rp_vbatch_variant(int batch, const int *m, const int *n, int max_m, int max_n,
+                                     const struct blasfeo_dmat *sC, const struct blasfeo_dmat *sD, int *ipiv,
+                                     int ipiv_stride, int *info, int variant, void *stream) {
+	if (batch < 0 || !m || !n || !sC || !sD || !ipiv || max_m < 0 || max_n < 0 || variant > 5) return BLASFEO_B200_EINVAL;
+	if (batch == 0 || max_m == 0 || max_n == 0) return BLASFEO_B200_OK;
+	return getrf_launch<double>(batch, var_sizes(m, n, nullptr), vbatch_arg<double>(sC), vbatch_arg<double>(sD), ipiv,
+	                            ipiv_stride, info, (cudaStream_t)stream, max_m, max_n, variant);
 }
 int blasfeo_dgetrf_rp_vbatch(int batch, const int *m, const int *n, int max_m, int max_n,
                              const struct blasfeo_dmat *sC, const struct blasfeo_dmat *sD, int *ipiv, int ipiv_stride,
                              int *info, void *stream) {
-	if (batch < 0 || !m || !n || !sC || !sD || !ipiv) return BLASFEO_B200_EINVAL;
-	(void)max_m;
-	(void)max_n;
-	if (batch == 0) return BLASFEO_B200_OK;
-	return getrf_launch<double>(batch, var_sizes(m, n, nullptr), vbatch_arg<double>(sC), vbatch_arg<double>(sD), ipiv,
-	                            ipiv_stride, info, (cudaStream_t)stream);
+	return blasfeo_dgetrf_rp_vbatch_variant(batch, m, n, max_m, max_n, sC, sD, ipiv, ipiv_stride, info, -1, stream);
+}
+int blasfeo_dgeqrf_vbatch_variant(int batch, const int *m, const int *n, int max_m, int max_n,
+                                  const struct blasfeo_dmat *sC, const struct blasfeo_dmat *sD, int variant,
+                                  void *stream) {
+	if (batch < 0 || !m || !n || !sC || !sD || max_m < 0 || max_n < 0 || variant > 5) return BLASFEO_B200_EINVAL;
+	if (batch == 0 || max_m == 0 || max_n == 0) return BLASFEO_B200_OK;
+	return geqrf_launch<double>(batch, var_sizes(m, n, nullptr), vbatch_arg<double>(sC), vbatch_arg<double>(sD),
+	                            (cudaStream_t)stream, max_m, max_n, variant);
 }
 int blasfeo_dgeqrf_vbatch(int batch, const int *m, const int *n, int max_m, int max_n, const struct blasfeo_dmat *sC,
                           const struct blasfeo_dmat *sD, void *stream) {
-	if (batch < 0 || !m || !n || !sC || !sD) return BLASFEO_B200_EINVAL;
-	(void)max_m;
-	(void)max_n;
-	if (batch == 0) return BLASFEO_B200_OK;
-	k_geqrf_global<double><<<batch, 256, 0, (cudaStream_t)stream>>>(var_sizes(m, n, nullptr), vbatch_arg<double>(sC),
-	                                                                 vbatch_arg<double>(sD));
-	return bf::check_launch();
+	return blasfeo_dgeqrf_vbatch_variant(batch, m, n, max_m, max_n, sC, sD, -1, stream);
 }
 
 }  // extern "C"

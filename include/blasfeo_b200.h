@@ -237,6 +237,24 @@ int blasfeo_dgetrf_rp_vbatch(int batch, const int *m, const int *n, int max_m, i
 int blasfeo_dgeqrf_vbatch(int batch, const int *m, const int *n, int max_m, int max_n,
 	const struct blasfeo_dmat *sC, const struct blasfeo_dmat *sD, void *stream);
 
+/* Kernel-variant selection for the variable-size batches (used by the
+ * autotuner and the learned cost model; variant -1 = built-in heuristic).
+ * op: 0 gemm_nt (4 tile shapes), 1 potrf_l (shared memory with 64/128/256/512
+ * threads, or global memory), 2 getrf_rp and 3 geqrf (global or shared
+ * memory, 128/256/512 threads each).  Variants only change speed, never the
+ * arithmetic of an element. */
+int blasfeo_b200_num_variants(int op);
+int blasfeo_dgemm_nt_vbatch_variant(int batch, const int *m, const int *n, const int *k, int max_m, int max_n, int max_k,
+	double alpha, const struct blasfeo_dmat *sA, const struct blasfeo_dmat *sB, double beta,
+	const struct blasfeo_dmat *sC, const struct blasfeo_dmat *sD, int variant, void *stream);
+int blasfeo_dpotrf_l_vbatch_variant(int batch, const int *m, int max_m, const struct blasfeo_dmat *sC,
+	const struct blasfeo_dmat *sD, int *info, int variant, void *stream);
+int blasfeo_dgetrf_rp_vbatch_variant(int batch, const int *m, const int *n, int max_m, int max_n,
+	const struct blasfeo_dmat *sC, const struct blasfeo_dmat *sD, int *ipiv, int ipiv_stride, int *info, int variant,
+	void *stream);
+int blasfeo_dgeqrf_vbatch_variant(int batch, const int *m, const int *n, int max_m, int max_n,
+	const struct blasfeo_dmat *sC, const struct blasfeo_dmat *sD, int variant, void *stream);
+
 /* ---- fused solvers (no reference counterpart; built from dpotrf_l + dtrsv_lnn + dtrsv_ltn) ----
  * Solve A x = b for a variable-size batch of SPD systems; A is read from the
  * lower triangle of each descriptor (full storage, upper part ignored).
@@ -292,6 +310,21 @@ int blasfeo_sric_trf_batch(int batch, int N, int nx, int nu, struct blasfeo_smat
 int blasfeo_dsposv_l_vbatch_mapped(int batch, const int *n, int max_n, const struct blasfeo_dmat *sA,
 	const struct blasfeo_dvec *sb, const struct blasfeo_dvec *sx, int max_iter, double tol,
 	int *iters, double *berr, int *info, void *work, size_t work_bytes, void *stream);
+
+/* Learned cost model kernels (no reference counterpart): an MLP
+ * nin -> hidden -> hidden -> hidden -> 1 (ReLU, FP32), parameters in one flat
+ * device array of blasfeo_b200_mlp_param_count(nin, hidden) floats (W1, b1,
+ * W2, b2, W3, b3, W4, b4; y = x W + b).  work: device buffer of
+ * blasfeo_b200_mlp_work_bytes(hidden, batch) bytes.  param_count returns -1
+ * for nin <= 0 or hidden <= 0. */
+int blasfeo_b200_mlp_param_count(int nin, int hidden);
+size_t blasfeo_b200_mlp_work_bytes(int hidden, int batch);
+int blasfeo_b200_mlp_forward(int nin, int hidden, const float *params, int batch, const float *X, float *y,
+	float *work, void *stream);
+int blasfeo_b200_mlp_grad(int nin, int hidden, const float *params, int batch, const float *X, const float *target,
+	float *grads, float *loss, float *work, void *stream);
+int blasfeo_b200_mlp_adam(int nparams, float *params, const float *grads, float *m, float *v, int step, float lr,
+	void *stream);
 
 /* Allocation-free variant of blasfeo_dsposv_l_vbatch (no counterpart in the
  * reference, which has no batched or GPU solver).  For callers that must not
