@@ -119,32 +119,58 @@ __device__ __forceinline__ void chol_pivot_rsqrt(double c, double &d, double &in
 
 // One column J of the 16x16 diagonal-block factorization; lane i holds row i
 // of the block in r[] (compile-time indices only, so r stays in registers).
-// The pivot is broadcast by a shuffle and every lane computes the reciprocal
-// square root itself; column J reaches the other rows by shuffles.
-template <int J>
+// The pivot is broadcast by a shuffle and every lane computes its reciprocal
+// square root in FP64 (T = float: FP32 entries and updates, FP64 pivots);
+// column J reaches the other rows by shuffles.  The pivot rule is applied
+// without branches so the compiler can overlap the column update with the
+// next pivot.  The terminal step records the first non-positive pivot
+// (c0 + j + 1) in *bad by one ballot over the rows.
+template <int J, typename T = double>
 struct DiagCol {
-	static __device__ __forceinline__ void run(double (&r)[CHOL_NB], int lane, int nbk, int c0, double *dinv,
-	                                           int *bad) {
-		const double cj = __shfl_sync(0xffffffffu, r[J], J);
-		double d, inv;
-		chol_pivot_rsqrt(cj, d, inv);
-		r[J] = (lane == J) ? d : r[J] * inv;
-		if (lane == J && J < nbk) {
-			dinv[c0 + J] = inv;
-			if (!(cj > 0.0) && *bad == 0) *bad = c0 + J + 1;
-		}
+	static __device__ __forceinline__ void run(T (&r)[CHOL_NB], int lane, int nbk, int c0, double *dinv, int *bad) {
+		const double cj = (double)__shfl_sync(0xffffffffu, r[J], J);
+		const bool ok = cj > 0.0;
+		const double inv = ok ? rsqrt(cj) : 0.0;
+		r[J] = (lane == J) ? (T)(ok ? cj * inv : 0.0) : r[J] * (T)inv;
+		if (lane == J && J < nbk) dinv[c0 + J] = inv;
 #pragma unroll
 		for (int l = J + 1; l < CHOL_NB; l++) {
-			const double t = __shfl_sync(0xffffffffu, r[J], l);
+			const T t = __shfl_sync(0xffffffffu, r[J], l);
 			if (lane >= l) r[l] = fma(-r[J], t, r[l]);
 		}
-		DiagCol<J + 1>::run(r, lane, nbk, c0, dinv, bad);
+		DiagCol<J + 1, T>::run(r, lane, nbk, c0, dinv, bad);
 	}
 };
-template <>
-struct DiagCol<CHOL_NB> {
-	static __device__ __forceinline__ void run(double (&)[CHOL_NB], int, int, int, double *, int *) {}
+template <typename T>
+struct DiagCol<CHOL_NB, T> {
+	static __device__ __forceinline__ void run(T (&r)[CHOL_NB], int lane, int nbk, int c0, double *, int *bad) {
+		T d = T(1);
+#pragma unroll
+		for (int l = 0; l < CHOL_NB; l++)
+			if (l == lane) d = r[l];
+		const unsigned m = __ballot_sync(0xffffffffu, lane < nbk && !(d > T(0)));
+		if (m && lane == 0 && *bad == 0) *bad = c0 + __ffs(m);
+	}
 };
+
+// Write the factored diagonal block (lane i: row i in r) back into S and into
+// the row-major Lt (reciprocal pivots, from the FP64 dinv, in column 16).
+template <typename T>
+__device__ __forceinline__ void chol_diag_store(T *S, int c0, int nbk, const double *dinv, T *Lt, const T (&r)[CHOL_NB],
+                                                int lane) {
+	if (lane < CHOL_NB) {
+#pragma unroll
+		for (int l = 0; l < CHOL_NB; l++) Lt[lane * 17 + l] = (l <= lane) ? r[l] : T(0);
+		if (lane < nbk) {
+#pragma unroll
+			for (int l = 0; l < CHOL_NB; l++)
+				if (l <= lane) lp_at(S, c0 + lane, c0 + l) = r[l];
+		}
+	}
+	__syncwarp();
+	if (lane < CHOL_NB) Lt[lane * 17 + 16] = (lane < nbk) ? (T)dinv[c0 + lane] : T(1);
+	__syncwarp();
+}
 
 // Warp 0: factor the diagonal block at column c0 (nbk <= 16 real columns; the
 // padding is the identity) in FP64 registers; write L_KK back into S, 1/L_jj
@@ -154,34 +180,65 @@ struct DiagCol<CHOL_NB> {
 template <typename T>
 __device__ void chol_diag_factor(T *S, int c0, int nbk, double *dinv, T *Lt, int *bad) {
 	const int lane = threadIdx.x & 31;
-	double r[CHOL_NB];
+	T r[CHOL_NB];
 #pragma unroll
 	for (int l = 0; l < CHOL_NB; l++) {
-		double x = 0.0;
+		T x = T(0);
 		if (lane < CHOL_NB && l <= lane) {
 			if (lane < nbk && l < nbk)
-				x = (double)lp_at(S, c0 + lane, c0 + l);
+				x = lp_at(S, c0 + lane, c0 + l);
 			else if (l == lane)
-				x = 1.0;
+				x = T(1);
 		}
 		r[l] = x;
 	}
-	DiagCol<0>::run(r, lane, nbk, c0, dinv, bad);
-	if (lane < CHOL_NB) {
-		double dd = 1.0;
+	DiagCol<0, T>::run(r, lane, nbk, c0, dinv, bad);
+	chol_diag_store<T>(S, c0, nbk, dinv, Lt, r, lane);
+}
+
+// Warp 0, look-ahead step: the rank-16 update of diagonal block K+1 (columns
+// c0n..c0n+15) with the panel of block column K (columns c0..c0+15, already
+// solved), fused with its factorization.  Lane i (and lane i+16) own row i of
+// the block; the two half-warps take 8 of the 16 panel columns each, reading
+// the panel rows of the block as broadcast tile-column loads, and their
+// partial sums meet by one shuffle.  The update runs in the working precision
+// T, the factorization in FP64 registers (DiagCol).  Outputs as
+// chol_diag_factor.
+template <typename T>
+__device__ void chol_diag_update_factor(T *S, int c0n, int nbk, int c0, double *dinv, T *Lt, int *bad) {
+	const int lane = threadIdx.x & 31;
+	const int i = lane & 15, h = lane >> 4;
+	const int pn = c0n >> 2, kb = c0 >> 2;
+	T u[CHOL_NB];
 #pragma unroll
-		for (int l = 0; l < CHOL_NB; l++) {
-			Lt[lane * 17 + l] = (l <= lane) ? (T)r[l] : T(0);
-			if (l == lane) dd = r[l];
-		}
-		Lt[lane * 17 + 16] = (dd != 0.0) ? (T)(1.0 / dd) : T(0);
-		if (lane < nbk) {
+	for (int l = 0; l < CHOL_NB; l++) u[l] = (h == 0 && l <= i && i < nbk && l < nbk) ? lp_at(S, c0n + i, c0n + l) : T(0);
+	// row i of the panel block, the half-warp's 8 columns
+	T pr[8];
 #pragma unroll
-			for (int l = 0; l < CHOL_NB; l++)
-				if (l <= lane) lp_at(S, c0 + lane, c0 + l) = (T)r[l];
+	for (int l = 0; l < 8; l++) pr[l] = (i < nbk) ? lp_at(S, c0n + i, c0 + 8 * h + l) : T(0);
+#pragma unroll
+	for (int jq = 0; jq < 4; jq++) {
+		if (4 * jq >= nbk) break;  // row panels past the end of the matrix
+#pragma unroll
+		for (int l = 0; l < 8; l++) {
+			const int col = 8 * h + l;
+			T v0, v1, v2, v3;
+			tile_col_ld<T>(S, pn + jq, kb + (col >> 2), col & 3, v0, v1, v2, v3);
+			u[4 * jq] = fma(-pr[l], v0, u[4 * jq]);
+			u[4 * jq + 1] = fma(-pr[l], v1, u[4 * jq + 1]);
+			u[4 * jq + 2] = fma(-pr[l], v2, u[4 * jq + 2]);
+			u[4 * jq + 3] = fma(-pr[l], v3, u[4 * jq + 3]);
 		}
 	}
-	__syncwarp();
+	T r[CHOL_NB];
+#pragma unroll
+	for (int l = 0; l < CHOL_NB; l++) {
+		const T s = u[l] + __shfl_xor_sync(0xffffffffu, u[l], 16);
+		// real entries of the lower triangle; identity in the padding
+		r[l] = (l <= i && i < nbk && l < nbk) ? s : ((l == i && i >= nbk) ? T(1) : T(0));
+	}
+	DiagCol<0, T>::run(r, lane, nbk, c0n, dinv, bad);
+	chol_diag_store<T>(S, c0n, nbk, dinv, Lt, r, lane);
 }
 
 // panel of block column c0, rows r in [rbeg, rend): substitution with the
@@ -308,13 +365,7 @@ __device__ void chol_smem(T *S, int n, double *dinv, T *Lt, int *bad, T *invL_al
 		const int ntiles = R * (R + 1) / 2;
 		const int ndiag = ntiles < 10 ? ntiles : 10;
 		if (warp == 0) {
-			if (lane < ndiag) {
-				int ti, tj;
-				tri_index(lane, ti, tj);
-				chol_tile_update<T>(S, ti + k0 + 4, tj + k0 + 4, c0);
-			}
-			__syncwarp();
-			chol_diag_factor<T>(S, c0 + CHOL_NB, min(CHOL_NB, n - c0 - CHOL_NB), dinv, Lt, bad);
+			chol_diag_update_factor<T>(S, c0 + CHOL_NB, min(CHOL_NB, n - c0 - CHOL_NB), c0, dinv, Lt, bad);
 		} else {
 			for (int t = ndiag + tid - 32; t < ntiles; t += nt - 32) {
 				int ti, tj;

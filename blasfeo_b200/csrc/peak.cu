@@ -57,3 +57,4 @@ double blasfeo_b200_measure_fma_peak(char prec, int iters) {
 }
 
 }  // extern "C"
+

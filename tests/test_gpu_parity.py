@@ -274,3 +274,4 @@ def test_level2_solves(bf, orc):
     r = bf.DVec(n)
     bf.blasfeo_dgemv_n(n, n, 1.0, dS, 0, 0, x, 0, -1.0, xb, 0, r, 0)
     assert np.abs(r.unpack()).max() < 1e-11
+
