@@ -92,10 +92,14 @@ __global__ void k_posv_classify(int batch, const int *__restrict__ nvec, int max
 
 // shared-memory plan of the posv kernel
 struct PosvPlan {
-	size_t S_off, inv_off, dinv_off, scr_off, w_off, x_off, r_off, ybuf_off, asum_off, misc_off, total;
+	size_t S_off, inv_off, dinv_off, scr_off, w_off, x_off, r_off, ybuf_off, asum_off, red_off, misc_off, total;
 };
+// CTA size of a size class (largest n of the class)
+__host__ __device__ inline int posv_threads(int upper) {
+	return upper <= 64 ? 64 : (upper <= 128 ? 128 : (upper <= 192 ? 256 : 512));
+}
 template <typename T, bool MIXED>
-__host__ __device__ inline PosvPlan posv_plan(int max_n) {
+__host__ __device__ inline PosvPlan posv_plan(int max_n, int nt) {
 	PosvPlan p;
 	const int P = (max_n + 3) / 4;
 	const int NB = (max_n + 15) / 16;
@@ -109,7 +113,10 @@ __host__ __device__ inline PosvPlan posv_plan(int max_n) {
 	p.r_off = p.x_off + (MIXED ? a16((size_t)nv * sizeof(double)) : 0);
 	p.ybuf_off = p.r_off + (MIXED ? a16((size_t)nv * sizeof(double)) : 0);
 	p.asum_off = p.ybuf_off + a16(16 * sizeof(T));
-	p.misc_off = p.asum_off + (MIXED ? a16((size_t)nv * sizeof(double)) : 0);
+	p.red_off = p.asum_off + (MIXED ? a16((size_t)nv * sizeof(double)) : 0);
+	// residual: column partial sums of the upper half of the warps, 8 per lane
+	const int nw = nt / 32;
+	p.misc_off = p.red_off + (MIXED ? a16((size_t)(nw > 1 ? nw / 2 : 1) * 32 * 8 * sizeof(double)) : 0);
 	p.total = p.misc_off + 64 * sizeof(double);
 	return p;
 }
@@ -214,98 +221,135 @@ __device__ double block_max(double v, double *red) {
 	return r;
 }
 
-// r = b - A x (FP64), A symmetric given by its lower triangle.
+// r = b - A x (FP64), A symmetric given by its lower triangle, in one pass
+// over the 4x4 tiles of the lower triangle (every tile read once).
 // LP = false: A in BLASFEO panel-major storage (tile (ti,tj) at base + 4*ti*cn + 16*tj);
 // LP = true: A in lower panels (tile at base + lp_off(ti) + 16*tj).
-// Two deterministic passes, no atomics: pass 1 gives every 4-row tile row to
-// one warp (row part A(i,j<=i) x_j, lanes over the tiles of the row, 128-byte
-// tile loads, warp reduction); pass 2 gives every tile column to one warp
-// (column part sum_{i>j} A(i,j) x_i for the rows of that column).  With
-// want_norm the row sums of |A| are accumulated the same way into asum.
+// Warp w takes tile rows ti = w, w + NW, ...; lane l the tiles tj = l, l + 32
+// of the row.  A tile adds A_tile x_tj to rows ti (row part, reduced over the
+// lanes by a shuffle tree) and, below the diagonal, A_tile^T x_ti to rows tj
+// (column part, kept per lane in registers and summed over the warps by a
+// fixed tree through shared memory), so the result does not depend on timing.
+// RES: the residual into r; NORM: the row sums of |A| into asum (same scheme).
+// red: (NW/2) * 32 * 8 doubles of shared memory.  n <= 256 (two tile
+// columns per lane).
 template <bool LP>
 __device__ __forceinline__ const double *res_tile(const double *base, int cn, int ti, int tj) {
 	return LP ? base + lp_off(ti) + 16 * tj : base + (size_t)(4 * ti) * cn + 16 * tj;
 }
 
-template <bool LP>
+template <bool LP, bool RES, bool NORM>
 __device__ void sym_residual(const double *base, int cn, int n, const double *b, const double *x, double *r,
-                             double *asum, bool want_norm) {
+                             double *asum, double *red) {
 	const int tid = threadIdx.x, nt = blockDim.x;
 	const int lane = tid & 31, warp = tid >> 5, nw = nt >> 5;
 	const int P = (n + 3) >> 2;
-	for (int pass = 0; pass < 2; pass++) {
-		for (int t0 = warp; t0 < P; t0 += nw) {
-			double acc[4] = {0.0, 0.0, 0.0, 0.0}, sa[4] = {0.0, 0.0, 0.0, 0.0};
-			// pass 0: tiles (t0, t1), t1 <= t0 (row part); pass 1: tiles (t1, t0), t1 > t0 (column part)
-			const int lo = pass == 0 ? 0 : t0 + 1, hi = pass == 0 ? t0 : P - 1;
-			for (int t1 = lo + lane; t1 <= hi; t1 += 32) {
-				const int ti = pass == 0 ? t0 : t1, tj = pass == 0 ? t1 : t0;
-				const double *t = res_tile<LP>(base, cn, ti, tj);
-				double e[16];
+	double cacc[2][4], cabs[2][4];
 #pragma unroll
-				for (int q = 0; q < 8; q++) {
-					double2 v = __ldg((const double2 *)(t + 2 * q));
-					e[2 * q] = v.x;
-					e[2 * q + 1] = v.y;
-				}
+	for (int m = 0; m < 2; m++)
 #pragma unroll
-				for (int q = 0; q < 4; q++)
+		for (int q = 0; q < 4; q++) cacc[m][q] = cabs[m][q] = 0.0;
+	for (int ti = warp; ti < P; ti += nw) {
+		double racc[4] = {0.0, 0.0, 0.0, 0.0}, rabs[4] = {0.0, 0.0, 0.0, 0.0};
+		const double2 xr01 = *(const double2 *)(x + 4 * ti), xr23 = *(const double2 *)(x + 4 * ti + 2);
+		const double xr[4] = {xr01.x, xr01.y, xr23.x, xr23.y};
 #pragma unroll
-					for (int rr = 0; rr < 4; rr++) {
-						int gi = 4 * ti + rr, gj = 4 * tj + q;
-						if (!(gi < n && gj < n && (tj < ti || gj <= gi))) e[4 * q + rr] = 0.0;
-					}
-				if (pass == 0) {
-					const double x0 = x[4 * tj], x1 = x[4 * tj + 1], x2 = x[4 * tj + 2], x3 = x[4 * tj + 3];
+		for (int m = 0; m < 2; m++) {
+			const int tj = lane + 32 * m;
+			if (tj > ti) continue;
+			// e[4*q + a]: row 4ti+a, column 4tj+q; padding and the upper part of the diagonal tile masked
+			double e[16];
+			const double *t = res_tile<LP>(base, cn, ti, tj);
 #pragma unroll
-					for (int rr = 0; rr < 4; rr++) {
-						acc[rr] = fma(e[rr], x0, fma(e[4 + rr], x1, fma(e[8 + rr], x2, fma(e[12 + rr], x3, acc[rr]))));
-						if (want_norm) sa[rr] += fabs(e[rr]) + fabs(e[4 + rr]) + fabs(e[8 + rr]) + fabs(e[12 + rr]);
-					}
-					if (tj == ti) {
-						// strictly-upper part of the diagonal tile mirrors the lower part
-						acc[0] = fma(e[1], x1, fma(e[2], x2, fma(e[3], x3, acc[0])));
-						acc[1] = fma(e[6], x2, fma(e[7], x3, acc[1]));
-						acc[2] = fma(e[11], x3, acc[2]);
-						if (want_norm) {
-							sa[0] += fabs(e[1]) + fabs(e[2]) + fabs(e[3]);
-							sa[1] += fabs(e[6]) + fabs(e[7]);
-							sa[2] += fabs(e[11]);
-						}
-					}
-				} else {
-					const double x0 = x[4 * ti], x1 = x[4 * ti + 1], x2 = x[4 * ti + 2], x3 = x[4 * ti + 3];
-#pragma unroll
-					for (int q = 0; q < 4; q++) {
-						acc[q] = fma(e[4 * q], x0, fma(e[4 * q + 1], x1, fma(e[4 * q + 2], x2, fma(e[4 * q + 3], x3, acc[q]))));
-						if (want_norm)
-							sa[q] += fabs(e[4 * q]) + fabs(e[4 * q + 1]) + fabs(e[4 * q + 2]) + fabs(e[4 * q + 3]);
-					}
-				}
+			for (int q = 0; q < 8; q++) {
+				const double2 v = __ldg((const double2 *)(t + 2 * q));
+				e[2 * q] = v.x;
+				e[2 * q + 1] = v.y;
 			}
 #pragma unroll
-			for (int off = 16; off > 0; off >>= 1)
+			for (int q = 0; q < 4; q++)
 #pragma unroll
-				for (int rr = 0; rr < 4; rr++) {
-					acc[rr] += __shfl_down_sync(0xffffffffu, acc[rr], off);
-					if (want_norm) sa[rr] += __shfl_down_sync(0xffffffffu, sa[rr], off);
+				for (int a = 0; a < 4; a++) {
+					const int gi = 4 * ti + a, gj = 4 * tj + q;
+					if (!(gi < n && gj < n && (tj < ti || gj <= gi))) e[4 * q + a] = 0.0;
 				}
-			if (lane == 0) {
+			const double2 xc01 = *(const double2 *)(x + 4 * tj), xc23 = *(const double2 *)(x + 4 * tj + 2);
+			const double xc[4] = {xc01.x, xc01.y, xc23.x, xc23.y};
 #pragma unroll
-				for (int rr = 0; rr < 4; rr++) {
-					const int i = 4 * t0 + rr;
-					if (pass == 0) {
-						r[i] = (i < n ? b[i] : 0.0) - acc[rr];
-						if (want_norm) asum[i] = sa[rr];
-					} else {
-						r[i] -= acc[rr];
-						if (want_norm) asum[i] += sa[rr];
-					}
+			for (int a = 0; a < 4; a++) {
+				if (RES) racc[a] = fma(e[a], xc[0], fma(e[4 + a], xc[1], fma(e[8 + a], xc[2], fma(e[12 + a], xc[3], racc[a]))));
+				if (NORM) rabs[a] += fabs(e[a]) + fabs(e[4 + a]) + fabs(e[8 + a]) + fabs(e[12 + a]);
+			}
+			if (tj < ti) {
+#pragma unroll
+				for (int q = 0; q < 4; q++) {
+					if (RES) cacc[m][q] = fma(e[4 * q], xr[0], fma(e[4 * q + 1], xr[1], fma(e[4 * q + 2], xr[2], fma(e[4 * q + 3], xr[3], cacc[m][q]))));
+					if (NORM) cabs[m][q] += fabs(e[4 * q]) + fabs(e[4 * q + 1]) + fabs(e[4 * q + 2]) + fabs(e[4 * q + 3]);
+				}
+			} else {
+				// strictly upper part of the diagonal tile mirrors the lower part
+				if (RES) {
+					racc[0] = fma(e[1], xc[1], fma(e[2], xc[2], fma(e[3], xc[3], racc[0])));
+					racc[1] = fma(e[6], xc[2], fma(e[7], xc[3], racc[1]));
+					racc[2] = fma(e[11], xc[3], racc[2]);
+				}
+				if (NORM) {
+					rabs[0] += fabs(e[1]) + fabs(e[2]) + fabs(e[3]);
+					rabs[1] += fabs(e[6]) + fabs(e[7]);
+					rabs[2] += fabs(e[11]);
 				}
 			}
 		}
+#pragma unroll
+		for (int off = 16; off > 0; off >>= 1)
+#pragma unroll
+			for (int a = 0; a < 4; a++) {
+				if (RES) racc[a] += __shfl_xor_sync(0xffffffffu, racc[a], off);
+				if (NORM) rabs[a] += __shfl_xor_sync(0xffffffffu, rabs[a], off);
+			}
+		if (lane < 4) {
+			const int i = 4 * ti + lane;
+			const double ra = lane == 0 ? racc[0] : (lane == 1 ? racc[1] : (lane == 2 ? racc[2] : racc[3]));
+			if (RES) r[i] = (i < n ? b[i] : 0.0) - ra;
+			if (NORM) asum[i] = lane == 0 ? rabs[0] : (lane == 1 ? rabs[1] : (lane == 2 ? rabs[2] : rabs[3]));
+		}
+	}
+	// column parts: fixed-order tree over the warps, then warp 0 adds them to r
+	for (int half = nw >> 1; half >= 1; half >>= 1) {
+		if (warp >= half && warp < 2 * half) {
+			double *d = red + ((size_t)(warp - half) * 32 + lane) * 8;
+#pragma unroll
+			for (int m = 0; m < 2; m++)
+#pragma unroll
+				for (int q = 0; q < 4; q++) d[4 * m + q] = RES ? cacc[m][q] : cabs[m][q];
+		}
+		__syncthreads();
+		if (warp < half) {
+			const double *d = red + ((size_t)warp * 32 + lane) * 8;
+#pragma unroll
+			for (int m = 0; m < 2; m++)
+#pragma unroll
+				for (int q = 0; q < 4; q++) {
+					if (RES) cacc[m][q] += d[4 * m + q];
+					else cabs[m][q] += d[4 * m + q];
+				}
+		}
 		__syncthreads();
 	}
+	if (warp == 0) {
+#pragma unroll
+		for (int m = 0; m < 2; m++) {
+			const int tj = lane + 32 * m;
+			if (tj < P) {
+#pragma unroll
+				for (int q = 0; q < 4; q++) {
+					if (RES) r[4 * tj + q] -= cacc[m][q];
+					if (NORM) asum[4 * tj + q] += cabs[m][q];
+				}
+			}
+		}
+	}
+	__syncthreads();
 }
 
 template <typename T, bool MIXED, int NT, int MINB>
@@ -315,7 +359,7 @@ __global__ void __launch_bounds__(NT, MINB) k_posv(int cls, int max_n, PosvWs ws
                                               const DevVec<double> *__restrict__ sx, int max_iter, double tol,
                                               int *iters, double *berr, int *info, double *slots) {
 	extern __shared__ __align__(16) unsigned char smem[];
-	const PosvPlan pl = posv_plan<T, MIXED>(max_n);
+	const PosvPlan pl = posv_plan<T, MIXED>(max_n, NT);
 	// per-CTA FP64 copy of the lower panels (refinement residuals read it from
 	// L2 instead of the caller's matrix, which may sit in host memory)
 	double *slot = slots ? slots + (size_t)blockIdx.x * lp_size(max_n) : nullptr;
@@ -329,6 +373,7 @@ __global__ void __launch_bounds__(NT, MINB) k_posv(int cls, int max_n, PosvWs ws
 	double *rs = (double *)(smem + pl.r_off);
 	T *ybuf = (T *)(smem + pl.ybuf_off);
 	double *misc = (double *)(smem + pl.misc_off);
+	double *red = (double *)(smem + pl.red_off);
 	int *s_bad = (int *)(misc + 40);
 	int *s_item = (int *)(misc + 41);
 	const int tid = threadIdx.x, nt = blockDim.x;
@@ -402,10 +447,14 @@ __global__ void __launch_bounds__(NT, MINB) k_posv(int cls, int max_n, PosvWs ws
 			trsv_bwd<T>(S, n, invL, dinv, w, ybuf);
 			for (int i = tid; i < n; i += nt) xs[i] += (double)w[i] / scale;
 			__syncthreads();
-			if (slot)
-				sym_residual<true>(slot, 0, n, bg, xs, rs, asum, it == 0);
-			else
-				sym_residual<false>(a.p, a.cn, n, bg, xs, rs, asum, it == 0);
+			// ||A||_inf (row sums of |A|) once, before the first residual
+			if (slot) {
+				if (it == 0) sym_residual<true, false, true>(slot, 0, n, bg, xs, rs, asum, red);
+				sym_residual<true, true, false>(slot, 0, n, bg, xs, rs, asum, red);
+			} else {
+				if (it == 0) sym_residual<false, false, true>(a.p, a.cn, n, bg, xs, rs, asum, red);
+				sym_residual<false, true, false>(a.p, a.cn, n, bg, xs, rs, asum, red);
+			}
 			// norms
 			double rm = 0.0, xm = 0.0;
 			for (int i = tid; i < n; i += nt) {
@@ -569,13 +618,13 @@ int posv_run(int batch, const int *n, int max_n, const void *sA, const void *sb,
 	int nc = 0;
 	int smem_limit_n = 0;  // largest n the shared-memory kernel takes
 	for (int v = 4; v <= 4096; v += 4)
-		if (posv_plan<T, MIXED>(v).total <= smem_cap) smem_limit_n = v;
+		if (posv_plan<T, MIXED>(v, posv_threads(v)).total <= smem_cap) smem_limit_n = v;
 	for (int u : uppers) {
 		if (nc >= POSV_MAX_CLASSES - 1) break;
 		int uu = u < smem_limit_n ? u : smem_limit_n;
 		if (nc > 0 && uu <= cfg[nc - 1].upper) continue;
 		cfg[nc].upper = uu;
-		cfg[nc].threads = uu <= 64 ? 64 : (uu <= 128 ? 128 : (uu <= 192 ? 256 : 512));
+		cfg[nc].threads = posv_threads(uu);
 		nc++;
 		if (uu >= max_n) break;
 	}
@@ -629,7 +678,7 @@ int posv_run(int batch, const int *n, int max_n, const void *sA, const void *sb,
 			                                     (const DevVec<double> *)sb, (const DevVec<double> *)sx,
 			                                     (double *)(wsp + slots_off), info);
 		} else {
-			PosvPlan pl = posv_plan<T, MIXED>(cfg[c].upper);
+			PosvPlan pl = posv_plan<T, MIXED>(cfg[c].upper, cfg[c].threads);
 			double *rs = rslots ? (double *)(wsp + rslots_off) : nullptr;
 			int st;
 			if (cfg[c].upper <= 64)
