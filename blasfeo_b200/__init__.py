@@ -94,6 +94,8 @@ _sig("blasfeo_b200_error_string", C.c_char_p, _i)
 _sig("blasfeo_b200_set_stream", None, _vp)
 _sig("blasfeo_b200_get_stream", _vp)
 _sig("blasfeo_b200_set_sync", None, _i)
+_sig("blasfeo_b200_set_posv_engine", _i, _i)
+_sig("blasfeo_b200_get_posv_engine", _i)
 _sig("blasfeo_b200_version", _i)
 _sig("blasfeo_b200_measure_fma_peak", _d, C.c_char, _i)
 for p, M, V, R in (("d", _DM, _DV, _d), ("s", _SM, _SV, _f)):

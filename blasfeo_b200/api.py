@@ -19,6 +19,7 @@ from . import lib, dmat, smat, dvec, svec, dmat_batch, smat_batch, check
 
 __all__ = [
     "DMat", "SMat", "DVec", "SVec", "DMatBatch", "SMatBatch", "device_buffer", "set_stream", "set_sync",
+    "set_posv_engine", "POSV_DEFAULT", "POSV_SIMT", "POSV_TENSOR",
     "blasfeo_dgemm_nt", "blasfeo_dsyrk_ln", "blasfeo_dtrsm_rltn", "blasfeo_dtrmm_rlnn", "blasfeo_dpotrf_l",
     "blasfeo_dsyrk_dpotrf_ln", "blasfeo_dgetrf_rp", "blasfeo_dgeqrf", "blasfeo_dgeqrf_worksize",
     "blasfeo_sgemm_nt", "blasfeo_ssyrk_ln", "blasfeo_strsm_rltn", "blasfeo_strmm_rlnn", "blasfeo_spotrf_l",
@@ -42,6 +43,17 @@ def set_stream(stream):
 
 def set_sync(sync):
     lib.blasfeo_b200_set_sync(1 if sync else 0)
+
+
+POSV_DEFAULT, POSV_SIMT, POSV_TENSOR = 0, 1, 2
+
+
+def set_posv_engine(engine):
+    """Engine of blasfeo_dsposv_l_vbatch for n <= 256 (this host thread):
+    POSV_SIMT, POSV_TENSOR or POSV_DEFAULT; returns the previous engine."""
+    prev = lib.blasfeo_b200_get_posv_engine()
+    check(lib.blasfeo_b200_set_posv_engine(int(engine)))
+    return prev
 
 
 class _Mat:

@@ -30,6 +30,7 @@ int finish_single();                      // launch check + optional stream sync
 void *workspace(size_t bytes, cudaStream_t s);
 int num_sms();
 size_t max_smem_optin();
+int posv_engine();                        // engine of the mixed SPD solver (BLASFEO_B200_POSV_*)
 
 template <typename T> struct MatT;
 template <> struct MatT<double> { typedef struct blasfeo_dmat type; typedef struct blasfeo_dmat_batch batch; typedef struct blasfeo_dvec vec; };

@@ -22,24 +22,9 @@
 #include "chol.cuh"
 #include "common.cuh"
 #include "kernels.cuh"
+#include "posv.cuh"
 
 namespace {
-
-constexpr int POSV_MAX_CLASSES = 10;
-
-struct ClassTable {
-	int nclass;
-	int upper[POSV_MAX_CLASSES];  // inclusive upper bound of n per class (ascending)
-};
-
-// workspace: [0] list (batch ints)  [then] per class: start, count, counter
-struct PosvWs {
-	int *list;
-	int *start;
-	int *count;
-	int *counter;
-	int *hist;  // 1 + max n buckets
-};
 
 __host__ __device__ inline size_t a16(size_t x) { return (x + 15) / 16 * 16; }
 
@@ -604,6 +589,12 @@ int launch_posv(int c, int upper, size_t smem, int batch, int rslots, PosvWs ws,
 	return bf::check_launch();
 }
 
+// the mixed solver's engine for n <= 256 (tensor cores unless SIMT is asked for)
+inline bool tensor_engine() {
+	const int e = bf::posv_engine();
+	return e == BLASFEO_B200_POSV_TENSOR || (e == BLASFEO_B200_POSV_DEFAULT && POSV_TENSOR_DEFAULT);
+}
+
 template <typename T, bool MIXED>
 int posv_run(int batch, const int *n, int max_n, const void *sA, const void *sb, const void *sx, int max_iter,
              double tol, int *iters, double *berr, int *info, void *work, size_t work_bytes, cudaStream_t s,
@@ -677,6 +668,10 @@ int posv_run(int batch, const int *n, int max_n, const void *sA, const void *sb,
 			k_posv_global<<<gslots, 256, 0, s>>>(c, max_n, ws, n, (const DevDesc<double> *)sA,
 			                                     (const DevVec<double> *)sb, (const DevVec<double> *)sx,
 			                                     (double *)(wsp + slots_off), info);
+		} else if (MIXED && !use_slots && cfg[c].upper <= 256 && tensor_engine()) {
+			const int st = bf::posv_tc_launch(c, cfg[c].upper, batch, ws, n, sA, sb, sx, max_iter, tol, iters, berr,
+			                                  info, s);
+			if (st) return st;
 		} else {
 			PosvPlan pl = posv_plan<T, MIXED>(cfg[c].upper, cfg[c].threads);
 			double *rs = rslots ? (double *)(wsp + rslots_off) : nullptr;

@@ -11,6 +11,7 @@ namespace bf {
 static thread_local int g_last_error = BLASFEO_B200_OK;
 static thread_local cudaStream_t g_stream = nullptr;
 static thread_local int g_sync = 1;
+static thread_local int g_posv_engine = BLASFEO_B200_POSV_DEFAULT;
 
 void set_error(int status) {
 	if (status != BLASFEO_B200_OK) g_last_error = status;
@@ -26,6 +27,7 @@ int check_launch() {
 }
 
 cudaStream_t cur_stream() { return g_stream; }
+int posv_engine() { return g_posv_engine; }
 bool sync_mode() { return g_sync != 0; }
 
 int finish_single() {
@@ -122,6 +124,12 @@ const char *blasfeo_b200_error_string(int status) {
 void blasfeo_b200_set_stream(void *stream) { bf::g_stream = (cudaStream_t)stream; }
 void *blasfeo_b200_get_stream(void) { return (void *)bf::g_stream; }
 void blasfeo_b200_set_sync(int sync) { bf::g_sync = sync; }
+int blasfeo_b200_set_posv_engine(int engine) {
+	if (engine < BLASFEO_B200_POSV_DEFAULT || engine > BLASFEO_B200_POSV_TENSOR) return BLASFEO_B200_EINVAL;
+	bf::g_posv_engine = engine;
+	return BLASFEO_B200_OK;
+}
+int blasfeo_b200_get_posv_engine(void) { return bf::g_posv_engine; }
 int blasfeo_b200_version(void) { return 100; }
 
 }  // extern "C"

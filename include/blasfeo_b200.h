@@ -274,6 +274,20 @@ int blasfeo_dsposv_l_vbatch(int batch, const int *n, int max_n, const struct bla
 	const struct blasfeo_dvec *sb, const struct blasfeo_dvec *sx, int max_iter, double tol,
 	int *iters, double *berr, int *info, void *work, size_t work_bytes, void *stream);
 
+/* Engine of blasfeo_dsposv_l_vbatch for systems with n <= 256 (per calling
+ * host thread; larger systems always take the SIMT/global-memory kernels):
+ *   SIMT:   FP32 Cholesky with FP32 FMA trailing updates in shared memory;
+ *   TENSOR: trailing matrix in tensor memory, rank-16 trailing updates as
+ *           3xTF32 tcgen05.mma with FP32 accumulation (same FP64 diagonal
+ *           blocks, residual and refinement).
+ * DEFAULT is the engine the library measured fastest on the uneven-size
+ * workload.  set returns BLASFEO_B200_EINVAL for an unknown engine. */
+#define BLASFEO_B200_POSV_DEFAULT 0
+#define BLASFEO_B200_POSV_SIMT 1
+#define BLASFEO_B200_POSV_TENSOR 2
+int blasfeo_b200_set_posv_engine(int engine);
+int blasfeo_b200_get_posv_engine(void);
+
 /* Fused per-instance chain on a uniform batch (m = 16, 1 <= k <= 64; all
  * slabs from blasfeo_create_dmat_batch, zero offsets), replacing the sequence
  * blasfeo_dsyrk_ln (d_blas3_lib4.c:5400) + blasfeo_ddiare + blasfeo_dpotrf_l
