@@ -102,11 +102,18 @@ template <typename T, bool LOWER>
 int gemm_nt_launch(int batch, SizeArg sz, int max_m, int max_n, int max_k, T alpha, MatArg<T> A, MatArg<T> B,
                    T beta, MatArg<T> C, MatArg<T> D, cudaStream_t s, int variant) {
 	if (batch <= 0 || max_m <= 0 || max_n <= 0) return BLASFEO_B200_OK;
+	const int mx = max_m > max_n ? max_m : max_n;
 	if (variant < 0) {
-		int mx = max_m > max_n ? max_m : max_n;
-		variant = mx > 48 ? 2 : (mx > 16 ? 1 : 0);
+		if (sizeof(T) == 8)  // FP64 tensor cores: 64x64 tiles once the batch fills the GPU
+			variant = (mx > 32 && (long long)batch * cdiv(max_m, 64) * cdiv(max_n, 64) >= 2 * num_sms()) ? 4 : 5;
+		else
+			variant = mx > 48 ? 2 : (mx > 16 ? 1 : 0);
 	}
 	(void)max_k;
+	if constexpr (sizeof(T) == 8) {
+		if (variant == 4 || variant == 5)
+			return dgemm_nt_dmma_launch<LOWER>(batch, sz, max_m, max_n, alpha, A, B, beta, C, D, s, variant - 4);
+	}
 	switch (variant) {
 	case 0: return launch_gemm_cfg<T, 16, 16, 16, 2, 2, LOWER>(batch, sz, max_m, max_n, alpha, A, B, beta, C, D, s);
 	case 1: return launch_gemm_cfg<T, 32, 32, 16, 2, 2, LOWER>(batch, sz, max_m, max_n, alpha, A, B, beta, C, D, s);
@@ -388,7 +395,7 @@ int blasfeo_dgemm_nt_vbatch_variant(int batch, const int *m, const int *n, const
                                     double beta, const struct blasfeo_dmat *sC, const struct blasfeo_dmat *sD,
                                     int variant, void *stream) {
 	if (batch < 0 || !m || !n || !k || !sA || !sB || !sC || !sD) return BLASFEO_B200_EINVAL;
-	if (variant > 3) return BLASFEO_B200_EINVAL;
+	if (variant > 5) return BLASFEO_B200_EINVAL;
 	return bf::gemm_nt_launch<double, false>(batch, var_sizes(m, n, k), max_m, max_n, max_k, alpha,
 	                                         vbatch_arg<double>(sA), vbatch_arg<double>(sB), beta,
 	                                         vbatch_arg<double>(sC), vbatch_arg<double>(sD), (cudaStream_t)stream,
@@ -404,7 +411,7 @@ int blasfeo_dgemm_nt_vbatch(int batch, const int *m, const int *n, const int *k,
 /* number of kernel variants of a routine: op 0 gemm_nt, 1 potrf_l, 2 getrf_rp, 3 geqrf */
 int blasfeo_b200_num_variants(int op) {
 	switch (op) {
-	case 0: return 4;
+	case 0: return 6;
 	case 1: return 5;
 	case 2: return 6;
 	case 3: return 6;

@@ -9,6 +9,11 @@ template <typename T, bool LOWER>
 int gemm_nt_launch(int batch, SizeArg sz, int max_m, int max_n, int max_k, T alpha, MatArg<T> A, MatArg<T> B,
                    T beta, MatArg<T> C, MatArg<T> D, cudaStream_t s, int variant);
 
+// FP64 tensor-core (DMMA) gemm_nt / syrk_ln; tile 0 = 64x64, 1 = 32x32 (gemm_dmma.cu)
+template <bool LOWER>
+int dgemm_nt_dmma_launch(int batch, SizeArg sz, int max_m, int max_n, double alpha, MatArg<double> A,
+                         MatArg<double> B, double beta, MatArg<double> C, MatArg<double> D, cudaStream_t s, int tile);
+
 // D = chol(C) lower, inverse diagonal into D's dA, info (device, may be null)
 template <typename T>
 int potrf_launch(int batch, SizeArg sz, int max_m, MatArg<T> C, MatArg<T> D, int *info, cudaStream_t s,

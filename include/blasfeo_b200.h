@@ -239,7 +239,8 @@ int blasfeo_dgeqrf_vbatch(int batch, const int *m, const int *n, int max_m, int 
 
 /* Kernel-variant selection for the variable-size batches (used by the
  * autotuner and the learned cost model; variant -1 = built-in heuristic).
- * op: 0 gemm_nt (4 tile shapes), 1 potrf_l (shared memory with 64/128/256/512
+ * op: 0 gemm_nt (4 SIMT tile shapes; FP64 adds 4 = 64x64 and 5 = 32x32 tiles
+ * on the FP64 tensor cores, which the s-twin runs as SIMT tiles), 1 potrf_l (shared memory with 64/128/256/512
  * threads, or global memory), 2 getrf_rp and 3 geqrf (global or shared
  * memory, 128/256/512 threads each).  Variants only change speed, never the
  * arithmetic of an element. */

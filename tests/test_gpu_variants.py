@@ -44,11 +44,11 @@ def nvar(bf, op):
 
 
 def test_variant_counts(bf):
-    assert [nvar(bf, i) for i in range(4)] == [4, 5, 6, 6]
+    assert [nvar(bf, i) for i in range(4)] == [6, 5, 6, 6]
     assert nvar(bf, 9) == 0
 
 
-@pytest.mark.parametrize("variant", range(4))
+@pytest.mark.parametrize("variant", range(6))
 def test_gemm_variants(bf, variant):
     import torch
     rng = np.random.default_rng(variant)
@@ -147,4 +147,4 @@ def test_variant_out_of_range_rejected(bf):
     d = bf.descriptor_array([bf.DMat(4, 4)])
     assert bf.lib.blasfeo_dpotrf_l_vbatch_variant(1, P(nv), 4, P(d), P(d), None, 5, None) == 1
     assert bf.lib.blasfeo_dgemm_nt_vbatch_variant(1, P(nv), P(nv), P(nv), 4, 4, 4, 1.0, P(d), P(d), 0.0, P(d), P(d),
-                                                  4, None) == 1
+                                                  6, None) == 1
