@@ -412,7 +412,7 @@ int blasfeo_dgemm_nt_vbatch(int batch, const int *m, const int *n, const int *k,
 int blasfeo_b200_num_variants(int op) {
 	switch (op) {
 	case 0: return 6;
-	case 1: return 5;
+	case 1: return 6;
 	case 2: return 6;
 	case 3: return 6;
 	default: return 0;

@@ -14,6 +14,10 @@ template <bool LOWER>
 int dgemm_nt_dmma_launch(int batch, SizeArg sz, int max_m, int max_n, double alpha, MatArg<double> A,
                          MatArg<double> B, double beta, MatArg<double> C, MatArg<double> D, cudaStream_t s, int tile);
 
+// FP64 potrf_l for max_m <= 64, one warp per instance on the FP64 tensor cores (potrf_dmma.cu)
+int dpotrf_dmma_launch(int batch, SizeArg sz, int max_m, MatArg<double> C, MatArg<double> D, int *info,
+                       cudaStream_t s);
+
 // D = chol(C) lower, inverse diagonal into D's dA, info (device, may be null)
 template <typename T>
 int potrf_launch(int batch, SizeArg sz, int max_m, MatArg<T> C, MatArg<T> D, int *info, cudaStream_t s,

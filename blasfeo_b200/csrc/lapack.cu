@@ -363,10 +363,15 @@ namespace bf {
 
 // variant: -1 auto; 0..3: shared memory with 64/128/256/512 threads for the
 // instances that fit (the others in global memory, a second launch);
-// 4: everything in global memory.
+// 4: everything in global memory; 5 (FP64, max_m <= 64): one warp per
+// instance on the FP64 tensor cores (potrf_dmma.cu), the auto choice there.
 template <typename T>
 int potrf_launch(int batch, SizeArg sz, int max_m, MatArg<T> C, MatArg<T> D, int *info, cudaStream_t s, int variant) {
 	if (batch <= 0 || max_m <= 0) return BLASFEO_B200_OK;
+	if constexpr (sizeof(T) == 8) {
+		if (max_m <= 64 && (variant < 0 || variant == 5)) return dpotrf_dmma_launch(batch, sz, max_m, C, D, info, s);
+	}
+	if (variant == 5) variant = -1;
 	static int limit_cache[2] = {0, 0};
 	int &lim = limit_cache[sizeof(T) == 8];
 	if (!lim)
@@ -643,7 +648,7 @@ int blasfeo_sgeqrf_batch(int batch, int m, int n, struct blasfeo_smat_batch *sC,
 
 int blasfeo_dpotrf_l_vbatch_variant(int batch, const int *m, int max_m, const struct blasfeo_dmat *sC,
                                     const struct blasfeo_dmat *sD, int *info, int variant, void *stream) {
-	if (batch < 0 || !m || !sC || !sD || max_m < 0 || variant > 4) return BLASFEO_B200_EINVAL;
+	if (batch < 0 || !m || !sC || !sD || max_m < 0 || variant > 5) return BLASFEO_B200_EINVAL;
 	if (batch == 0 || max_m == 0) return BLASFEO_B200_OK;
 	return bf::potrf_launch<double>(batch, var_sizes(m, m, nullptr), max_m, vbatch_arg<double>(sC),
 	                                vbatch_arg<double>(sD), info, (cudaStream_t)stream, variant);

@@ -239,11 +239,15 @@ int blasfeo_dgeqrf_vbatch(int batch, const int *m, const int *n, int max_m, int 
 
 /* Kernel-variant selection for the variable-size batches (used by the
  * autotuner and the learned cost model; variant -1 = built-in heuristic).
- * op: 0 gemm_nt (4 SIMT tile shapes; FP64 adds 4 = 64x64 and 5 = 32x32 tiles
- * on the FP64 tensor cores, which the s-twin runs as SIMT tiles), 1 potrf_l (shared memory with 64/128/256/512
- * threads, or global memory), 2 getrf_rp and 3 geqrf (global or shared
- * memory, 128/256/512 threads each).  Variants only change speed, never the
- * arithmetic of an element. */
+ * op 0 gemm_nt: 0..3 SIMT tile shapes; 4 = 64x64 and 5 = 32x32 tiles on the
+ *   FP64 tensor cores (the s-twin runs 4 and 5 as SIMT tiles);
+ * op 1 potrf_l: 0..3 shared memory with 64/128/256/512 threads, 4 global
+ *   memory, 5 one warp per instance on the FP64 tensor cores (max_m <= 64;
+ *   larger batches take the heuristic);
+ * op 2 getrf_rp and 3 geqrf: global or shared memory, 128/256/512 threads.
+ * Variants change the schedule and, through the summation order of the dot
+ * products, the rounding of an element; every variant meets the routine's
+ * tolerance against the reference (pivot choices of getrf are identical). */
 int blasfeo_b200_num_variants(int op);
 int blasfeo_dgemm_nt_vbatch_variant(int batch, const int *m, const int *n, const int *k, int max_m, int max_n, int max_k,
 	double alpha, const struct blasfeo_dmat *sA, const struct blasfeo_dmat *sB, double beta,

@@ -60,7 +60,7 @@ def test_sampler_and_features():
             assert (m == 2 * n).all()
         f = at.features(op, b, m, n, k, at.NVAR[op] - 1)
         assert f.shape == (at.NFEAT,) and f[at.OPS.index(op)] == 1 and f[-at.MAXVAR:].sum() == 1
-    assert at.NVAR == {"gemm_nt": 6, "potrf_l": 5, "getrf_rp": 6, "geqrf": 6}
+    assert at.NVAR == {"gemm_nt": 6, "potrf_l": 6, "getrf_rp": 6, "geqrf": 6}
 
 
 def test_flop_counts():

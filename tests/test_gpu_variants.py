@@ -44,7 +44,7 @@ def nvar(bf, op):
 
 
 def test_variant_counts(bf):
-    assert [nvar(bf, i) for i in range(4)] == [6, 5, 6, 6]
+    assert [nvar(bf, i) for i in range(4)] == [6, 6, 6, 6]
     assert nvar(bf, 9) == 0
 
 
@@ -70,7 +70,7 @@ def test_gemm_variants(bf, variant):
         assert relfro(d.unpack(), 1.5 * a @ b.T - 0.5 * c) <= 1e-14
 
 
-@pytest.mark.parametrize("variant", [-1, 0, 1, 2, 3, 4])
+@pytest.mark.parametrize("variant", [-1, 0, 1, 2, 3, 4, 5])
 def test_potrf_variants(bf, orc, variant):
     import torch
     rng = np.random.default_rng(40 + variant)
@@ -145,6 +145,40 @@ def test_geqrf_variants(bf, orc, variant):
 def test_variant_out_of_range_rejected(bf):
     nv = ivec([4])
     d = bf.descriptor_array([bf.DMat(4, 4)])
-    assert bf.lib.blasfeo_dpotrf_l_vbatch_variant(1, P(nv), 4, P(d), P(d), None, 5, None) == 1
+    assert bf.lib.blasfeo_dpotrf_l_vbatch_variant(1, P(nv), 4, P(d), P(d), None, 6, None) == 1
     assert bf.lib.blasfeo_dgemm_nt_vbatch_variant(1, P(nv), P(nv), P(nv), 4, 4, 4, 1.0, P(d), P(d), 0.0, P(d), P(d),
                                                   6, None) == 1
+
+
+def test_potrf_dmma_warp_kernel_mixed_sizes_and_bad_pivots(bf, orc):
+    # the one-warp FP64 tensor-core Cholesky (variant 5, n <= 64): every 8-block
+    # padding case, plus indefinite instances whose zero pivots must follow the
+    # reference (L_jj = 0, dA_j = 0, computation continues)
+    import torch
+    rng = np.random.default_rng(123)
+    ns = [1, 2, 3, 7, 8, 9, 15, 16, 17, 31, 33, 40, 47, 55, 63, 64, 64, 20]
+    S = [spd(rng, n) for n in ns]
+    S[-2][10, 10] = -3.0                       # first bad pivot at 10 (or earlier)
+    S[-1] = S[-1] - 40.0 * np.eye(20)          # indefinite from the start
+    dC = [bf.DMat(n, n).pack(s) for n, s in zip(ns, S)]
+    dD = [bf.DMat(n, n) for n in ns]
+    aC, aD = bf.descriptor_array(dC), bf.descriptor_array(dD)
+    info = ivec([-9] * len(ns))
+    st = bf.lib.blasfeo_dpotrf_l_vbatch_variant(len(ns), P(ivec(ns)), max(ns), P(aC), P(aD), P(info), 5, None)
+    assert st == 0
+    torch.cuda.synchronize()
+    inf = info.cpu().numpy()
+    assert (inf[:-2] == 0).all(), inf
+    assert 1 <= inf[-2] <= 11 and inf[-1] >= 1, inf
+    for n, s, d, i in zip(ns, S, dD, inf):
+        hC, hD = host(n, n, s), host(n, n)
+        orc.potrf_l("d", n, hC, 0, 0, hD, 0, 0)
+        ref = np.tril(hD.get())
+        if i == 0:
+            assert relfro(np.tril(d.unpack()), ref) <= 1e-13, n
+            assert relfro(d.diag_array(), hD.diag(n)) <= 1e-13, n
+        else:
+            # same zero pattern on the diagonal from the first bad pivot on
+            got = np.tril(d.unpack())
+            assert (np.diag(got) == 0).sum() == (np.diag(ref) == 0).sum()
+            assert np.allclose(got[: i - 1, : i - 1], ref[: i - 1, : i - 1], rtol=1e-12, atol=1e-12)
