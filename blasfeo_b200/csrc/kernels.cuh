@@ -18,6 +18,12 @@ int dgemm_nt_dmma_launch(int batch, SizeArg sz, int max_m, int max_n, double alp
 int dpotrf_dmma_launch(int batch, SizeArg sz, int max_m, MatArg<double> C, MatArg<double> D, int *info,
                        cudaStream_t s);
 
+// FP64 potrf_l for min_n < n <= max_m beyond shared memory: one CTA per
+// instance, left-looking panels with FP64 tensor-core updates (potrf_ll.cu)
+int dpotrf_ll_max_n();
+int dpotrf_ll_launch(int batch, SizeArg sz, int min_n, int max_m, MatArg<double> C, MatArg<double> D, int *info,
+                     cudaStream_t s);
+
 // D = chol(C) lower, inverse diagonal into D's dA, info (device, may be null)
 template <typename T>
 int potrf_launch(int batch, SizeArg sz, int max_m, MatArg<T> C, MatArg<T> D, int *info, cudaStream_t s,

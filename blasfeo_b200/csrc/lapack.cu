@@ -387,7 +387,14 @@ int potrf_launch(int batch, SizeArg sz, int max_m, MatArg<T> C, MatArg<T> D, int
 	case 3: launch_potrf_smem<T, 512, 1>(batch, sz, smax, pl.total, C, D, info, s); break;
 	default: break;
 	}
-	if (variant >= 4 || max_m > smax) k_potrf_global<T><<<batch, 256, 0, s>>>(sz, C, D, info, variant >= 4 ? 0 : smax);
+	if (variant >= 4 || max_m > smax) {
+		const int min_n = variant >= 4 ? 0 : smax;
+		if constexpr (sizeof(T) == 8) {
+			// FP64 beyond shared memory: blocked, FP64 tensor-core updates
+			if (max_m <= dpotrf_ll_max_n()) return dpotrf_ll_launch(batch, sz, min_n, max_m, C, D, info, s);
+		}
+		k_potrf_global<T><<<batch, 256, 0, s>>>(sz, C, D, info, min_n);
+	}
 	return check_launch();
 }
 template int potrf_launch<double>(int, SizeArg, int, MatArg<double>, MatArg<double>, int *, cudaStream_t, int);

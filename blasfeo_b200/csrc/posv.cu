@@ -20,6 +20,7 @@
 #include <climits>
 
 #include "chol.cuh"
+#include "chol_ll.cuh"
 #include "common.cuh"
 #include "kernels.cuh"
 #include "posv.cuh"
@@ -475,22 +476,29 @@ __global__ void __launch_bounds__(NT, MINB) k_posv(int cls, int max_n, PosvWs ws
 	}
 }
 
-// Global-memory path for systems whose FP64 lower panels exceed shared memory:
-// factor in a per-CTA workspace slot (unblocked right-looking), then one-warp
-// substitutions.
-__global__ void __launch_bounds__(256) k_posv_global(int cls, int max_n, PosvWs ws, const int *__restrict__ nvec,
-                                                     const DevDesc<double> *__restrict__ sA,
-                                                     const DevVec<double> *__restrict__ sb,
-                                                     const DevVec<double> *__restrict__ sx, double *slots,
-                                                     int *info) {
+// Systems whose FP64 lower panels exceed shared memory: the factor goes to a
+// per-CTA workspace slot (panel layout, blocked left-looking with FP64
+// tensor-core updates, chol_ll.cuh), then the two blocked triangular solves
+// read it from there (L2-resident), the right-hand side in shared memory.
+__host__ __device__ inline size_t posv_slot_elems(int max_n) {
+	const size_t p4 = (size_t)(max_n + 3) / 4 * 4;
+	return p4 * p4 + (size_t)(max_n + 15) / 16 * 16;
+}
+constexpr int POSV_GLOBAL_NT = 256;
+__global__ void __launch_bounds__(POSV_GLOBAL_NT, 2)
+    k_posv_global(int cls, int max_n, PosvWs ws, const int *__restrict__ nvec, const DevDesc<double> *__restrict__ sA,
+                  const DevVec<double> *__restrict__ sb, const DevVec<double> *__restrict__ sx, double *slots,
+                  int *info) {
+	extern __shared__ __align__(16) double pg_smem[];
 	__shared__ int s_item, s_bad;
-	__shared__ double s_inv;
-	const int tid = threadIdx.x, nt = blockDim.x;
+	const int tid = threadIdx.x;
 	const int start = ws.start[cls], count = ws.count[cls];
-	const size_t slot_elems = (size_t)max_n * max_n + 2 * (size_t)max_n;
-	double *L = slots + slot_elems * blockIdx.x;  // column-major n x n
-	double *dv = L + (size_t)max_n * max_n;
-	double *wv = dv + max_n;
+	double *y = pg_smem + ll_smem_bytes(max_n) / sizeof(double);
+	PMat<double> L;
+	L.p = slots + posv_slot_elems(max_n) * blockIdx.x;
+	L.cn = (max_n + 3) / 4 * 4;
+	L.d = L.p + (size_t)L.cn * L.cn;
+	L.ri = L.cj = 0;
 	for (;;) {
 		if (tid == 0) {
 			int k = atomicAdd(&ws.counter[cls], 1);
@@ -508,61 +516,17 @@ __global__ void __launch_bounds__(256) k_posv_global(int cls, int max_n, PosvWs 
 		}
 		PMat<double> a;
 		a.p = sA[sys].pA;
+		a.d = nullptr;
 		a.cn = sA[sys].cn;
 		a.ri = a.cj = 0;
-		{
-			const int warp = tid >> 5, lane = tid & 31, nw = nt >> 5;
-			for (int j = warp; j < n; j += nw)
-				for (int i = j + lane; i < n; i += 32) L[(size_t)j * n + i] = a.at(i, j);
-		}
-		__syncthreads();
-		for (int j = 0; j < n; j++) {
-			if (tid == 0) {
-				double d, inv;
-				double c = L[(size_t)j * n + j];
-				chol_pivot(c, d, inv);
-				if (!(c > 0.0) && s_bad == 0) s_bad = j + 1;
-				L[(size_t)j * n + j] = d;
-				dv[j] = inv;
-				s_inv = inv;
-			}
-			__syncthreads();
-			for (int i = j + 1 + tid; i < n; i += nt) L[(size_t)j * n + i] *= s_inv;
-			__syncthreads();
-			{
-				const int warp = tid >> 5, lane = tid & 31, nw = nt >> 5;
-				const double *lj = L + (size_t)j * n;
-				for (int l = j + 1 + warp; l < n; l += nw) {
-					const double ljl = lj[l];
-					double *col = L + (size_t)l * n;
-					for (int i = l + lane; i < n; i += 32) col[i] = fma(-lj[i], ljl, col[i]);
-				}
-			}
-			__syncthreads();
-		}
-		// solves by warp 0
-		if (tid < 32) {
-			const double *bg = sb[sys].pa;
-			for (int i = tid; i < n; i += 32) wv[i] = bg[i];
-			__syncwarp();
-			for (int j = 0; j < n; j++) {
-				double zj = wv[j] * dv[j];
-				__syncwarp();
-				for (int i = j + 1 + tid; i < n; i += 32) wv[i] = fma(-L[(size_t)j * n + i], zj, wv[i]);
-				if (tid == 0) wv[j] = zj;
-				__syncwarp();
-			}
-			for (int j = n - 1; j >= 0; j--) {
-				double zj = wv[j] * dv[j];
-				__syncwarp();
-				for (int i = tid; i < j; i += 32) wv[i] = fma(-L[(size_t)i * n + j], zj, wv[i]);
-				if (tid == 0) wv[j] = zj;
-				__syncwarp();
-			}
-			double *xg = sx[sys].pa;
-			for (int i = tid; i < n; i += 32) xg[i] = wv[i];
-			if (tid == 0 && info) info[sys] = s_bad;
-		}
+		const double *bg = sb[sys].pa;
+		for (int i = tid; i < n; i += POSV_GLOBAL_NT) y[i] = bg[i];
+		chol_ll<POSV_GLOBAL_NT>(a, L, n, pg_smem, &s_bad);
+		trsv_ll_fwd<POSV_GLOBAL_NT>(L, n, y);
+		trsv_ll_bwd<POSV_GLOBAL_NT>(L, n, y);
+		double *xg = sx[sys].pa;
+		for (int i = tid; i < n; i += POSV_GLOBAL_NT) xg[i] = y[i];
+		if (tid == 0 && info) info[sys] = s_bad;
 		__syncthreads();
 	}
 }
@@ -628,10 +592,11 @@ int posv_run(int batch, const int *n, int max_n, const void *sA, const void *sb,
 	ct.nclass = nc;
 	for (int c = 0; c < nc; c++) ct.upper[c] = cfg[c].upper;
 
+	if (need_global && max_n > bf::dpotrf_ll_max_n()) return BLASFEO_B200_ENOTSUP;
 	// workspace
 	const int gslots = need_global ? 2 * bf::num_sms() : 0;
 	size_t need = a16((size_t)batch * sizeof(int)) + 4 * a16(POSV_MAX_CLASSES * sizeof(int));
-	size_t slot_bytes = ((size_t)max_n * max_n + 2 * (size_t)max_n) * sizeof(double);
+	size_t slot_bytes = posv_slot_elems(max_n) * sizeof(double);
 	size_t slots_off = need;
 	need += (size_t)gslots * slot_bytes;
 	// refinement slots of the mixed kernel: one per resident CTA of the largest class
@@ -665,9 +630,12 @@ int posv_run(int batch, const int *n, int max_n, const void *sA, const void *sb,
 	for (int c = 0; c < nc; c++) {
 		const bool glob = need_global && c == nc - 1;
 		if (glob) {
-			k_posv_global<<<gslots, 256, 0, s>>>(c, max_n, ws, n, (const DevDesc<double> *)sA,
-			                                     (const DevVec<double> *)sb, (const DevVec<double> *)sx,
-			                                     (double *)(wsp + slots_off), info);
+			const size_t gsm = ll_smem_bytes(max_n) + (size_t)max_n * sizeof(double);
+			if (gsm > 48 * 1024)
+				cudaFuncSetAttribute(k_posv_global, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)gsm);
+			k_posv_global<<<gslots, POSV_GLOBAL_NT, gsm, s>>>(c, max_n, ws, n, (const DevDesc<double> *)sA,
+			                                                  (const DevVec<double> *)sb, (const DevVec<double> *)sx,
+			                                                  (double *)(wsp + slots_off), info);
 		} else if (MIXED && !use_slots && cfg[c].upper <= 256 && tensor_engine()) {
 			const int st = bf::posv_tc_launch(c, cfg[c].upper, batch, ws, n, sA, sb, sx, max_iter, tol, iters, berr,
 			                                  info, s);
