@@ -22,8 +22,9 @@
 //      its factorization in FP64 registers (pivot rule of
 //      kernel/generic/kernel_dgemm_4x4_lib4.c:5700-5710: c>0 -> sqrt(c) and its
 //      reciprocal, else 0 and 0) and its explicit inverse in FP64;
-//      all other warps: rank-16 update of the rest of the trailing matrix
-//      (one 4x4 tile per thread), which hides the serial diagonal work.
+//      the warps on the other three schedulers: rank-16 update of the rest of
+//      the trailing matrix (one 4x4 tile per thread), which hides the serial
+//      diagonal work.
 // The inverses of the diagonal blocks are kept (invL_all) for the triangular
 // solves of the refinement loop.
 #pragma once
@@ -366,8 +367,13 @@ __device__ void chol_smem(T *S, int n, double *dinv, T *Lt, int *bad, T *invL_al
 		const int ndiag = ntiles < 10 ? ntiles : 10;
 		if (warp == 0) {
 			chol_diag_update_factor<T>(S, c0 + CHOL_NB, min(CHOL_NB, n - c0 - CHOL_NB), c0, dinv, Lt, bad);
-		} else {
-			for (int t = ndiag + tid - 32; t < ntiles; t += nt - 32) {
+		} else if (warp & 3) {
+			// warps 4, 8, ... share warp 0's scheduler (warp w issues from
+			// sub-partition w % 4): they sit the update out so that the serial
+			// diagonal chain keeps its issue slots
+			const int nupd = ((nt >> 5) - ((nt >> 5) + 3) / 4) * 32;
+			const int urank = (warp - (warp >> 2) - 1) * 32 + lane;
+			for (int t = ndiag + urank; t < ntiles; t += nupd) {
 				int ti, tj;
 				tri_index(t, ti, tj);
 				chol_tile_update<T>(S, ti + k0 + 4, tj + k0 + 4, c0);

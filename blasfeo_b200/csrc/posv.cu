@@ -300,27 +300,30 @@ __device__ void sym_residual(const double *base, int cn, int n, const double *b,
 			if (NORM) asum[i] = lane == 0 ? rabs[0] : (lane == 1 ? rabs[1] : (lane == 2 ? rabs[2] : rabs[3]));
 		}
 	}
-	// column parts: fixed-order tree over the warps, then warp 0 adds them to r
-	for (int half = nw >> 1; half >= 1; half >>= 1) {
-		if (warp >= half && warp < 2 * half) {
-			double *d = red + ((size_t)(warp - half) * 32 + lane) * 8;
+	// column parts: fixed-order tree over the warps (one tree per accumulated
+	// quantity), then warp 0 adds them to r / asum
 #pragma unroll
-			for (int m = 0; m < 2; m++)
+	for (int pass = 0; pass < 2; pass++) {
+		if (pass == 0 ? !RES : !NORM) continue;
+		double(&acc)[2][4] = pass == 0 ? cacc : cabs;
+		for (int half = nw >> 1; half >= 1; half >>= 1) {
+			if (warp >= half && warp < 2 * half) {
+				double *d = red + ((size_t)(warp - half) * 32 + lane) * 8;
 #pragma unroll
-				for (int q = 0; q < 4; q++) d[4 * m + q] = RES ? cacc[m][q] : cabs[m][q];
+				for (int m = 0; m < 2; m++)
+#pragma unroll
+					for (int q = 0; q < 4; q++) d[4 * m + q] = acc[m][q];
+			}
+			__syncthreads();
+			if (warp < half) {
+				const double *d = red + ((size_t)warp * 32 + lane) * 8;
+#pragma unroll
+				for (int m = 0; m < 2; m++)
+#pragma unroll
+					for (int q = 0; q < 4; q++) acc[m][q] += d[4 * m + q];
+			}
+			__syncthreads();
 		}
-		__syncthreads();
-		if (warp < half) {
-			const double *d = red + ((size_t)warp * 32 + lane) * 8;
-#pragma unroll
-			for (int m = 0; m < 2; m++)
-#pragma unroll
-				for (int q = 0; q < 4; q++) {
-					if (RES) cacc[m][q] += d[4 * m + q];
-					else cabs[m][q] += d[4 * m + q];
-				}
-		}
-		__syncthreads();
 	}
 	if (warp == 0) {
 #pragma unroll
@@ -434,12 +437,17 @@ __global__ void __launch_bounds__(NT, MINB) k_posv(int cls, int max_n, PosvWs ws
 			for (int i = tid; i < n; i += nt) xs[i] += (double)w[i] / scale;
 			__syncthreads();
 			// ||A||_inf (row sums of |A|) once, before the first residual
+			// (the first pass also accumulates the row sums of |A|: one read of A)
 			if (slot) {
-				if (it == 0) sym_residual<true, false, true>(slot, 0, n, bg, xs, rs, asum, red);
-				sym_residual<true, true, false>(slot, 0, n, bg, xs, rs, asum, red);
+				if (it == 0)
+					sym_residual<true, true, true>(slot, 0, n, bg, xs, rs, asum, red);
+				else
+					sym_residual<true, true, false>(slot, 0, n, bg, xs, rs, asum, red);
 			} else {
-				if (it == 0) sym_residual<false, false, true>(a.p, a.cn, n, bg, xs, rs, asum, red);
-				sym_residual<false, true, false>(a.p, a.cn, n, bg, xs, rs, asum, red);
+				if (it == 0)
+					sym_residual<false, true, true>(a.p, a.cn, n, bg, xs, rs, asum, red);
+				else
+					sym_residual<false, true, false>(a.p, a.cn, n, bg, xs, rs, asum, red);
 			}
 			// norms
 			double rm = 0.0, xm = 0.0;
