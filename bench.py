@@ -13,6 +13,8 @@ N(0,1) matrix and log10(lambda) ~ U[0,6], b ~ N(0,1); every system solved to
           in pinned host memory (matrices, right-hand sides, sizes,
           descriptors): the kernels read the lower triangles over the host link
           and write x back to host memory inside the timed region
+  fp64_batched : plain FP64 batched dgemm_nt and dpotrf_l on uniform batches
+          (n = 64, 128, 256, inputs larger than L2) against the FP64 roofline
   cpu_baseline / --impl reference : the reference's own CPU path
           (blasfeo_dpotrf_l + blasfeo_dtrsv_lnn + blasfeo_dtrsv_ltn, BLASFEO
           compiled from source) on the host cores, threads over instances.
@@ -53,6 +55,7 @@ def parse():
     ap.add_argument("--num", type=int, default=NUM)
     ap.add_argument("--cpu-sample", type=int, default=4000)
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--no-fp64", action="store_true", help="skip the FP64 batched dgemm/dpotrf roofline legs")
     return ap.parse_args()
 
 
@@ -330,6 +333,12 @@ def main():
     plain_roof = {"achieved_gflops": flops / (ms_plain * 1e-3) / 1e9, "fp64_peak_gflops": fp64_peak,
                   "frac": flops / (ms_plain * 1e-3) / 1e9 / fp64_peak if fp64_peak > 0 else None,
                   "hbm_frac": bytes_pass / (ms_plain * 1e-3) / 1e9 / peak_bw}
+    fp64 = None
+    if not args.no_fp64:
+        try:
+            fp64 = fp64_batched(lib, torch, dev, stream, fp64_peak, peak_bw)
+        except Exception as ex:  # reported, never silently replaced
+            fp64 = {"error": repr(ex)}
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         try:
@@ -346,13 +355,61 @@ def main():
             "mixed_vs_plain": value / plain_value,
             "refinement": {"mean_steps": float(it.mean()), "max_steps": int(it.max()), "max_berr": float(be.max()),
                            "sampled_host_residual": worst, "sampled_host_residual_plain": worst_plain},
-            "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "clocks": clocks,
+            "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "clocks": clocks, "fp64_batched": fp64,
             "gpu_launches": (args.steps * nclass) * 2}
     if rank == 0:
         print(json.dumps(line), flush=True)
     if world > 1:
         dist.destroy_process_group()
     return 0
+
+
+def fp64_batched(lib, torch, dev, stream, fp64_peak, peak_bw, sizes=(64, 128, 256)):
+    """Plain FP64 batched dgemm_nt (D = A B^T, beta = 0) and dpotrf_l on uniform
+    batches larger than L2, per size: GFLOP/s (LAPACK flop counts), fraction of
+    the measured FP64 FMA peak and of the roofline min(peak, AI * HBM) with
+    algorithmic bytes = inputs read once + outputs written once (gemm: A, B, D;
+    potrf: lower triangle in and out)."""
+    from blasfeo_b200.workloads import fp64_roofline_batches
+    sh = C.c_void_p(stream.cuda_stream)
+    out = {"peak_gflops": fp64_peak, "peak_source": "blasfeo_b200_measure_fma_peak('d'), same run", "hbm_gbs": peak_bw}
+
+    def tm(fn, reps=5):
+        for _ in range(3):
+            fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(reps):
+            fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / reps
+
+    for n in sizes:
+        w = fp64_roofline_batches(n, device=dev)
+        bg, A, B, D = w["gemm"]
+        ms = tm(lambda: lib.blasfeo_dgemm_nt_batch(bg, n, n, n, 1.0, A.ref, 0, 0, B.ref, 0, 0, 0.0, D.ref, 0, 0, D.ref,
+                                                   0, 0, sh))
+        fl, by = 2.0 * n ** 3 * bg, 3.0 * n * n * 8 * bg
+        g = fl / ms / 1e6
+        roof = min(fp64_peak, fl / by * peak_bw)
+        out["dgemm_nt_n%d" % n] = {"batch": bg, "ms": ms, "gflops": g, "frac_of_peak": g / fp64_peak,
+                                   "roofline_gflops": roof, "frac_of_roofline": g / roof}
+        bp, Cm, L = w["potrf"]
+        info = torch.zeros(bp, dtype=torch.int32, device=dev)
+        ms = tm(lambda: lib.blasfeo_dpotrf_l_batch(bp, n, Cm.ref, 0, 0, L.ref, 0, 0, C.c_void_p(info.data_ptr()), sh))
+        torch.cuda.synchronize()
+        if not bool((info == 0).all().item()):
+            raise RuntimeError("dpotrf_l batch reported a non-positive pivot at n=%d" % n)
+        fl, by = (n ** 3 / 3.0 + n * n / 2.0 + n / 6.0) * bp, 2.0 * n * (n + 1) / 2 * 8 * bp
+        g = fl / ms / 1e6
+        roof = min(fp64_peak, fl / by * peak_bw)
+        out["dpotrf_l_n%d" % n] = {"batch": bp, "ms": ms, "gflops": g, "frac_of_peak": g / fp64_peak,
+                                   "roofline_gflops": roof, "frac_of_roofline": g / roof}
+        del w, A, B, D, Cm, L
+        torch.cuda.empty_cache()
+    return out
 
 
 def run_e2e(args, W, lib, torch, dev, stream, barrier, world):

@@ -145,6 +145,7 @@ _sig("blasfeo_dpotrf_l_vbatch_variant", _i, _i, _vp, _i, _vp, _vp, _vp, _i, _vp)
 _sig("blasfeo_dgetrf_rp_vbatch_variant", _i, _i, _vp, _vp, _i, _i, _vp, _vp, _vp, _i, _vp, _i, _vp)
 _sig("blasfeo_dgeqrf_vbatch_variant", _i, _i, _vp, _vp, _i, _i, _vp, _vp, _i, _vp)
 _sig("blasfeo_dposv_worksize", _sz, _i)
+_sig("blasfeo_dposv_worksize_n", _sz, _i, _i, _i)
 _sig("blasfeo_dposv_l_vbatch", _i, _i, _vp, _i, _vp, _vp, _vp, _vp, _vp, _sz, _vp)
 _sig("blasfeo_dsposv_l_vbatch", _i, _i, _vp, _i, _vp, _vp, _vp, _i, _d, _vp, _vp, _vp, _vp, _sz, _vp)
 _sig("blasfeo_dsposv_l_vbatch_mapped", _i, _i, _vp, _i, _vp, _vp, _vp, _i, _d, _vp, _vp, _vp, _vp, _sz, _vp)

@@ -78,6 +78,7 @@ __device__ void chol_ll(const PMat<double> &c, const PMat<double> &d, int n, dou
 						acc[u][fc][h] = v;
 					}
 			}
+#pragma unroll 2
 			for (int k = 0; k < c0; k += 8) {
 				double a0[4], a1[4];
 				const double b00 = ll_ld(d, c0 + r, k + q, n), b01 = ll_ld(d, c0 + 8 + r, k + q, n);

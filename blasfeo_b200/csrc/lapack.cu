@@ -84,11 +84,12 @@ __device__ void store_lower_panels(const T *S, int n, const PMat<T> &d) {
 // Instances with n <= max_n are factored here; larger ones of a
 // variable-size batch are left to the global-memory kernel.
 template <typename T, int NT, int MINB>
-__global__ void __launch_bounds__(NT, MINB) k_potrf_smem(SizeArg sz, MatArg<T> C, MatArg<T> D, int *info, int max_n) {
+__global__ void __launch_bounds__(NT, MINB)
+    k_potrf_smem(SizeArg sz, MatArg<T> C, MatArg<T> D, int *info, int max_n, int min_n) {
 	extern __shared__ __align__(16) unsigned char smem[];
 	const int b = blockIdx.x;
 	const int n = sz.M(b);
-	if (n <= 0 || n > max_n) return;
+	if (n <= 0 || n > max_n || n <= min_n) return;
 	PotrfSmem pl = potrf_smem_plan<T>(max_n);
 	T *S = (T *)smem;
 	double *dinv = (double *)(smem + pl.dinv_off);
@@ -352,10 +353,10 @@ __global__ void __launch_bounds__(NT) k_geqrf(SizeArg sz, MatArg<T> C, MatArg<T>
 namespace {
 template <typename T, int NT, int MINB>
 void launch_potrf_smem(int batch, SizeArg sz, int max_m, size_t smem, MatArg<T> C, MatArg<T> D, int *info,
-                       cudaStream_t s) {
+                       cudaStream_t s, int min_n = 0) {
 	auto kern = k_potrf_smem<T, NT, MINB>;
 	if (smem > 48 * 1024) cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-	kern<<<batch, NT, smem, s>>>(sz, C, D, info, max_m);
+	kern<<<batch, NT, smem, s>>>(sz, C, D, info, max_m, min_n);
 }
 }  // namespace
 
@@ -363,13 +364,27 @@ namespace bf {
 
 // variant: -1 auto; 0..3: shared memory with 64/128/256/512 threads for the
 // instances that fit (the others in global memory, a second launch);
-// 4: everything in global memory; 5 (FP64, max_m <= 64): one warp per
-// instance on the FP64 tensor cores (potrf_dmma.cu), the auto choice there.
+// 4: everything in global memory (FP64: blocked, FP64 tensor-core updates);
+// 5 (FP64, max_m <= 64): one warp per instance on the FP64 tensor cores
+// (potrf_dmma.cu).  FP64 auto: 5 for n <= 64, 1 for 64 < n <= 128, the
+// blocked global-memory kernel above.
 template <typename T>
 int potrf_launch(int batch, SizeArg sz, int max_m, MatArg<T> C, MatArg<T> D, int *info, cudaStream_t s, int variant) {
 	if (batch <= 0 || max_m <= 0) return BLASFEO_B200_OK;
 	if constexpr (sizeof(T) == 8) {
 		if (max_m <= 64 && (variant < 0 || variant == 5)) return dpotrf_dmma_launch(batch, sz, max_m, C, D, info, s);
+		if (variant < 0 && max_m <= dpotrf_ll_max_n()) {
+			// by size (measured fastest per range): n <= 64 one warp on the FP64
+			// tensor cores, 64 < n <= 128 shared memory with 128 threads, larger
+			// n blocked from L2 with FP64 tensor-core updates; one launch per
+			// range, each kernel skips the instances of the other ranges
+			int st = dpotrf_dmma_launch(batch, sz, 64, C, D, info, s);
+			if (st) return st;
+			const int m2 = max_m < 128 ? max_m : 128;
+			launch_potrf_smem<T, 128, 4>(batch, sz, m2, potrf_smem_plan<T>(m2).total, C, D, info, s, 64);
+			if ((st = check_launch()) || max_m <= 128) return st;
+			return dpotrf_ll_launch(batch, sz, 128, max_m, C, D, info, s);
+		}
 	}
 	if (variant == 5) variant = -1;
 	static int limit_cache[2] = {0, 0};

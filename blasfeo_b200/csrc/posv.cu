@@ -492,8 +492,8 @@ __host__ __device__ inline size_t posv_slot_elems(int max_n) {
 	const size_t p4 = (size_t)(max_n + 3) / 4 * 4;
 	return p4 * p4 + (size_t)(max_n + 15) / 16 * 16;
 }
-constexpr int POSV_GLOBAL_NT = 256;
-__global__ void __launch_bounds__(POSV_GLOBAL_NT, 2)
+constexpr int POSV_GLOBAL_NT = 128;
+__global__ void __launch_bounds__(POSV_GLOBAL_NT, 4)
     k_posv_global(int cls, int max_n, PosvWs ws, const int *__restrict__ nvec, const DevDesc<double> *__restrict__ sA,
                   const DevVec<double> *__restrict__ sb, const DevVec<double> *__restrict__ sx, double *slots,
                   int *info) {
@@ -567,54 +567,77 @@ inline bool tensor_engine() {
 	return e == BLASFEO_B200_POSV_TENSOR || (e == BLASFEO_B200_POSV_DEFAULT && POSV_TENSOR_DEFAULT);
 }
 
+// size classes and workspace layout of one call
+struct PosvLayout {
+	ClassTable ct;
+	PosvClassCfg cfg[POSV_MAX_CLASSES];
+	int nc;
+	bool need_global;
+	int gslots, rslots;
+	size_t need, slots_off, rslots_off;
+};
+
+template <typename T, bool MIXED>
+PosvLayout posv_layout(int batch, int max_n, bool use_slots) {
+	PosvLayout L;
+	// size classes: shared memory and CTA size follow the largest member
+	const size_t smem_cap = bf::max_smem_optin();
+	const int uppers[] = {16, 32, 64, 96, 128, 160, 192, 256};
+	int nc = 0;
+	int smem_limit_n = 0;  // largest n the shared-memory kernel takes
+	for (int v = 4; v <= 4096; v += 4)
+		if (posv_plan<T, MIXED>(v, posv_threads(v)).total <= smem_cap) smem_limit_n = v;
+	// plain FP64: above n = 128 the blocked kernel with FP64 tensor-core
+	// updates (L2-resident factor, 4 systems per SM) beats the shared-memory one
+	if (!MIXED && smem_limit_n > 128) smem_limit_n = 128;
+	for (int u : uppers) {
+		if (nc >= POSV_MAX_CLASSES - 1) break;
+		int uu = u < smem_limit_n ? u : smem_limit_n;
+		if (nc > 0 && uu <= L.cfg[nc - 1].upper) continue;
+		L.cfg[nc].upper = uu;
+		L.cfg[nc].threads = posv_threads(uu);
+		nc++;
+		if (uu >= max_n) break;
+	}
+	L.need_global = max_n > L.cfg[nc - 1].upper;
+	if (L.need_global) {
+		L.cfg[nc].upper = max_n;
+		L.cfg[nc].threads = POSV_GLOBAL_NT;
+		nc++;
+	}
+	L.nc = nc;
+	L.ct.nclass = nc;
+	for (int c = 0; c < nc; c++) L.ct.upper[c] = L.cfg[c].upper;
+	// workspace: work list and class tables, global-path factor slots,
+	// mapped-path refinement slots
+	L.gslots = L.need_global ? 4 * bf::num_sms() : 0;
+	L.need = a16((size_t)batch * sizeof(int)) + 4 * a16(POSV_MAX_CLASSES * sizeof(int));
+	L.slots_off = L.need;
+	L.need += (size_t)L.gslots * posv_slot_elems(max_n) * sizeof(double);
+	L.rslots_off = a16(L.need);
+	L.rslots = 0;
+	if (MIXED && use_slots) {
+		const int per_sm = 16;  // upper bound of resident CTAs per SM over all classes
+		L.rslots = bf::num_sms() * per_sm;
+		L.need = L.rslots_off + (size_t)L.rslots * lp_size(max_n) * sizeof(double);
+	}
+	return L;
+}
+
 template <typename T, bool MIXED>
 int posv_run(int batch, const int *n, int max_n, const void *sA, const void *sb, const void *sx, int max_iter,
              double tol, int *iters, double *berr, int *info, void *work, size_t work_bytes, cudaStream_t s,
              bool use_slots) {
 	if (batch < 0 || !n || !sA || !sb || !sx || max_n < 0) return BLASFEO_B200_EINVAL;
 	if (batch == 0 || max_n == 0) return BLASFEO_B200_OK;
-	// size classes: shared memory and CTA size follow the largest member
-	const size_t smem_cap = bf::max_smem_optin();
-	ClassTable ct;
-	PosvClassCfg cfg[POSV_MAX_CLASSES];
-	const int uppers[] = {16, 32, 64, 96, 128, 160, 192, 256};
-	int nc = 0;
-	int smem_limit_n = 0;  // largest n the shared-memory kernel takes
-	for (int v = 4; v <= 4096; v += 4)
-		if (posv_plan<T, MIXED>(v, posv_threads(v)).total <= smem_cap) smem_limit_n = v;
-	for (int u : uppers) {
-		if (nc >= POSV_MAX_CLASSES - 1) break;
-		int uu = u < smem_limit_n ? u : smem_limit_n;
-		if (nc > 0 && uu <= cfg[nc - 1].upper) continue;
-		cfg[nc].upper = uu;
-		cfg[nc].threads = posv_threads(uu);
-		nc++;
-		if (uu >= max_n) break;
-	}
-	bool need_global = max_n > cfg[nc - 1].upper;
-	if (need_global) {
-		cfg[nc].upper = max_n;
-		cfg[nc].threads = 256;
-		nc++;
-	}
-	ct.nclass = nc;
-	for (int c = 0; c < nc; c++) ct.upper[c] = cfg[c].upper;
-
+	const PosvLayout lay = posv_layout<T, MIXED>(batch, max_n, use_slots);
+	const PosvClassCfg *cfg = lay.cfg;
+	const ClassTable ct = lay.ct;
+	const int nc = lay.nc;
+	const bool need_global = lay.need_global;
 	if (need_global && max_n > bf::dpotrf_ll_max_n()) return BLASFEO_B200_ENOTSUP;
-	// workspace
-	const int gslots = need_global ? 2 * bf::num_sms() : 0;
-	size_t need = a16((size_t)batch * sizeof(int)) + 4 * a16(POSV_MAX_CLASSES * sizeof(int));
-	size_t slot_bytes = posv_slot_elems(max_n) * sizeof(double);
-	size_t slots_off = need;
-	need += (size_t)gslots * slot_bytes;
-	// refinement slots of the mixed kernel: one per resident CTA of the largest class
-	size_t rslots_off = a16(need);
-	int rslots = 0;
-	if (MIXED && use_slots) {
-		const int per_sm = 16;  // upper bound of resident CTAs per SM over all classes
-		rslots = bf::num_sms() * per_sm;
-		need = rslots_off + (size_t)rslots * lp_size(max_n) * sizeof(double);
-	}
+	const int gslots = lay.gslots, rslots = lay.rslots;
+	const size_t need = lay.need, slots_off = lay.slots_off, rslots_off = lay.rslots_off;
 	char *wsp = (char *)work;
 	if (!wsp) {
 		wsp = (char *)bf::workspace(need, s);
@@ -676,9 +699,13 @@ int posv_run(int batch, const int *n, int max_n, const void *sA, const void *sb,
 extern "C" {
 
 size_t blasfeo_dposv_worksize(int batch) {
-	// list + class tables; the global-memory slots of very large systems are
-	// sized separately by the library workspace when work == NULL
+	// list + class tables (enough for every system that takes a shared-memory kernel)
 	return a16((size_t)(batch > 0 ? batch : 0) * sizeof(int)) + 4 * a16(POSV_MAX_CLASSES * sizeof(int));
+}
+
+size_t blasfeo_dposv_worksize_n(int batch, int max_n, int mixed) {
+	if (batch < 0 || max_n <= 0) return blasfeo_dposv_worksize(batch);
+	return mixed ? posv_layout<float, true>(batch, max_n, false).need : posv_layout<double, false>(batch, max_n, false).need;
 }
 
 int blasfeo_dposv_l_vbatch(int batch, const int *n, int max_n, const struct blasfeo_dmat *sA,

@@ -6,9 +6,11 @@
 
 namespace {
 
-constexpr int LL_NT = 256;
+// 128 threads, 4 resident CTAs per SM: the serial panel chain of one instance
+// is hidden behind the other instances on the SM
+constexpr int LL_NT = 128;
 
-__global__ void __launch_bounds__(LL_NT, 2)
+__global__ void __launch_bounds__(LL_NT, 4)
     k_potrf_ll(SizeArg sz, MatArg<double> C, MatArg<double> D, int *info, int min_n, int max_n) {
 	extern __shared__ __align__(16) double ll_smem[];
 	__shared__ int s_bad;

@@ -144,3 +144,35 @@ def spd_config3(num=20000, nmin=4, nmax=256, logcond=6.0, seed=0, device="cuda")
         mats[int(n)] = (idx, A)
     rhs = [rng.standard_normal(int(n)) for n in ns]
     return SpdBatch(ns, mats, rhs, device=device)
+
+
+def fill_batch(B, X):
+    """Write a (batch, m, n) FP64 tensor into the uniform-batch slab B (api.DMatBatch), on the device."""
+    b = X.shape[0]
+    pm, cn, st = B.s.pm, B.s.cn, B.s.stride
+    view = B.buf[: b * st * 8].view(X.dtype).view(b, st)
+    view[:, : pm * cn] = to_panel_major(X, pm, cn)
+
+
+def fp64_roofline_batches(n, target_bytes=2.0e9, seed=0, device="cuda"):
+    """Uniform batches for the FP64 batched-routine rooflines at size n (inputs
+    larger than L2): gemm_nt operands A, B (U[-1,1]) and output D; potrf_l
+    input C = G G^T / n + I (G ~ N(0,1)) and output L."""
+    import torch
+    from .api import DMatBatch
+    g = torch.Generator(device=device)
+    g.manual_seed(seed + n)
+    bg = max(64, int(target_bytes / (3 * n * n * 8)))
+    A, B, D = DMatBatch(n, n, bg), DMatBatch(n, n, bg), DMatBatch(n, n, bg)
+    fill_batch(A, torch.rand((bg, n, n), generator=g, dtype=torch.float64, device=device) * 2 - 1)
+    fill_batch(B, torch.rand((bg, n, n), generator=g, dtype=torch.float64, device=device) * 2 - 1)
+    bp = max(64, int(target_bytes / (2 * n * n * 8)))
+    Cm, L = DMatBatch(n, n, bp), DMatBatch(n, n, bp)
+    pm, cn, st = Cm.s.pm, Cm.s.cn, Cm.s.stride
+    slab = Cm.buf[: bp * st * 8].view(torch.float64).view(bp, st)
+    for s0 in range(0, bp, 4096):
+        s1 = min(bp, s0 + 4096)
+        G = torch.randn((s1 - s0, n, n), generator=g, dtype=torch.float64, device=device)
+        S = G @ G.transpose(1, 2) / n + torch.eye(n, dtype=torch.float64, device=device)
+        slab[s0:s1, : pm * cn] = to_panel_major(S, pm, cn)
+    return {"gemm": (bg, A, B, D), "potrf": (bp, Cm, L)}

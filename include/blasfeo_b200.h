@@ -269,9 +269,13 @@ int blasfeo_dgeqrf_vbatch_variant(int batch, const int *m, const int *n, int max
  *           or max_iter refinement steps; iters[b] / berr[b] (device, may be NULL)
  *           receive the step count and final backward error; info[b] = -1 when
  *           refinement did not reach tol.
- * work/work_bytes: device workspace (size from blasfeo_dposv_worksize); NULL
- * uses a library-owned workspace. */
+ * work/work_bytes: device workspace; NULL uses a library-owned workspace.
+ * blasfeo_dposv_worksize_n(batch, max_n, mixed) gives its size for a call
+ * (mixed = 1: dsposv); blasfeo_dposv_worksize(batch) is the size when every
+ * system fits a shared-memory kernel (dsposv with n <= 256, dposv with
+ * n <= 128); larger plain systems also need per-CTA factor slots. */
 size_t blasfeo_dposv_worksize(int batch);
+size_t blasfeo_dposv_worksize_n(int batch, int max_n, int mixed);
 int blasfeo_dposv_l_vbatch(int batch, const int *n, int max_n, const struct blasfeo_dmat *sA,
 	const struct blasfeo_dvec *sb, const struct blasfeo_dvec *sx, int *info,
 	void *work, size_t work_bytes, void *stream);

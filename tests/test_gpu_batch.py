@@ -277,3 +277,35 @@ def test_posv_vbatch(bf, orc, mixed):
             xr = hx.get()
             # two backward-stable solvers differ by ~cond*eps in x
             assert relfro(x, xr) <= 1e-6
+
+
+@pytest.mark.parametrize("mixed", [False, True])
+def test_posv_vbatch_caller_workspace(bf, mixed):
+    # a caller-provided workspace of blasfeo_dposv_worksize_n bytes is enough
+    # (plain systems above n = 128 take the blocked path with per-CTA factor
+    # slots), one byte less is rejected before any device work
+    import torch
+    rng = np.random.default_rng(91)
+    ns = [3, 100, 129, 200, 256, 57]
+    As, bs, mats, bvecs, xvecs = _posv_inputs(bf, rng, ns)
+    dA, db, dx = bf.descriptor_array(mats), bf.vector_array(bvecs), bf.vector_array(xvecs)
+    nb = len(ns)
+    nv = torch.tensor(ns, dtype=torch.int32, device="cuda")
+    info = torch.full((nb,), -9, dtype=torch.int32, device="cuda")
+    P = lambda t: C.c_void_p(t.data_ptr())
+    need = bf.lib.blasfeo_dposv_worksize_n(nb, max(ns), 1 if mixed else 0)
+    assert need >= bf.lib.blasfeo_dposv_worksize(nb)
+    work = torch.zeros(need, dtype=torch.uint8, device="cuda")
+
+    def call(nbytes):
+        if mixed:
+            return bf.lib.blasfeo_dsposv_l_vbatch(nb, P(nv), max(ns), P(dA), P(db), P(dx), 30, 1e-12, None, None,
+                                                  P(info), P(work), nbytes, None)
+        return bf.lib.blasfeo_dposv_l_vbatch(nb, P(nv), max(ns), P(dA), P(db), P(dx), P(info), P(work), nbytes, None)
+    assert call(need - 1) == 3  # BLASFEO_B200_ENOMEM
+    assert call(need) == 0
+    sync()
+    assert (info.cpu().numpy() == 0).all()
+    for n, a, b, xv in zip(ns, As, bs, xvecs):
+        x = xv.unpack()
+        assert np.abs(b - a @ x).max() / (np.abs(a).sum(1).max() * np.abs(x).max()) <= 1e-12, n
