@@ -75,7 +75,7 @@ __device__ __forceinline__ void stage_operand(double *dst, const PMat<double> &a
 template <int BM, int BN, bool LOWER>
 __global__ void __launch_bounds__((BM / 32) * (BN / 32) * 32)
     k_dgemm_nt_dmma(SizeArg sz, double alpha, MatArg<double> A, MatArg<double> B, double beta, MatArg<double> C,
-                    MatArg<double> D, int tiles_n) {
+                    MatArg<double> D, int tiles_n, int tiles_mn) {
 	constexpr int WN = BN / 32;
 	constexpr int NT = (BM / 32) * WN * 32;
 	constexpr int SA = BM * DM_BK, SB = BN * DM_BK;  // doubles per stage
@@ -83,9 +83,12 @@ __global__ void __launch_bounds__((BM / 32) * (BN / 32) * 32)
 	double *sA = dm_smem;
 	double *sB = dm_smem + DM_STAGES * SA;
 
-	const int b = blockIdx.x;
+	// one-dimensional grid with the output tiles of one instance consecutive:
+	// the CTAs that share an instance's A and B slices run together and meet in L2
+	const int b = (int)(blockIdx.x / (unsigned)tiles_mn);
+	const int tile = (int)(blockIdx.x % (unsigned)tiles_mn);
 	const int m = sz.M(b), n = sz.N(b), k = sz.K(b);
-	const int tmi = blockIdx.y / tiles_n, tni = blockIdx.y % tiles_n;
+	const int tmi = tile / tiles_n, tni = tile % tiles_n;
 	const int i0 = tmi * BM, j0 = tni * BN;
 	if (i0 >= m || j0 >= n) return;
 	if (LOWER && j0 > i0 + BM - 1) return;
@@ -176,8 +179,9 @@ int launch_dmma(int batch, SizeArg sz, int max_m, int max_n, double alpha, MatAr
 	auto kern = k_dgemm_nt_dmma<BM, BN, LOWER>;
 	if (smem > 48 * 1024) cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
 	const int tm = cdiv(max_m, BM), tn = cdiv(max_n, BN);
-	dim3 grid(batch, tm * tn);
-	kern<<<grid, NT, smem, s>>>(sz, alpha, A, B, beta, C, D, tn);
+	const long long ctas = (long long)batch * tm * tn;
+	if (ctas > 0x7fffffffLL) return BLASFEO_B200_ENOTSUP;
+	kern<<<(unsigned)ctas, NT, smem, s>>>(sz, alpha, A, B, beta, C, D, tn, tm * tn);
 	return bf::check_launch();
 }
 
