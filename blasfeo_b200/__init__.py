@@ -120,6 +120,10 @@ for p, M, V, R in (("d", _DM, _DV, _d), ("s", _SM, _SV, _f)):
     _sig("blasfeo_%sgetrf_rp" % p, None, _i, _i, M, _i, _i, M, _i, _i, P(_i))
     _sig("blasfeo_%sgeqrf_worksize" % p, _i, _i, _i)
     _sig("blasfeo_%sgeqrf" % p, None, _i, _i, M, _i, _i, M, _i, _i, _vp)
+    _sig("blasfeo_%ssyrk_ln_mn" % p, None, _i, *_syrk_args(M, R))
+    _sig("blasfeo_%strsm_rltu" % p, None, *_trsm_args(M, R))
+    _sig("blasfeo_%spotrf_l_mn" % p, None, _i, _i, M, _i, _i, M, _i, _i)
+    _sig("blasfeo_%sgetrf_np" % p, None, _i, _i, M, _i, _i, M, _i, _i)
 _sig("blasfeo_dgemv_n", None, _i, _i, _d, _DM, _i, _i, _DV, _i, _d, _DV, _i, _DV, _i)
 _sig("blasfeo_dtrsv_lnn", None, _i, _DM, _i, _i, _DV, _i, _DV, _i)
 _sig("blasfeo_dtrsv_ltn", None, _i, _DM, _i, _i, _DV, _i, _DV, _i)
@@ -135,6 +139,10 @@ for p, B, R, M in (("d", _DB, _d, _DM), ("s", _SB, _f, _SM)):
          _vp, _vp)
     _sig("blasfeo_%sgetrf_rp_batch" % p, _i, _i, _i, _i, B, _i, _i, B, _i, _i, _vp, _vp, _vp)
     _sig("blasfeo_%sgeqrf_batch" % p, _i, _i, _i, _i, B, _i, _i, B, _i, _i, _vp)
+    _sig("blasfeo_%ssyrk_ln_mn_batch" % p, _i, _i, _i, *(_syrk_args(B, R) + [_vp]))
+    _sig("blasfeo_%strsm_rltu_batch" % p, _i, _i, *(_trsm_args(B, R) + [_vp]))
+    _sig("blasfeo_%spotrf_l_mn_batch" % p, _i, _i, _i, _i, B, _i, _i, B, _i, _i, _vp, _vp)
+    _sig("blasfeo_%sgetrf_np_batch" % p, _i, _i, _i, _i, B, _i, _i, B, _i, _i, _vp, _vp)
 _sig("blasfeo_dgemm_nt_vbatch", _i, _i, _vp, _vp, _vp, _i, _i, _i, _d, _vp, _vp, _d, _vp, _vp, _vp)
 _sig("blasfeo_dpotrf_l_vbatch", _i, _i, _vp, _i, _vp, _vp, _vp, _vp)
 _sig("blasfeo_dgetrf_rp_vbatch", _i, _i, _vp, _vp, _i, _i, _vp, _vp, _vp, _i, _vp, _vp)

@@ -26,6 +26,8 @@ __all__ = [
     "blasfeo_ssyrk_spotrf_ln", "blasfeo_sgetrf_rp", "blasfeo_sgeqrf", "blasfeo_sgeqrf_worksize",
     "blasfeo_dgecp", "blasfeo_ddiare", "blasfeo_drowsw", "blasfeo_dgemv_n", "blasfeo_dtrsv_lnn",
     "blasfeo_dtrsv_ltn", "descriptor_array", "vector_array",
+    "blasfeo_dsyrk_ln_mn", "blasfeo_dtrsm_rltu", "blasfeo_dpotrf_l_mn", "blasfeo_dgetrf_np",
+    "blasfeo_ssyrk_ln_mn", "blasfeo_strsm_rltu", "blasfeo_spotrf_l_mn", "blasfeo_sgetrf_np",
 ]
 
 
@@ -250,7 +252,7 @@ def _wrap(name):
 
 for _p in ("d", "s"):
     for _r in ("gemm_nt", "syrk_ln", "trsm_rltn", "trmm_rlnn", "potrf_l", "geqrf_worksize", "gecp", "diare",
-               "rowsw"):
+               "rowsw", "syrk_ln_mn", "trsm_rltu", "potrf_l_mn", "getrf_np"):
         globals()["blasfeo_%s%s" % (_p, _r)] = _wrap("blasfeo_%s%s" % (_p, _r))
     globals()["blasfeo_%ssyrk_%spotrf_ln" % (_p, _p)] = _wrap("blasfeo_%ssyrk_%spotrf_ln" % (_p, _p))
 for _r in ("dgemv_n", "dtrsv_lnn", "dtrsv_ltn"):

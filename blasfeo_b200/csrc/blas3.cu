@@ -146,10 +146,12 @@ __global__ void k_invdiag(SizeArg sz, MatArg<T> A) {
 	a.d[l] = T(1) / a.at(l, l);
 }
 
-// D = alpha * B * A^{-T}, A lower non-unit: one thread per row of D, columns
-// left to right, each column multiplied by the cached inverse diagonal
-// (kernel/generic/kernel_dgemm_4x4_lib4.c:5970 kernel_dtrsm_nt_rl_inv).
-template <typename T>
+// D = alpha * B * A^{-T}, A lower: one thread per row of D, columns left to
+// right; non-unit (trsm_rltn) multiplies each column by the cached inverse
+// diagonal (kernel/generic/kernel_dgemm_4x4_lib4.c:5970
+// kernel_dtrsm_nt_rl_inv), unit (trsm_rltu, blasfeo_ref/x_blas3_ref.c:1760)
+// takes the diagonal of A as 1 and never reads it.
+template <typename T, bool UNIT>
 __global__ void k_trsm_rltn(SizeArg sz, T alpha, MatArg<T> A, MatArg<T> B, MatArg<T> D) {
 	int b = blockIdx.x;
 	int m = sz.M(b), n = sz.N(b);
@@ -160,7 +162,7 @@ __global__ void k_trsm_rltn(SizeArg sz, T alpha, MatArg<T> A, MatArg<T> B, MatAr
 	for (int j = 0; j < n; j++) {
 		T c = alpha * bb.at(i, j);
 		for (int l = 0; l < j; l++) c = fma(-d.at(i, l), a.at(j, l), c);
-		d.at(i, j) = c * inv[j];
+		d.at(i, j) = UNIT ? c : c * inv[j];
 	}
 }
 
@@ -219,15 +221,19 @@ __global__ void k_trsv_l(int m, PMat<T> a, const T *x, T *z) {
 
 template <typename T>
 int trsm_core(int batch, int m, int n, T alpha, MatArg<T> A, int ai, int aj, int *use_dA, MatArg<T> B, MatArg<T> D,
-              cudaStream_t s) {
+              cudaStream_t s, bool unit = false) {
 	SizeArg sz = uniform_sizes(m, n, 0);
+	if (unit) {
+		k_trsm_rltn<T, true><<<dim3(batch, cdiv(m, 64)), 64, 0, s>>>(sz, alpha, A, B, D);
+		return bf::check_launch();
+	}
 	// inverse diagonal of A into A's dA, reused when already valid
 	bool need = !(ai == 0 && aj == 0 && *use_dA >= n);
 	if (need) {
 		k_invdiag<T><<<dim3(batch, cdiv(n, 128)), 128, 0, s>>>(sz, A);
 		*use_dA = (ai == 0 && aj == 0) ? n : 0;
 	}
-	k_trsm_rltn<T><<<dim3(batch, cdiv(m, 64)), 64, 0, s>>>(sz, alpha, A, B, D);
+	k_trsm_rltn<T, false><<<dim3(batch, cdiv(m, 64)), 64, 0, s>>>(sz, alpha, A, B, D);
 	return bf::check_launch();
 }
 
@@ -260,22 +266,23 @@ int gemm_batch(int batch, int m, int n, int k, T alpha, BT *sA, int ai, int aj, 
 }
 
 template <typename T, typename S>
-void trsm_single(int m, int n, T alpha, S *sA, int ai, int aj, S *sB, int bi, int bj, S *sD, int di, int dj) {
+void trsm_single(int m, int n, T alpha, S *sA, int ai, int aj, S *sB, int bi, int bj, S *sD, int di, int dj,
+                 bool unit = false) {
 	if (m <= 0 || n <= 0) return;
 	sD->use_dA = 0;
 	trsm_core<T>(1, m, n, alpha, single_arg<T>(sA, ai, aj), ai, aj, &sA->use_dA, single_arg<T>(sB, bi, bj),
-	             single_arg<T>(sD, di, dj), bf::cur_stream());
+	             single_arg<T>(sD, di, dj), bf::cur_stream(), unit);
 	bf::finish_single();
 }
 
 template <typename T, typename BT>
 int trsm_batch(int batch, int m, int n, T alpha, BT *sA, int ai, int aj, BT *sB, int bi, int bj, BT *sD, int di,
-               int dj, void *stream) {
+               int dj, void *stream, bool unit = false) {
 	if (batch < 0 || !sA || !sB || !sD) return BLASFEO_B200_EINVAL;
 	if (m <= 0 || n <= 0 || batch == 0) return BLASFEO_B200_OK;
 	sD->use_dA = 0;
 	return trsm_core<T>(batch, m, n, alpha, batch_arg<T>(sA, ai, aj), ai, aj, &sA->use_dA, batch_arg<T>(sB, bi, bj),
-	                    batch_arg<T>(sD, di, dj), (cudaStream_t)stream);
+	                    batch_arg<T>(sD, di, dj), (cudaStream_t)stream, unit);
 }
 
 template <typename T, typename S>
@@ -329,6 +336,25 @@ void blasfeo_dtrsm_rltn(int m, int n, double alpha, struct blasfeo_dmat *sA, int
 void blasfeo_strsm_rltn(int m, int n, float alpha, struct blasfeo_smat *sA, int ai, int aj, struct blasfeo_smat *sB,
                         int bi, int bj, struct blasfeo_smat *sD, int di, int dj) {
 	trsm_single<float>(m, n, alpha, sA, ai, aj, sB, bi, bj, sD, di, dj);
+}
+void blasfeo_dtrsm_rltu(int m, int n, double alpha, struct blasfeo_dmat *sA, int ai, int aj, struct blasfeo_dmat *sB,
+                        int bi, int bj, struct blasfeo_dmat *sD, int di, int dj) {
+	trsm_single<double>(m, n, alpha, sA, ai, aj, sB, bi, bj, sD, di, dj, true);
+}
+void blasfeo_strsm_rltu(int m, int n, float alpha, struct blasfeo_smat *sA, int ai, int aj, struct blasfeo_smat *sB,
+                        int bi, int bj, struct blasfeo_smat *sD, int di, int dj) {
+	trsm_single<float>(m, n, alpha, sA, ai, aj, sB, bi, bj, sD, di, dj, true);
+}
+// lower trapezoid (m x n, element (i,j) for j <= i) of D = beta*C + alpha*A*B^T
+void blasfeo_dsyrk_ln_mn(int m, int n, int k, double alpha, struct blasfeo_dmat *sA, int ai, int aj,
+                         struct blasfeo_dmat *sB, int bi, int bj, double beta, struct blasfeo_dmat *sC, int ci, int cj,
+                         struct blasfeo_dmat *sD, int di, int dj) {
+	gemm_single<double>(m, n, k, alpha, sA, ai, aj, sB, bi, bj, beta, sC, ci, cj, sD, di, dj, true);
+}
+void blasfeo_ssyrk_ln_mn(int m, int n, int k, float alpha, struct blasfeo_smat *sA, int ai, int aj,
+                         struct blasfeo_smat *sB, int bi, int bj, float beta, struct blasfeo_smat *sC, int ci, int cj,
+                         struct blasfeo_smat *sD, int di, int dj) {
+	gemm_single<float>(m, n, k, alpha, sA, ai, aj, sB, bi, bj, beta, sC, ci, cj, sD, di, dj, true);
 }
 void blasfeo_dtrmm_rlnn(int m, int n, double alpha, struct blasfeo_dmat *sA, int ai, int aj, struct blasfeo_dmat *sB,
                         int bi, int bj, struct blasfeo_dmat *sD, int di, int dj) {
@@ -388,6 +414,29 @@ int blasfeo_strsm_rltn_batch(int batch, int m, int n, float alpha, struct blasfe
                              struct blasfeo_smat_batch *sB, int bi, int bj, struct blasfeo_smat_batch *sD, int di,
                              int dj, void *stream) {
 	return trsm_batch<float>(batch, m, n, alpha, sA, ai, aj, sB, bi, bj, sD, di, dj, stream);
+}
+
+int blasfeo_dtrsm_rltu_batch(int batch, int m, int n, double alpha, struct blasfeo_dmat_batch *sA, int ai, int aj,
+                             struct blasfeo_dmat_batch *sB, int bi, int bj, struct blasfeo_dmat_batch *sD, int di,
+                             int dj, void *stream) {
+	return trsm_batch<double>(batch, m, n, alpha, sA, ai, aj, sB, bi, bj, sD, di, dj, stream, true);
+}
+int blasfeo_strsm_rltu_batch(int batch, int m, int n, float alpha, struct blasfeo_smat_batch *sA, int ai, int aj,
+                             struct blasfeo_smat_batch *sB, int bi, int bj, struct blasfeo_smat_batch *sD, int di,
+                             int dj, void *stream) {
+	return trsm_batch<float>(batch, m, n, alpha, sA, ai, aj, sB, bi, bj, sD, di, dj, stream, true);
+}
+int blasfeo_dsyrk_ln_mn_batch(int batch, int m, int n, int k, double alpha, struct blasfeo_dmat_batch *sA, int ai,
+                              int aj, struct blasfeo_dmat_batch *sB, int bi, int bj, double beta,
+                              struct blasfeo_dmat_batch *sC, int ci, int cj, struct blasfeo_dmat_batch *sD, int di,
+                              int dj, void *stream) {
+	return gemm_batch<double>(batch, m, n, k, alpha, sA, ai, aj, sB, bi, bj, beta, sC, ci, cj, sD, di, dj, stream, true);
+}
+int blasfeo_ssyrk_ln_mn_batch(int batch, int m, int n, int k, float alpha, struct blasfeo_smat_batch *sA, int ai,
+                              int aj, struct blasfeo_smat_batch *sB, int bi, int bj, float beta,
+                              struct blasfeo_smat_batch *sC, int ci, int cj, struct blasfeo_smat_batch *sD, int di,
+                              int dj, void *stream) {
+	return gemm_batch<float>(batch, m, n, k, alpha, sA, ai, aj, sB, bi, bj, beta, sC, ci, cj, sD, di, dj, stream, true);
 }
 
 int blasfeo_dgemm_nt_vbatch_variant(int batch, const int *m, const int *n, const int *k, int max_m, int max_n,

@@ -150,6 +150,49 @@ __global__ void __launch_bounds__(256) k_potrf_global(SizeArg sz, MatArg<T> C, M
 	if (info && tid == 0) info[b] = s_bad;
 }
 
+// Cholesky of the m x n lower trapezoid (potrf_l_mn, blasfeo_hp_pm/
+// d_lapack_lib4.c:1155; blasfeo_ref/x_lapack_ref.c:185): the first n columns of
+// chol, rows n..m-1 of them solved against the n x n factor; same pivot rule
+// and inverse diagonal as potrf_l.  One CTA per instance, right-looking in
+// global memory (L1/L2 resident at these sizes).
+template <typename T>
+__global__ void __launch_bounds__(256) k_potrf_mn(SizeArg sz, MatArg<T> C, MatArg<T> D, int *info) {
+	__shared__ double s_inv;
+	__shared__ int s_bad;
+	const int b = blockIdx.x;
+	const int m = sz.M(b);
+	const int n = sz.N(b) < m ? sz.N(b) : m;
+	if (m <= 0 || n <= 0) return;
+	const PMat<T> c = C.get(b), d = D.get(b);
+	const int tid = threadIdx.x, nt = blockDim.x;
+	const int warp = tid >> 5, lane = tid & 31, nw = nt >> 5;
+	for (int j = warp; j < n; j += nw)
+		for (int i = j + lane; i < m; i += 32) d.at(i, j) = c.at(i, j);
+	if (tid == 0) s_bad = 0;
+	__syncthreads();
+	for (int j = 0; j < n; j++) {
+		if (tid == 0) {
+			double dd, inv;
+			double cc = (double)d.at(j, j);
+			chol_pivot(cc, dd, inv);
+			if (!(cc > 0.0) && s_bad == 0) s_bad = j + 1;
+			d.at(j, j) = (T)dd;
+			d.d[j] = (T)inv;
+			s_inv = inv;
+		}
+		__syncthreads();
+		const T inv = (T)s_inv;
+		for (int i = j + 1 + tid; i < m; i += nt) d.at(i, j) *= inv;
+		__syncthreads();
+		for (int l = j + 1 + warp; l < n; l += nw) {
+			const T djl = d.at(l, j);
+			for (int i = l + lane; i < m; i += 32) d.at(i, l) = fma(-d.at(i, j), djl, d.at(i, l));
+		}
+		__syncthreads();
+	}
+	if (info && tid == 0) info[b] = s_bad;
+}
+
 // CTA-wide argmax of |x| with first-index tie-break; returns index (valid in all threads)
 template <typename T>
 __device__ int block_argmax_first(T v, int idx, int *s_idx, T *s_val) {
@@ -191,7 +234,7 @@ __device__ int block_argmax_first(T v, int idx, int *s_idx, T *s_val) {
 // do not fit are taken (the other kernel of the launch has the rest).
 template <typename T, int NT, bool SMEM>
 __global__ void __launch_bounds__(NT) k_getrf(SizeArg sz, MatArg<T> C, MatArg<T> D, int *ipiv, long long ipiv_stride,
-                                               int *info, int smem_cap) {
+                                               int *info, int smem_cap, bool piv_on) {
 	extern __shared__ __align__(16) unsigned char smem_raw[];
 	__shared__ int s_idx[33];
 	__shared__ T s_val[32];
@@ -209,7 +252,7 @@ __global__ void __launch_bounds__(NT) k_getrf(SizeArg sz, MatArg<T> C, MatArg<T>
 		d.ri = d.cj = 0;
 	}
 	const int tid = threadIdx.x;
-	int *piv = ipiv + ipiv_stride * b;
+	int *piv = piv_on ? ipiv + ipiv_stride * b : nullptr;
 	const int warp = tid >> 5, lane = tid & 31, nw = NT >> 5;
 	for (int j = warp; j < n; j += nw)
 		for (int i = lane; i < m; i += 32) d.at(i, j) = c.at(i, j);
@@ -217,28 +260,33 @@ __global__ void __launch_bounds__(NT) k_getrf(SizeArg sz, MatArg<T> C, MatArg<T>
 	__syncthreads();
 	const int mn = m < n ? m : n;
 	for (int j = 0; j < mn; j++) {
-		// pivot search over rows j..m-1
-		T best = T(-1);
-		int bi = INT_MAX;
-		for (int i = j + tid; i < m; i += NT) {
-			T a = dev_abs(d.at(i, j));
-			if (a > best) {
-				best = a;
-				bi = i;
+		int ip = j;
+		if (piv_on) {
+			// pivot search over rows j..m-1
+			T best = T(-1);
+			int bi = INT_MAX;
+			for (int i = j + tid; i < m; i += NT) {
+				T a = dev_abs(d.at(i, j));
+				if (a > best) {
+					best = a;
+					bi = i;
+				}
 			}
+			ip = block_argmax_first<T>(best, bi, s_idx, s_val);
+			if (ip != j)
+				for (int l = tid; l < n; l += NT) {
+					T t = d.at(j, l);
+					d.at(j, l) = d.at(ip, l);
+					d.at(ip, l) = t;
+				}
 		}
-		const int ip = block_argmax_first<T>(best, bi, s_idx, s_val);
-		if (ip != j)
-			for (int l = tid; l < n; l += NT) {
-				T t = d.at(j, l);
-				d.at(j, l) = d.at(ip, l);
-				d.at(ip, l) = t;
-			}
 		__syncthreads();
 		const T p = d.at(j, j);
-		const T inv = (p != T(0)) ? T(1) / p : T(0);
+		// getrf_rp: a zero pivot gives inverse 0; getrf_np divides as the
+		// reference does (blasfeo_ref/x_lapack_ref.c, REF_GETRF_NOPIVOT: 1.0/d_00)
+		const T inv = piv_on ? ((p != T(0)) ? T(1) / p : T(0)) : T(1) / p;
 		if (tid == 0) {
-			piv[j] = ip;
+			if (piv_on) piv[j] = ip;
 			dg.d[j] = inv;
 			if (p == T(0) && s_bad == 0) s_bad = j + 1;
 		}
@@ -469,10 +517,10 @@ int syrk_potrf_batch(int batch, int m, int k, BT *sA, int ai, int aj, BT *sB, in
 // the others in global memory (a second launch, 512 threads).
 template <typename T, int NT, bool SMEM>
 void launch_getrf(int batch, SizeArg sz, int cap, size_t smem, MatArg<T> C, MatArg<T> D, int *ipiv,
-                  long long ipiv_stride, int *info, cudaStream_t s) {
+                  long long ipiv_stride, int *info, cudaStream_t s, bool piv = true) {
 	auto kern = k_getrf<T, NT, SMEM>;
 	if (smem > 48 * 1024) cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-	kern<<<batch, NT, smem, s>>>(sz, C, D, ipiv, ipiv_stride, info, cap);
+	kern<<<batch, NT, smem, s>>>(sz, C, D, ipiv, ipiv_stride, info, cap, piv);
 }
 template <typename T, int NT, bool SMEM>
 void launch_geqrf(int batch, SizeArg sz, int cap, size_t smem, MatArg<T> C, MatArg<T> D, cudaStream_t s) {
@@ -495,21 +543,21 @@ inline int pick_lu_variant(int variant, int max_m, int max_n) {
 
 template <typename T>
 int getrf_launch(int batch, SizeArg sz, MatArg<T> C, MatArg<T> D, int *ipiv, long long ipiv_stride, int *info,
-                 cudaStream_t s, int max_m, int max_n, int variant = -1) {
+                 cudaStream_t s, int max_m, int max_n, int variant = -1, bool piv = true) {
 	const size_t cap_full = bf::max_smem_optin() - 1024;
 	const size_t need = lu_smem_bytes(max_m, max_n, sizeof(T));
 	const size_t smem = need < cap_full ? need : cap_full;
 	const int cap = (int)smem;
 	variant = pick_lu_variant(variant, max_m, max_n);
 	switch (variant) {
-	case 0: launch_getrf<T, 128, false>(batch, sz, -1, 0, C, D, ipiv, ipiv_stride, info, s); break;
-	case 1: launch_getrf<T, 256, false>(batch, sz, -1, 0, C, D, ipiv, ipiv_stride, info, s); break;
-	case 2: launch_getrf<T, 512, false>(batch, sz, -1, 0, C, D, ipiv, ipiv_stride, info, s); break;
-	case 3: launch_getrf<T, 128, true>(batch, sz, cap, smem, C, D, ipiv, ipiv_stride, info, s); break;
-	case 4: launch_getrf<T, 256, true>(batch, sz, cap, smem, C, D, ipiv, ipiv_stride, info, s); break;
-	default: launch_getrf<T, 512, true>(batch, sz, cap, smem, C, D, ipiv, ipiv_stride, info, s); break;
+	case 0: launch_getrf<T, 128, false>(batch, sz, -1, 0, C, D, ipiv, ipiv_stride, info, s, piv); break;
+	case 1: launch_getrf<T, 256, false>(batch, sz, -1, 0, C, D, ipiv, ipiv_stride, info, s, piv); break;
+	case 2: launch_getrf<T, 512, false>(batch, sz, -1, 0, C, D, ipiv, ipiv_stride, info, s, piv); break;
+	case 3: launch_getrf<T, 128, true>(batch, sz, cap, smem, C, D, ipiv, ipiv_stride, info, s, piv); break;
+	case 4: launch_getrf<T, 256, true>(batch, sz, cap, smem, C, D, ipiv, ipiv_stride, info, s, piv); break;
+	default: launch_getrf<T, 512, true>(batch, sz, cap, smem, C, D, ipiv, ipiv_stride, info, s, piv); break;
 	}
-	if (variant >= 3 && need > smem) launch_getrf<T, 512, false>(batch, sz, cap, 0, C, D, ipiv, ipiv_stride, info, s);
+	if (variant >= 3 && need > smem) launch_getrf<T, 512, false>(batch, sz, cap, 0, C, D, ipiv, ipiv_stride, info, s, piv);
 	return bf::check_launch();
 }
 
@@ -566,6 +614,46 @@ int getrf_batch(int batch, int m, int n, BT *sC, int ci, int cj, BT *sD, int di,
 	int mn = m < n ? m : n;
 	return getrf_launch<T>(batch, uniform_sizes(m, n, 0), batch_arg<T>(sC, ci, cj), batch_arg<T>(sD, di, dj), ipiv, mn,
 	                       info, (cudaStream_t)stream, m, n);
+}
+
+// LU without pivoting (getrf_np, blasfeo_hp_pm/d_lapack_lib4.c:2078)
+template <typename T, typename S>
+void getrf_np_single(int m, int n, S *sC, int ci, int cj, S *sD, int di, int dj) {
+	if (m <= 0 || n <= 0) return;
+	sD->use_dA = (di == 0 && dj == 0) ? 1 : 0;
+	getrf_launch<T>(1, uniform_sizes(m, n, 0), single_arg<T>(sC, ci, cj), single_arg<T>(sD, di, dj), nullptr, 0, nullptr,
+	                bf::cur_stream(), m, n, -1, false);
+	bf::finish_single();
+}
+
+template <typename T, typename BT>
+int getrf_np_batch(int batch, int m, int n, BT *sC, int ci, int cj, BT *sD, int di, int dj, int *info, void *stream) {
+	if (batch < 0 || !sC || !sD) return BLASFEO_B200_EINVAL;
+	if (m <= 0 || n <= 0 || batch == 0) return BLASFEO_B200_OK;
+	sD->use_dA = (di == 0 && dj == 0) ? 1 : 0;
+	return getrf_launch<T>(batch, uniform_sizes(m, n, 0), batch_arg<T>(sC, ci, cj), batch_arg<T>(sD, di, dj), nullptr, 0,
+	                       info, (cudaStream_t)stream, m, n, -1, false);
+}
+
+// potrf_l_mn: use_dA = 1 with zero offsets, as blasfeo_hp_dpotrf_l_mn sets it
+// (blasfeo_hp_pm/d_lapack_lib4.c:1184-1187)
+template <typename T, typename S>
+void potrf_mn_single(int m, int n, S *sC, int ci, int cj, S *sD, int di, int dj) {
+	if (m <= 0 || n <= 0) return;
+	sD->use_dA = (di == 0 && dj == 0) ? 1 : 0;
+	k_potrf_mn<T><<<1, 256, 0, bf::cur_stream()>>>(uniform_sizes(m, n, 0), single_arg<T>(sC, ci, cj),
+	                                                single_arg<T>(sD, di, dj), nullptr);
+	bf::finish_single();
+}
+
+template <typename T, typename BT>
+int potrf_mn_batch(int batch, int m, int n, BT *sC, int ci, int cj, BT *sD, int di, int dj, int *info, void *stream) {
+	if (batch < 0 || !sC || !sD) return BLASFEO_B200_EINVAL;
+	if (m <= 0 || n <= 0 || batch == 0) return BLASFEO_B200_OK;
+	sD->use_dA = (di == 0 && dj == 0) ? 1 : 0;
+	k_potrf_mn<T><<<batch, 256, 0, (cudaStream_t)stream>>>(uniform_sizes(m, n, 0), batch_arg<T>(sC, ci, cj),
+	                                                         batch_arg<T>(sD, di, dj), info);
+	return bf::check_launch();
 }
 
 template <typename T, typename S>
@@ -631,6 +719,35 @@ void blasfeo_sgeqrf(int m, int n, struct blasfeo_smat *sC, int ci, int cj, struc
                     void *work) {
 	(void)work;
 	geqrf_single<float>(m, n, sC, ci, cj, sD, di, dj);
+}
+
+void blasfeo_dpotrf_l_mn(int m, int n, struct blasfeo_dmat *sC, int ci, int cj, struct blasfeo_dmat *sD, int di, int dj) {
+	potrf_mn_single<double>(m, n, sC, ci, cj, sD, di, dj);
+}
+void blasfeo_spotrf_l_mn(int m, int n, struct blasfeo_smat *sC, int ci, int cj, struct blasfeo_smat *sD, int di, int dj) {
+	potrf_mn_single<float>(m, n, sC, ci, cj, sD, di, dj);
+}
+void blasfeo_dgetrf_np(int m, int n, struct blasfeo_dmat *sC, int ci, int cj, struct blasfeo_dmat *sD, int di, int dj) {
+	getrf_np_single<double>(m, n, sC, ci, cj, sD, di, dj);
+}
+void blasfeo_sgetrf_np(int m, int n, struct blasfeo_smat *sC, int ci, int cj, struct blasfeo_smat *sD, int di, int dj) {
+	getrf_np_single<float>(m, n, sC, ci, cj, sD, di, dj);
+}
+int blasfeo_dpotrf_l_mn_batch(int batch, int m, int n, struct blasfeo_dmat_batch *sC, int ci, int cj,
+                              struct blasfeo_dmat_batch *sD, int di, int dj, int *info, void *stream) {
+	return potrf_mn_batch<double>(batch, m, n, sC, ci, cj, sD, di, dj, info, stream);
+}
+int blasfeo_spotrf_l_mn_batch(int batch, int m, int n, struct blasfeo_smat_batch *sC, int ci, int cj,
+                              struct blasfeo_smat_batch *sD, int di, int dj, int *info, void *stream) {
+	return potrf_mn_batch<float>(batch, m, n, sC, ci, cj, sD, di, dj, info, stream);
+}
+int blasfeo_dgetrf_np_batch(int batch, int m, int n, struct blasfeo_dmat_batch *sC, int ci, int cj,
+                            struct blasfeo_dmat_batch *sD, int di, int dj, int *info, void *stream) {
+	return getrf_np_batch<double>(batch, m, n, sC, ci, cj, sD, di, dj, info, stream);
+}
+int blasfeo_sgetrf_np_batch(int batch, int m, int n, struct blasfeo_smat_batch *sC, int ci, int cj,
+                            struct blasfeo_smat_batch *sD, int di, int dj, int *info, void *stream) {
+	return getrf_np_batch<float>(batch, m, n, sC, ci, cj, sD, di, dj, info, stream);
 }
 
 int blasfeo_dpotrf_l_batch(int batch, int m, struct blasfeo_dmat_batch *sC, int ci, int cj,

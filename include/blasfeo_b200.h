@@ -171,6 +171,30 @@ void blasfeo_sgetrf_rp(int m, int n, struct blasfeo_smat *sC, int ci, int cj, st
 int blasfeo_sgeqrf_worksize(int m, int n);
 void blasfeo_sgeqrf(int m, int n, struct blasfeo_smat *sC, int ci, int cj, struct blasfeo_smat *sD, int di, int dj, void *work);
 
+/* ---- adjacent variants: include/blasfeo_d_blasfeo_api.h:150 (syrk_ln_mn), :224 (trsm_rltu),
+ *      :281 (potrf_l_mn), :289 (getrf_np); s twins include/blasfeo_s_blasfeo_api.h:146, :208, :242, :249 ----
+ * syrk_ln_mn: lower trapezoid (m x n, j <= i) of D = beta*C + alpha*A*B^T.
+ * trsm_rltu:  D = alpha * B * A^{-T}, A lower with unit diagonal (not read).
+ * potrf_l_mn: Cholesky of the m x n lower trapezoid (n clamped to m): the n x n
+ *             factor and the rows below solved against it; 1/L_jj in dA,
+ *             use_dA = 1 with zero offsets (as the reference sets it).
+ * getrf_np:   LU without pivoting, unit L below and U on/above the diagonal of
+ *             D, 1/U_jj in dA (a zero pivot divides by zero, as the reference). */
+void blasfeo_dsyrk_ln_mn(int m, int n, int k, double alpha, struct blasfeo_dmat *sA, int ai, int aj,
+	struct blasfeo_dmat *sB, int bi, int bj, double beta, struct blasfeo_dmat *sC, int ci, int cj,
+	struct blasfeo_dmat *sD, int di, int dj);
+void blasfeo_dtrsm_rltu(int m, int n, double alpha, struct blasfeo_dmat *sA, int ai, int aj,
+	struct blasfeo_dmat *sB, int bi, int bj, struct blasfeo_dmat *sD, int di, int dj);
+void blasfeo_dpotrf_l_mn(int m, int n, struct blasfeo_dmat *sC, int ci, int cj, struct blasfeo_dmat *sD, int di, int dj);
+void blasfeo_dgetrf_np(int m, int n, struct blasfeo_dmat *sC, int ci, int cj, struct blasfeo_dmat *sD, int di, int dj);
+void blasfeo_ssyrk_ln_mn(int m, int n, int k, float alpha, struct blasfeo_smat *sA, int ai, int aj,
+	struct blasfeo_smat *sB, int bi, int bj, float beta, struct blasfeo_smat *sC, int ci, int cj,
+	struct blasfeo_smat *sD, int di, int dj);
+void blasfeo_strsm_rltu(int m, int n, float alpha, struct blasfeo_smat *sA, int ai, int aj,
+	struct blasfeo_smat *sB, int bi, int bj, struct blasfeo_smat *sD, int di, int dj);
+void blasfeo_spotrf_l_mn(int m, int n, struct blasfeo_smat *sC, int ci, int cj, struct blasfeo_smat *sD, int di, int dj);
+void blasfeo_sgetrf_np(int m, int n, struct blasfeo_smat *sC, int ci, int cj, struct blasfeo_smat *sD, int di, int dj);
+
 /* ---- level 2 used by the solve chains: include/blasfeo_d_blasfeo_api.h:85 (gemv_n), :93 (trsv_lnn), :97 (trsv_ltn) ---- */
 void blasfeo_dgemv_n(int m, int n, double alpha, struct blasfeo_dmat *sA, int ai, int aj, struct blasfeo_dvec *sx, int xi,
 	double beta, struct blasfeo_dvec *sy, int yi, struct blasfeo_dvec *sz, int zi);
@@ -221,6 +245,25 @@ int blasfeo_sgetrf_rp_batch(int batch, int m, int n, struct blasfeo_smat_batch *
 	struct blasfeo_smat_batch *sD, int di, int dj, int *ipiv, int *info, void *stream);
 int blasfeo_sgeqrf_batch(int batch, int m, int n, struct blasfeo_smat_batch *sC, int ci, int cj,
 	struct blasfeo_smat_batch *sD, int di, int dj, void *stream);
+/* uniform batches of the adjacent variants (info: first bad pivot + 1, or 0) */
+int blasfeo_dsyrk_ln_mn_batch(int batch, int m, int n, int k, double alpha, struct blasfeo_dmat_batch *sA, int ai, int aj,
+	struct blasfeo_dmat_batch *sB, int bi, int bj, double beta, struct blasfeo_dmat_batch *sC, int ci, int cj,
+	struct blasfeo_dmat_batch *sD, int di, int dj, void *stream);
+int blasfeo_dtrsm_rltu_batch(int batch, int m, int n, double alpha, struct blasfeo_dmat_batch *sA, int ai, int aj,
+	struct blasfeo_dmat_batch *sB, int bi, int bj, struct blasfeo_dmat_batch *sD, int di, int dj, void *stream);
+int blasfeo_dpotrf_l_mn_batch(int batch, int m, int n, struct blasfeo_dmat_batch *sC, int ci, int cj,
+	struct blasfeo_dmat_batch *sD, int di, int dj, int *info, void *stream);
+int blasfeo_dgetrf_np_batch(int batch, int m, int n, struct blasfeo_dmat_batch *sC, int ci, int cj,
+	struct blasfeo_dmat_batch *sD, int di, int dj, int *info, void *stream);
+int blasfeo_ssyrk_ln_mn_batch(int batch, int m, int n, int k, float alpha, struct blasfeo_smat_batch *sA, int ai, int aj,
+	struct blasfeo_smat_batch *sB, int bi, int bj, float beta, struct blasfeo_smat_batch *sC, int ci, int cj,
+	struct blasfeo_smat_batch *sD, int di, int dj, void *stream);
+int blasfeo_strsm_rltu_batch(int batch, int m, int n, float alpha, struct blasfeo_smat_batch *sA, int ai, int aj,
+	struct blasfeo_smat_batch *sB, int bi, int bj, struct blasfeo_smat_batch *sD, int di, int dj, void *stream);
+int blasfeo_spotrf_l_mn_batch(int batch, int m, int n, struct blasfeo_smat_batch *sC, int ci, int cj,
+	struct blasfeo_smat_batch *sD, int di, int dj, int *info, void *stream);
+int blasfeo_sgetrf_np_batch(int batch, int m, int n, struct blasfeo_smat_batch *sC, int ci, int cj,
+	struct blasfeo_smat_batch *sD, int di, int dj, int *info, void *stream);
 
 /* ---- variable-size batches (no reference counterpart) ----
  * Size arrays (m, n, k) and descriptor arrays (sA, ...) are DEVICE arrays of

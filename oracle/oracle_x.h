@@ -264,6 +264,111 @@ void OX(getrf_rp)(int m, int n, struct XMAT *sC, int ci, int cj, struct XMAT *sD
 	}
 }
 
+/* Lower trapezoid (m x n, element (i,j) for j <= i < m, j < n) of
+ * D = beta*C + alpha*A*B^T, inner size k.
+ * blasfeo_hp_pm/d_blas3_lib4.c:6459 (blasfeo_hp_dsyrk_ln_mn);
+ * blasfeo_ref/x_blas3_ref.c:4229 (REF_SYRK_LN_MN).  use_dA of D invalidated. */
+void OX(syrk_ln_mn)(int m, int n, int k, REAL alpha, struct XMAT *sA, int ai, int aj,
+                    struct XMAT *sB, int bi, int bj, REAL beta, struct XMAT *sC, int ci, int cj,
+                    struct XMAT *sD, int di, int dj)
+{
+	if (m <= 0 || n <= 0) return;
+	sD->use_dA = 0;
+	for (int j = 0; j < n; j++)
+		for (int i = j; i < m; i++) {
+			REAL c = 0;
+			for (int l = 0; l < k; l++)
+				c += EL(sA, ai + i, aj + l) * EL(sB, bi + j, bj + l);
+			EL(sD, di + i, dj + j) = alpha * c + beta * EL(sC, ci + i, cj + j);
+		}
+}
+
+/* D = alpha * B * A^{-T}, A lower triangular with unit diagonal (the diagonal
+ * is not read), m x n result, A n x n.
+ * blasfeo_hp_pm/d_blas3_lib4.c:4359 (blasfeo_hp_dtrsm_rltu);
+ * blasfeo_ref/x_blas3_ref.c:1760 (REF_TRSM_RLTU).  use_dA of D invalidated. */
+void OX(trsm_rltu)(int m, int n, REAL alpha, struct XMAT *sA, int ai, int aj,
+                   struct XMAT *sB, int bi, int bj, struct XMAT *sD, int di, int dj)
+{
+	if (m <= 0 || n <= 0) return;
+	sD->use_dA = 0;
+	for (int j = 0; j < n; j++)
+		for (int i = 0; i < m; i++) {
+			REAL c = alpha * EL(sB, bi + i, bj + j);
+			for (int l = 0; l < j; l++)
+				c -= EL(sD, di + i, dj + l) * EL(sA, ai + j, aj + l);
+			EL(sD, di + i, dj + j) = c;
+		}
+}
+
+/* Cholesky of the m x n lower trapezoid (n clamped to m): the n x n factor of
+ * the leading block and rows n..m-1 of the first n columns solved against it
+ * (L_ij = (C_ij - sum_l L_il L_jl) / L_jj).  Pivot rule and inverse diagonal as
+ * potrf_l; use_dA = 1 when di == dj == 0, else 0, as the reference sets it.
+ * blasfeo_hp_pm/d_lapack_lib4.c:1155-1187 (blasfeo_hp_dpotrf_l_mn);
+ * blasfeo_ref/x_lapack_ref.c:185 (REF_POTRF_L_MN). */
+void OX(potrf_l_mn)(int m, int n, struct XMAT *sC, int ci, int cj, struct XMAT *sD, int di, int dj)
+{
+	if (m <= 0 || n <= 0) return;
+	if (n > m) n = m;
+	REAL *dD = sD->dA;
+	sD->use_dA = (di == 0 && dj == 0) ? 1 : 0;
+	for (int j = 0; j < n; j++) {
+		REAL c = EL(sC, ci + j, cj + j);
+		for (int l = 0; l < j; l++)
+			c -= EL(sD, di + j, dj + l) * EL(sD, di + j, dj + l);
+		REAL d, inv;
+		if (c > 0) { d = SQRTX(c); inv = (REAL)1.0 / d; }
+		else { d = 0; inv = 0; }
+		EL(sD, di + j, dj + j) = d;
+		dD[j] = inv;
+		for (int i = j + 1; i < m; i++) {
+			REAL e = EL(sC, ci + i, cj + j);
+			for (int l = 0; l < j; l++)
+				e -= EL(sD, di + i, dj + l) * EL(sD, di + j, dj + l);
+			EL(sD, di + i, dj + j) = e * inv;
+		}
+	}
+}
+
+/* LU without pivoting, C = L*U stored in D (unit L below, U on/above the
+ * diagonal); inv = 1/U_jj (no zero test: a zero pivot divides by zero, as
+ * REF_GETRF_NOPIVOT does) in dA[j], L entries a*inv; use_dA = 1 when
+ * di == dj == 0.  Crout column order as getrf_rp without the pivot search.
+ * blasfeo_hp_pm/d_lapack_lib4.c:2078 (blasfeo_hp_dgetrf_np);
+ * blasfeo_ref/x_lapack_ref.c (REF_GETRF_NOPIVOT). */
+void OX(getrf_np)(int m, int n, struct XMAT *sC, int ci, int cj, struct XMAT *sD, int di, int dj)
+{
+	if (m <= 0 || n <= 0) return;
+	REAL *dD = sD->dA;
+	sD->use_dA = (di == 0 && dj == 0) ? 1 : 0;
+	if (sC != sD || ci != di || cj != dj)
+		for (int j = 0; j < n; j++)
+			for (int i = 0; i < m; i++)
+				EL(sD, di + i, dj + j) = EL(sC, ci + i, cj + j);
+	int mn = m < n ? m : n;
+	for (int j = 0; j < n; j++) {
+		int iu = j < m ? j : m;
+		for (int i = 0; i < iu; i++) {
+			REAL u = EL(sD, di + i, dj + j);
+			for (int l = 0; l < i; l++)
+				u -= EL(sD, di + i, dj + l) * EL(sD, di + l, dj + j);
+			EL(sD, di + i, dj + j) = u;
+		}
+		if (j >= mn) continue;
+		for (int i = j; i < m; i++) {
+			REAL a = EL(sD, di + i, dj + j);
+			for (int l = 0; l < j; l++)
+				a -= EL(sD, di + i, dj + l) * EL(sD, di + l, dj + j);
+			EL(sD, di + i, dj + j) = a;
+		}
+		REAL inv = (REAL)1.0 / EL(sD, di + j, dj + j);
+		dD[j] = inv;
+		for (int i = j + 1; i < m; i++)
+			EL(sD, di + i, dj + j) *= inv;
+	}
+}
+
 /* Workspace bytes of the HP geqrf: blasfeo_hp_pm/d_lapack_lib4.c:3433-3440.  The
  * oracle itself needs none. */
 int OX(geqrf_worksize)(int m, int n)

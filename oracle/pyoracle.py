@@ -169,7 +169,9 @@ class Api:
                      "potrf_l": "potrf_l", "syrk_potrf_ln": "syrk_%spotrf_ln" % prec,
                      "getrf_rp": "getrf_rp", "geqrf": "geqrf", "geqrf_worksize": "geqrf_worksize",
                      "trmm_rlnn": "trmm_rlnn", "trsv_lnn": "trsv_lnn", "trsv_ltn": "trsv_ltn",
-                     "gemv_n": "gemv_n", "gecp": "gecp", "diare": "diare", "rowsw": "rowsw"}[name]
+                     "gemv_n": "gemv_n", "gecp": "gecp", "diare": "diare", "rowsw": "rowsw",
+                     "syrk_ln_mn": "syrk_ln_mn", "trsm_rltu": "trsm_rltu", "potrf_l_mn": "potrf_l_mn",
+                     "getrf_np": "getrf_np"}[name]
             pre = "blasfeo_" if self.kind == "hp" else "blasfeo_ref_"
             sym = pre + prec + bname
         f = getattr(self.lib, sym)
@@ -211,6 +213,21 @@ class Api:
         addr = work.ctypes.data
         addr = (addr + 63) // 64 * 64
         self.fn(prec, "geqrf")(m, n, Cm.ref, ci, cj, D.ref, di, dj, C.c_void_p(addr))
+
+    def syrk_ln_mn(self, prec, m, n, k, alpha, A, ai, aj, B, bi, bj, beta, Cm, ci, cj, D, di, dj):
+        R = self._R(prec)
+        self.fn(prec, "syrk_ln_mn")(m, n, k, R(alpha), A.ref, ai, aj, B.ref, bi, bj, R(beta), Cm.ref, ci, cj, D.ref,
+                                    di, dj)
+
+    def trsm_rltu(self, prec, m, n, alpha, A, ai, aj, B, bi, bj, D, di, dj):
+        R = self._R(prec)
+        self.fn(prec, "trsm_rltu")(m, n, R(alpha), A.ref, ai, aj, B.ref, bi, bj, D.ref, di, dj)
+
+    def potrf_l_mn(self, prec, m, n, Cm, ci, cj, D, di, dj):
+        self.fn(prec, "potrf_l_mn")(m, n, Cm.ref, ci, cj, D.ref, di, dj)
+
+    def getrf_np(self, prec, m, n, Cm, ci, cj, D, di, dj):
+        self.fn(prec, "getrf_np")(m, n, Cm.ref, ci, cj, D.ref, di, dj)
 
     def trmm_rlnn(self, prec, m, n, alpha, A, ai, aj, B, bi, bj, D, di, dj):
         R = self._R(prec)

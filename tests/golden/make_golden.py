@@ -2,7 +2,7 @@
 
 Run in a container where the reference sources are present:
     make -C oracle generic haswell        # builds oracle/_ref/*.so from the reference tree
-    python tests/golden/make_golden.py
+    python tests/golden/make_golden.py    # all fixtures; or name files: ... make_golden.py adjacent.npz
 
 Every output stored here comes from the reference library itself (its
 LA=HIGH_PERFORMANCE panel-major routines ``blasfeo_*``, TARGET=GENERIC so the
@@ -206,18 +206,57 @@ def cfg5(api):
     return out
 
 
-def main():
-    api = ref_api("generic")
-    files = {}
+def adjacent(api):
+    """The adjacent variants (zero offsets, which the HP routines take directly):
+    syrk_ln_mn on a 23 x 13 trapezoid (k = 9), trsm_rltu with a unit lower
+    factor, potrf_l_mn of a 23 x 13 trapezoid of an SPD matrix, getrf_np of a
+    diagonally dominant matrix (square and 17 x 11), both precisions."""
+    rng = np.random.default_rng(8)
+    out = {}
     for prec in ("d", "s"):
-        files["testx_%s.npz" % prec] = run_testx(api, prec)
-    files["cfg1.npz"] = cfg1(api)
-    files["cfg2.npz"] = cfg2(api)
-    files["cfg3.npz"] = cfg3(api)
-    files["cfg4.npz"] = cfg4(api)
-    files["cfg5.npz"] = cfg5(api)
-    manifest = {"generator": "tests/golden/make_golden.py", "reference": "BLASFEO 0.1.4.2 HP panel-major, TARGET=GENERIC "
-                "(oracle/Makefile)", "files": {}}
+        m, n, k = 23, 13, 9
+        A, B, Cm = rng.standard_normal((m, k)), rng.standard_normal((n, k)), rng.standard_normal((m, n))
+        hA, hB, hC, hD = (HostMat(m, k, NP[prec]).set(A), HostMat(n, k, NP[prec]).set(B),
+                          HostMat(m, n, NP[prec]).set(Cm), HostMat(m, n, NP[prec]))
+        api.syrk_ln_mn(prec, m, n, k, 0.5, hA, 0, 0, hB, 0, 0, -1.5, hC, 0, 0, hD, 0, 0)
+        out[prec + "_syrkmn_A"], out[prec + "_syrkmn_B"], out[prec + "_syrkmn_C"] = A, B, Cm
+        out[prec + "_syrkmn_D"] = hD.get()
+        Lu = np.tril(rng.standard_normal((n, n)), -1) * 0.3 + np.eye(n) * 7.0   # diagonal must not be read
+        X = rng.standard_normal((m, n))
+        hL, hX, hY = HostMat(n, n, NP[prec]).set(Lu), HostMat(m, n, NP[prec]).set(X), HostMat(m, n, NP[prec])
+        api.trsm_rltu(prec, m, n, 1.25, hL, 0, 0, hX, 0, 0, hY, 0, 0)
+        out[prec + "_trsmu_L"], out[prec + "_trsmu_X"], out[prec + "_trsmu_Y"] = Lu, X, hY.get()
+        g = rng.standard_normal((m, m))
+        S = g @ g.T + m * np.eye(m)
+        hS, hP = HostMat(m, m, NP[prec]).set(S), HostMat(m, m, NP[prec])
+        api.potrf_l_mn(prec, m, n, hS, 0, 0, hP, 0, 0)
+        out[prec + "_potrfmn_S"], out[prec + "_potrfmn_L"], out[prec + "_potrfmn_dA"] = S, hP.get(), hP.diag(n)
+        for tag, (r, c) in (("sq", (15, 15)), ("rect", (17, 11))):
+            M = rng.standard_normal((r, c)) + 4.0 * np.eye(r, c) * max(r, c) ** 0.5
+            hM, hLU = HostMat(r, c, NP[prec]).set(M), HostMat(r, c, NP[prec])
+            api.getrf_np(prec, r, c, hM, 0, 0, hLU, 0, 0)
+            out[prec + "_lunp_%s_in" % tag], out[prec + "_lunp_%s" % tag] = M, hLU.get()
+            out[prec + "_lunp_%s_dA" % tag] = hLU.diag(min(r, c))
+    return out
+
+
+def main(only=None):
+    api = ref_api("generic")
+    gens = {"cfg1.npz": cfg1, "cfg2.npz": cfg2, "cfg3.npz": cfg3, "cfg4.npz": cfg4, "cfg5.npz": cfg5,
+            "adjacent.npz": adjacent}
+    files = {}
+    if only is None:
+        for prec in ("d", "s"):
+            files["testx_%s.npz" % prec] = run_testx(api, prec)
+    for name, fn in gens.items():
+        if only is None or name in only:
+            files[name] = fn(api)
+    mpath = os.path.join(HERE, "manifest.json")
+    if only is None or not os.path.exists(mpath):
+        manifest = {"generator": "tests/golden/make_golden.py", "reference": "BLASFEO 0.1.4.2 HP panel-major, "
+                    "TARGET=GENERIC (oracle/Makefile)", "files": {}}
+    else:
+        manifest = json.load(open(mpath))
     for name, d in files.items():
         path = os.path.join(HERE, name)
         np.savez_compressed(path, **{k: np.asarray(v) for k, v in d.items()})
@@ -228,4 +267,5 @@ def main():
 
 
 if __name__ == "__main__":
-    main()
+    # optional arguments: only these fixture files (the others and their hashes stay as they are)
+    main(sys.argv[1:] or None)

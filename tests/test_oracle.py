@@ -195,3 +195,72 @@ def test_memsize_matches_reference_layout():
     assert lib.oracle_d_memsize_mat(64, 64) == 33280
     assert lib.oracle_d_memsize_mat(16, 16) == 2176
     assert lib.oracle_d_memsize_mat(16, 32) == 4224
+
+
+# ---- the adjacent variants: syrk_ln_mn, trsm_rltu, potrf_l_mn, getrf_np ----
+
+def adjacent_oracle(orc, prec, g):
+    """The oracle on the inputs stored in the golden fixture (zero offsets)."""
+    out = {}
+    m, n, k = g[prec + "_syrkmn_A"].shape[0], g[prec + "_syrkmn_B"].shape[0], g[prec + "_syrkmn_A"].shape[1]
+    hA, hB, hC, hD = (host(m, k, prec, g[prec + "_syrkmn_A"]), host(n, k, prec, g[prec + "_syrkmn_B"]),
+                      host(m, n, prec, g[prec + "_syrkmn_C"]), host(m, n, prec))
+    orc.syrk_ln_mn(prec, m, n, k, 0.5, hA, 0, 0, hB, 0, 0, -1.5, hC, 0, 0, hD, 0, 0)
+    out["syrkmn_D"] = hD.get()
+    hL, hX, hY = host(n, n, prec, g[prec + "_trsmu_L"]), host(m, n, prec, g[prec + "_trsmu_X"]), host(m, n, prec)
+    orc.trsm_rltu(prec, m, n, 1.25, hL, 0, 0, hX, 0, 0, hY, 0, 0)
+    out["trsmu_Y"] = hY.get()
+    hS, hP = host(m, m, prec, g[prec + "_potrfmn_S"]), host(m, m, prec)
+    orc.potrf_l_mn(prec, m, n, hS, 0, 0, hP, 0, 0)
+    out["potrfmn_L"], out["potrfmn_dA"] = hP.get(), hP.diag(n)
+    for tag in ("sq", "rect"):
+        M = g[prec + "_lunp_%s_in" % tag]
+        r, c = M.shape
+        hM, hLU = host(r, c, prec, M), host(r, c, prec)
+        orc.getrf_np(prec, r, c, hM, 0, 0, hLU, 0, 0)
+        out["lunp_%s" % tag], out["lunp_%s_dA" % tag] = hLU.get(), hLU.diag(min(r, c))
+    return out
+
+
+@pytest.mark.parametrize("prec", ["d", "s"])
+def test_oracle_vs_golden_adjacent(orc, prec):
+    g = gold("adjacent.npz")
+    out = adjacent_oracle(orc, prec, g)
+    for key, v in out.items():
+        assert relfro(v, g[prec + "_" + key]) <= TOL[prec] * 10, (key, relfro(v, g[prec + "_" + key]))
+
+
+@pytest.mark.parametrize("prec", ["d", "s"])
+@pytest.mark.parametrize("off", [(0, 0, 0), (1, 2, 3), (3, 0, 1)])
+def test_oracle_vs_reference_adjacent_offsets(orc, prec, off):
+    # the reference backend (blasfeo_ref_*) takes every offset; the HP routines
+    # leave non-zero row offsets to it
+    _, ref = _ref_or_skip()
+    oi, oj, od = off
+    rng = np.random.default_rng(17 + oi + oj + od)
+    m, n, k = 19, 10, 7
+    A, B, Cm = rng.standard_normal((m + oi, k + oj)), rng.standard_normal((n + oi, k + oj)), rng.standard_normal((m + oi, n + oj))
+    Lu = np.tril(rng.standard_normal((n + oi, n + oj)), -1) * 0.4 + 5 * np.eye(n + oi, n + oj)
+    X = rng.standard_normal((m + oi, n + oj))
+    g = rng.standard_normal((m + oi, m + oi))
+    S = g @ g.T + (m + oi) * np.eye(m + oi)
+    M = rng.standard_normal((m + oi, n + oj)) + 6 * np.eye(m + oi, n + oj)
+    res = []
+    for api in (orc, ref):
+        r = {}
+        hA, hB, hC, hD = (host(m + oi, k + oj, prec, A), host(n + oi, k + oj, prec, B),
+                          host(m + oi, n + oj, prec, Cm), host(m + od, n + od, prec))
+        api.syrk_ln_mn(prec, m, n, k, 1.0, hA, oi, oj, hB, oi, oj, 0.5, hC, oi, oj, hD, od, od)
+        r["syrk"] = hD.get()
+        hL, hX, hY = host(n + oi, n + oj, prec, Lu), host(m + oi, n + oj, prec, X), host(m + od, n + od, prec)
+        api.trsm_rltu(prec, m, n, -0.5, hL, oi, oj, hX, oi, oj, hY, od, od)
+        r["trsm"] = hY.get()
+        hS, hP = host(m + oi, m + oi, prec, S), host(m + od, m + od, prec)
+        api.potrf_l_mn(prec, m, n, hS, oi, oi, hP, od, od)
+        r["potrf"] = hP.get()
+        hM, hLU = host(m + oi, n + oj, prec, M), host(m + od, n + od, prec)
+        api.getrf_np(prec, m, n, hM, oi, oj, hLU, od, od)
+        r["getrf"] = hLU.get()
+        res.append(r)
+    for key in res[0]:
+        assert relfro(res[0][key], res[1][key]) <= TOL[prec] * 100, (key, relfro(res[0][key], res[1][key]))
