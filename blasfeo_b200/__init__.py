@@ -108,6 +108,8 @@ for p, M, V, R in (("d", _DM, _DV, _d), ("s", _SM, _SV, _f)):
     _sig("blasfeo_unpack_%smat" % p, None, _i, _i, M, _i, _i, _vp, _i)
     _sig("blasfeo_pack_%svec" % p, None, _i, _vp, _i, V, _i)
     _sig("blasfeo_unpack_%svec" % p, None, _i, V, _i, _vp, _i)
+    _sig("blasfeo_pack_tran_%smat" % p, None, _i, _i, _vp, _i, M, _i, _i)
+    _sig("blasfeo_unpack_tran_%smat" % p, None, _i, _i, M, _i, _i, _vp, _i)
     _sig("blasfeo_%sgecp" % p, None, _i, _i, M, _i, _i, M, _i, _i)
     _sig("blasfeo_%sdiare" % p, None, _i, R, M, _i, _i)
     _sig("blasfeo_%srowsw" % p, None, _i, M, _i, _i, M, _i, _i)
@@ -131,6 +133,8 @@ for p, B, R, M in (("d", _DB, _d, _DM), ("s", _SB, _f, _SM)):
     _sig("blasfeo_memsize_%smat_batch" % p, _sz, _i, _i, _i)
     _sig("blasfeo_create_%smat_batch" % p, None, _i, _i, _i, B, _vp)
     _sig("blasfeo_%smat_batch_instance" % p, None, B, _i, M)
+    _sig("blasfeo_pack_%smat_batch" % p, _i, _i, _i, _i, _vp, _i, C.c_longlong, B, _i, _i, _vp)
+    _sig("blasfeo_unpack_%smat_batch" % p, _i, _i, _i, _i, B, _i, _i, _vp, _i, C.c_longlong, _vp)
     _sig("blasfeo_%sgemm_nt_batch" % p, _i, _i, *(_gemm_args(B, R) + [_vp]))
     _sig("blasfeo_%ssyrk_ln_batch" % p, _i, _i, *(_syrk_args(B, R) + [_vp]))
     _sig("blasfeo_%strsm_rltn_batch" % p, _i, _i, *(_trsm_args(B, R) + [_vp]))

@@ -118,6 +118,12 @@ void blasfeo_create_svec(int m, struct blasfeo_svec *sa, void *memory);
 /* host column-major A (lda) <-> device panel-major sA: auxiliary/d_aux_lib4.c:1607 (pack), :2238 (unpack) */
 void blasfeo_pack_dmat(int m, int n, double *A, int lda, struct blasfeo_dmat *sA, int ai, int aj);
 void blasfeo_unpack_dmat(int m, int n, struct blasfeo_dmat *sA, int ai, int aj, double *A, int lda);
+/* transposed: auxiliary/d_aux_lib4.c:2086 (pack_tran: sA's n x m block at
+ * (ai,aj) = A^T, A m x n column-major), :2360 (unpack_tran: A n x m = block^T) */
+void blasfeo_pack_tran_dmat(int m, int n, double *A, int lda, struct blasfeo_dmat *sA, int ai, int aj);
+void blasfeo_unpack_tran_dmat(int m, int n, struct blasfeo_dmat *sA, int ai, int aj, double *A, int lda);
+void blasfeo_pack_tran_smat(int m, int n, float *A, int lda, struct blasfeo_smat *sA, int ai, int aj);
+void blasfeo_unpack_tran_smat(int m, int n, struct blasfeo_smat *sA, int ai, int aj, float *A, int lda);
 void blasfeo_pack_dvec(int m, double *x, int xi, struct blasfeo_dvec *sa, int ai);
 void blasfeo_unpack_dvec(int m, struct blasfeo_dvec *sa, int ai, double *x, int xi);
 void blasfeo_pack_smat(int m, int n, float *A, int lda, struct blasfeo_smat *sA, int ai, int aj);
@@ -205,6 +211,21 @@ void blasfeo_dtrsv_ltn(int m, struct blasfeo_dmat *sA, int ai, int aj, struct bl
 size_t blasfeo_memsize_dmat_batch(int m, int n, int batch);
 void blasfeo_create_dmat_batch(int m, int n, int batch, struct blasfeo_dmat_batch *sA, void *memory);
 void blasfeo_dmat_batch_instance(struct blasfeo_dmat_batch *sA, int b, struct blasfeo_dmat *out);
+/* Host column-major batch <-> uniform-batch slab (no reference counterpart;
+ * the batched form of blasfeo_pack_dmat / blasfeo_unpack_dmat): instance b of
+ * the host array starts at A + b*strideA (ld lda) and maps to the m x n block
+ * at (bi, bj) of slab instance b.  One host<->device copy of the whole batch
+ * (a single 2-D copy when strideA == lda*n) through the library staging
+ * buffer, one conversion kernel; returns after the copies completed on
+ * `stream`.  BLASFEO_B200_EINVAL for out-of-range sizes or offsets. */
+int blasfeo_pack_dmat_batch(int batch, int m, int n, const double *A, int lda, long long strideA,
+	struct blasfeo_dmat_batch *sB, int bi, int bj, void *stream);
+int blasfeo_unpack_dmat_batch(int batch, int m, int n, struct blasfeo_dmat_batch *sB, int bi, int bj, double *A,
+	int lda, long long strideA, void *stream);
+int blasfeo_pack_smat_batch(int batch, int m, int n, const float *A, int lda, long long strideA,
+	struct blasfeo_smat_batch *sB, int bi, int bj, void *stream);
+int blasfeo_unpack_smat_batch(int batch, int m, int n, struct blasfeo_smat_batch *sB, int bi, int bj, float *A,
+	int lda, long long strideA, void *stream);
 size_t blasfeo_memsize_smat_batch(int m, int n, int batch);
 void blasfeo_create_smat_batch(int m, int n, int batch, struct blasfeo_smat_batch *sA, void *memory);
 void blasfeo_smat_batch_instance(struct blasfeo_smat_batch *sA, int b, struct blasfeo_smat *out);

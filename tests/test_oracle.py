@@ -264,3 +264,30 @@ def test_oracle_vs_reference_adjacent_offsets(orc, prec, off):
         res.append(r)
     for key in res[0]:
         assert relfro(res[0][key], res[1][key]) <= TOL[prec] * 100, (key, relfro(res[0][key], res[1][key]))
+
+
+@pytest.mark.parametrize("shape", [(5, 7, 1, 2), (12, 3, 0, 0), (1, 9, 3, 1), (9, 1, 2, 0)])
+def test_reference_pack_tran_semantics(shape):
+    # pins the layout rule the device converters implement, on the compiled
+    # reference itself: pack_tran puts A^T (A m x n, column-major) into the
+    # n x m block at (ai, aj); unpack_tran writes the block's transpose
+    import ctypes as C
+    from oracle.pyoracle import HostMat, ref_available, ref_lib
+    if not ref_available("generic"):
+        pytest.skip("compiled reference not built (make -C oracle generic)")
+    lib = ref_lib("generic")
+    m, n, ai, aj = shape
+    rng = np.random.default_rng(m * 10 + n)
+    A = np.asfortranarray(rng.standard_normal((m, n)))
+    h = HostMat(n + ai + 1, m + aj + 2)
+    base = rng.standard_normal((n + ai + 1, m + aj + 2))
+    h.set(base)
+    lib.blasfeo_pack_tran_dmat(m, n, A.ctypes.data_as(C.c_void_p), m, h.ref, ai, aj)
+    want = base.copy()
+    want[ai:ai + n, aj:aj + m] = A.T
+    assert np.array_equal(h.get(), want)
+    # unpack_tran of an m x n block at (ai, aj) where it fits: n x m result
+    if ai + m <= h.m and aj + n <= h.n:
+        out = np.asfortranarray(np.zeros((n, m)))
+        lib.blasfeo_unpack_tran_dmat(m, n, h.ref, ai, aj, out.ctypes.data_as(C.c_void_p), n)
+        assert np.array_equal(out, h.get()[ai:ai + m, aj:aj + n].T)
