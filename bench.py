@@ -15,6 +15,8 @@ N(0,1) matrix and log10(lambda) ~ U[0,6], b ~ N(0,1); every system solved to
           and write x back to host memory inside the timed region
   fp64_batched : plain FP64 batched dgemm_nt and dpotrf_l on uniform batches
           (n = 64, 128, 256, inputs larger than L2) against the FP64 roofline
+  fused_kernels : the fused n=16 chain (100,000 instances) and the batched
+          Riccati factorization (4,096 problems, N=30), GB/s against HBM
   cpu_baseline / --impl reference : the reference's own CPU path
           (blasfeo_dpotrf_l + blasfeo_dtrsv_lnn + blasfeo_dtrsv_ltn, BLASFEO
           compiled from source) on the host cores, threads over instances.
@@ -339,6 +341,12 @@ def main():
             fp64 = fp64_batched(lib, torch, dev, stream, fp64_peak, peak_bw)
         except Exception as ex:  # reported, never silently replaced
             fp64 = {"error": repr(ex)}
+    others = None
+    if not args.no_fp64:
+        try:
+            others = other_configs(lib, torch, dev, stream, peak_bw)
+        except Exception as ex:  # reported, never silently replaced
+            others = {"error": repr(ex)}
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         try:
@@ -356,6 +364,7 @@ def main():
             "refinement": {"mean_steps": float(it.mean()), "max_steps": int(it.max()), "max_berr": float(be.max()),
                            "sampled_host_residual": worst, "sampled_host_residual_plain": worst_plain},
             "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "clocks": clocks, "fp64_batched": fp64,
+            "fused_kernels": others,
             "gpu_launches": (args.steps * nclass) * 2}
     if rank == 0:
         print(json.dumps(line), flush=True)
@@ -409,6 +418,84 @@ def fp64_batched(lib, torch, dev, stream, fp64_peak, peak_bw, sizes=(64, 128, 25
                                    "roofline_gflops": roof, "frac_of_roofline": g / roof}
         del w, A, B, D, Cm, L
         torch.cuda.empty_cache()
+    return out
+
+
+def other_configs(lib, torch, dev, stream, peak_bw):
+    """The two fused HBM-bound kernels on their own workloads (seeded, inputs
+    larger than L2), per instance: algorithmic bytes (inputs read once, outputs
+    written once) and flops as in the design record.
+      chain:    100,000 instances, n = 16: S = A A^T + 16 I (A 16x32), L = chol(S),
+                X = R L^-T, D = C - X G^T (R, C, G 16x16 ~ N(0,1)); one launch;
+      riccati:  4,096 problems, N = 30, nx = 12, nu = 4, A = I + 0.1 N(0,1) scaled
+                to spectral radius 0.95, B ~ N(0,1)/sqrt(nx), Q = I, R = I, S = 0,
+                P_N = I; the whole backward factorization in one launch, FP64 and FP32."""
+    import numpy as np
+    from blasfeo_b200.api import DMatBatch, SMatBatch
+    from blasfeo_b200.workloads import fill_batch
+    sh = C.c_void_p(stream.cuda_stream)
+    g = torch.Generator(device=dev)
+    g.manual_seed(2)
+
+    def tm(fn, reps=10):
+        for _ in range(3):
+            fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(reps):
+            fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / reps
+
+    out = {}
+    nb = 100000
+    slabs = {}
+    for name, (r, c) in (("A", (16, 32)), ("R", (16, 16)), ("C", (16, 16)), ("G", (16, 16))):
+        slabs[name] = DMatBatch(r, c, nb)
+        fill_batch(slabs[name], torch.randn((nb, r, c), generator=g, dtype=torch.float64, device=dev))
+    L, X, D = DMatBatch(16, 16, nb), DMatBatch(16, 16, nb), DMatBatch(16, 16, nb)
+    info = torch.zeros(nb, dtype=torch.int32, device=dev)
+    ms = tm(lambda: lib.blasfeo_dsyrk_dpotrf_dtrsm_dgemm_batch(nb, 16, 32, 16.0, slabs["A"].ref, slabs["R"].ref,
+                                                             slabs["C"].ref, slabs["G"].ref, L.ref, X.ref, D.ref,
+                                                             C.c_void_p(info.data_ptr()), sh))
+    if not bool((info == 0).all().item()):
+        raise RuntimeError("chain reported a non-positive pivot")
+    by, fl = 15424.0 * nb, 22.8e3 * nb
+    out["chain_n16"] = {"instances": nb, "ms": ms, "instances_per_s": nb / ms * 1e3, "gbs": by / ms / 1e6,
+                        "frac_of_hbm": by / ms / 1e6 / peak_bw, "gflops": fl / ms / 1e6,
+                        "bytes_per_instance": 15424, "flops_per_instance": 22.8e3}
+    del slabs, L, X, D
+    torch.cuda.empty_cache()
+
+    nbt, N, nx, nu = 4096, 30, 12, 4
+    A = torch.eye(nx, dtype=torch.float64, device=dev) + 0.1 * torch.randn((nbt, nx, nx), generator=g,
+                                                                          dtype=torch.float64, device=dev)
+    rho = torch.linalg.eigvals(A.cpu()).abs().max(dim=1).values.to(dev)
+    A = A * (0.95 / rho)[:, None, None]
+    B = torch.randn((nbt, nx, nu), generator=g, dtype=torch.float64, device=dev) / np.sqrt(nx)
+    BA = torch.zeros((nbt, 16, nx), dtype=torch.float64, device=dev)
+    BA[:, :nu] = B.transpose(1, 2)
+    BA[:, nu:nu + nx] = A.transpose(1, 2)
+    BAs = BA[:, None].expand(nbt, N, 16, nx).reshape(nbt * N, 16, nx)
+    RSQ = torch.eye(16, dtype=torch.float64, device=dev).expand(nbt * (N + 1), 16, 16)
+    for prec, Bt, dt in (("d", DMatBatch, torch.float64), ("s", SMatBatch, torch.float32)):
+        sBA, sRSQ, sL = Bt(16, nx, nbt * N), Bt(16, 16, nbt * (N + 1)), Bt(16, 16, nbt * (N + 1))
+        fill_batch(sBA, BAs.to(dt).contiguous())
+        fill_batch(sRSQ, RSQ.to(dt).contiguous())
+        info = torch.zeros(nbt, dtype=torch.int32, device=dev)
+        f = lib.blasfeo_dric_trf_batch if prec == "d" else lib.blasfeo_sric_trf_batch
+        ms = tm(lambda: f(nbt, N, nx, nu, sBA.ref, sRSQ.ref, sL.ref, C.c_void_p(info.data_ptr()), sh))
+        if not bool((info == 0).all().item()):
+            raise RuntimeError("Riccati factorization reported a non-positive pivot")
+        esz = 8 if prec == "d" else 4
+        by = (16 * nx + 16 * 16 + 136) * esz * N * nbt   # BAbt_k and RSQ_k in, lower L_k out per stage
+        out["riccati_%s_N30" % prec] = {"problems": nbt, "ms": ms, "problems_per_s": nbt / ms * 1e3,
+                                        "gbs": by / ms / 1e6, "frac_of_hbm": by / ms / 1e6 / peak_bw,
+                                        "gflops": 7.1e3 * N * nbt / ms / 1e6}
+        del sBA, sRSQ, sL
+    torch.cuda.empty_cache()
     return out
 
 

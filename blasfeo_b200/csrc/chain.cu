@@ -1,4 +1,5 @@
-// Fused uniform-batch chain, one warp per instance (m = 16):
+// Fused uniform-batch chain, two instances per warp (m = 16; one per
+// half-warp, lane i of a half owns row i):
 //   S = A A^T + shift*I          (blasfeo_dsyrk_ln + blasfeo_ddiare)
 //   L = chol(S)                  (blasfeo_dpotrf_l, inverse diagonal kept)
 //   X = R L^{-T}                 (blasfeo_dtrsm_rltn)
@@ -7,35 +8,28 @@
 // (blasfeo_hp_pm/d_blas3_lib4.c:5400, :4123, :727; d_lapack_lib4.c:918).
 //
 // The chain is HBM-bound (about 1.5 flop per byte), so the design is about
-// bytes: each warp streams its instances' inputs (A, R, C, G: 10 KB for
-// k = 32, contiguous panel-major slabs) into shared memory with bulk copies
-// (TMA) on an mbarrier; every intermediate (S, L, X) stays on chip; L (lower
-// triangle), X and D are written once.  Persistent grid: each warp walks the
-// batch with a stride of the total warp count.  Memory-level parallelism
-// comes from 16 resident warps per SM, each with one instance in flight
-// (CHAIN_NBUF = 2 double-buffers instead, with fewer warps; measured slower:
-// 0.89 ms vs 0.67 ms for 100k instances).
+// bytes and issue slots: each half-warp streams its instance's inputs (A, R,
+// C, G: 10 KB for k = 32, contiguous panel-major slabs) into shared memory
+// with bulk copies (TMA) on its own mbarrier; every intermediate (S, L, X)
+// stays on chip; L (lower triangle), X and D are written once.  A 16 x 16
+// instance has 16 rows, so a whole warp per instance would leave half of its
+// lanes idle in every row-parallel phase; two instances per warp halve the
+// instructions issued per instance.  Persistent grid: each warp walks the
+// batch in pairs with a stride of the total warp count.
 #include "chol.cuh"
 #include "common.cuh"
 #include "tma.cuh"
 
-#ifndef CHAIN_WARPS
-#define CHAIN_WARPS 8
-#endif
-#ifndef CHAIN_NBUF
-#define CHAIN_NBUF 1
-#endif
-
 namespace {
 
-constexpr int CM = 16;                 // chain size m
-constexpr int CH_WARPS = CHAIN_WARPS;   // warps per CTA
-constexpr int W_LD = 17;               // row stride of the FP64 work matrix
+constexpr int CM = 16;       // chain size m
+constexpr int CH_WARPS = 4;  // warps per CTA (8 instances in flight)
+constexpr int W_LD = 17;     // row stride of the FP64 work matrix
 
 struct ChainLayout {
-	int a_dbl;     // doubles of the A slab (16 x cnA)
-	int buf_dbl;   // A + R + C + G
-	int warp_bytes;
+	int a_dbl;      // doubles of the A slab (16 x cnA)
+	int buf_dbl;    // A + R + C + G
+	int half_bytes; // one instance slot: inputs, work matrix, pivots, mbarrier, flags
 };
 
 __host__ __device__ inline ChainLayout chain_layout(int k) {
@@ -43,9 +37,8 @@ __host__ __device__ inline ChainLayout chain_layout(int k) {
 	const int cna = (k + 3) / 4 * 4;
 	l.a_dbl = CM * cna;
 	l.buf_dbl = l.a_dbl + 3 * CM * CM;
-	// input buffer(s), the work matrix, reciprocal pivots, mbarriers
-	l.warp_bytes = CHAIN_NBUF * l.buf_dbl * 8 + CM * W_LD * 8 + CM * 8 + 16 + 16;
-	l.warp_bytes = (l.warp_bytes + 127) / 128 * 128;
+	l.half_bytes = l.buf_dbl * 8 + CM * W_LD * 8 + CM * 8 + 16 + 16;
+	l.half_bytes = (l.half_bytes + 127) / 128 * 128;
 	return l;
 }
 
@@ -60,101 +53,93 @@ __global__ void __launch_bounds__(CH_WARPS * 32) k_chain16(int batch, int k, dou
 	extern __shared__ __align__(128) unsigned char smem[];
 	const ChainLayout lay = chain_layout(k);
 	const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-	unsigned char *base = smem + (size_t)warp * lay.warp_bytes;
-	double *buf[2] = {(double *)base, (double *)base + (CHAIN_NBUF - 1) * lay.buf_dbl};
-	double *W = (double *)base + CHAIN_NBUF * lay.buf_dbl;
+	const int h = lane >> 4, li = lane & 15;
+	unsigned char *base = smem + (size_t)(2 * warp + h) * lay.half_bytes;
+	double *buf = (double *)base;
+	double *W = buf + lay.buf_dbl;
 	double *dv = W + CM * W_LD;
 	uint64_t *bar = (uint64_t *)(dv + CM);
-	int *bad = (int *)(bar + 2);
+	int *bad = (int *)(bar + 1);
 	const int cna = (k + 3) / 4 * 4;
 	const uint32_t a_bytes = (uint32_t)lay.a_dbl * 8, m_bytes = CM * CM * 8;
 	const uint32_t tx = a_bytes + 3 * m_bytes;
 
 	const long long gw = (long long)blockIdx.x * CH_WARPS + warp;
 	const long long nw = (long long)gridDim.x * CH_WARPS;
-	if (lane == 0) {
-		mbar_init(&bar[0], 1);
-		mbar_init(&bar[1], 1);
+	const long long npairs = ((long long)batch + 1) / 2;
+	if (li == 0) {
+		mbar_init(bar, 1);
 		mbar_fence_init();
 	}
 	__syncwarp();
-	auto issue = [&](long long b, int slot) {
-		double *d = buf[slot];
-		mbar_arrive_expect_tx(&bar[slot], tx);
-		bulk_g2s(d, pA + sa * b, a_bytes, &bar[slot]);
-		bulk_g2s(d + lay.a_dbl, pR + sr * b, m_bytes, &bar[slot]);
-		bulk_g2s(d + lay.a_dbl + CM * CM, pC + sc * b, m_bytes, &bar[slot]);
-		bulk_g2s(d + lay.a_dbl + 2 * CM * CM, pG + sg * b, m_bytes, &bar[slot]);
-	};
-	if (gw < batch && lane == 0) issue(gw, 0);
-	uint32_t phase[2] = {0u, 0u};
-	int slot = 0;
-	for (long long b = gw; b < batch; b += nw, slot ^= (CHAIN_NBUF - 1)) {
-		const long long nb = b + nw;
-		if (CHAIN_NBUF == 1 && b != gw && lane == 0) {
-			// single buffer: refill it for this instance (its last readers finished at the loop end)
-			fence_proxy_async_smem();
-			issue(b, slot);
+	uint32_t phase = 0u;
+	for (long long p = gw; p < npairs; p += nw) {  // warp-uniform loop
+		const long long b = 2 * p + h;
+		const bool act = b < batch;  // the second half of the last pair may be empty
+		if (act && li == 0) {
+			// (the slot's generic accesses by the previous pair were fenced at its end)
+			mbar_arrive_expect_tx(bar, tx);
+			bulk_g2s(buf, pA + sa * b, a_bytes, bar);
+			bulk_g2s(buf + lay.a_dbl, pR + sr * b, m_bytes, bar);
+			bulk_g2s(buf + lay.a_dbl + CM * CM, pC + sc * b, m_bytes, bar);
+			bulk_g2s(buf + lay.a_dbl + 2 * CM * CM, pG + sg * b, m_bytes, bar);
 		}
-		if (CHAIN_NBUF == 2 && nb < batch && lane == 0) {
-			// the other buffer was last read by generic loads (previous instance)
-			fence_proxy_async_smem();
-			issue(nb, slot ^ 1);
+		bool ok = true;
+		if (act) {
+			ok = mbar_wait(bar, phase);
+			phase ^= 1u;
 		}
-		if (!mbar_wait(&bar[slot], phase[slot])) {
-			if (lane == 0 && info) info[b] = -3;  // bulk copy did not complete in time
-			mbar_wait(&bar[slot], phase[slot]);
-			if (CHAIN_NBUF == 2 && nb < batch) mbar_wait(&bar[slot ^ 1], phase[slot ^ 1]);
+		if (!__all_sync(0xffffffffu, ok)) {  // a bulk copy did not complete in time
+			if (act && li == 0 && info) info[b] = -3;
+			if (act) mbar_wait(bar, phase ^ 1u);
 			return;
 		}
-		phase[slot] ^= 1u;
-		const double *A = buf[slot];
-		double *R = buf[slot] + lay.a_dbl;
+		const double *A = buf;
+		double *R = buf + lay.a_dbl;
 		double *Cm = R + CM * CM;
 		const double *G = Cm + CM * CM;
 
-		// 1. S = A A^T + shift I: lanes 0..19 own half 4x4 tiles (rows of tile ti, 2 columns of tile tj)
-		if (lane < 20) {
+		// 1. S = A A^T + shift I: lanes 0..9 of the half own one 4x4 tile (ti, tj) of the lower part
+		if (li < 10) {
 			int ti, tj;
-			tri_index(lane >> 1, ti, tj);
-			const int q = lane & 1;
-			double acc[8];
+			tri_index(li, ti, tj);
+			double acc[16];
 #pragma unroll
-			for (int e = 0; e < 8; e++) acc[e] = 0.0;
-			const double *ai = A + ti * 4 * cna, *aj = A + tj * 4 * cna + 2 * q;
+			for (int e = 0; e < 16; e++) acc[e] = 0.0;
+			const double *ai = A + ti * 4 * cna, *aj = A + tj * 4 * cna;
 			for (int kk = 0; kk < k; kk++) {
 				const double2 x01 = *(const double2 *)(ai + 4 * kk), x23 = *(const double2 *)(ai + 4 * kk + 2);
-				const double2 y = *(const double2 *)(aj + 4 * kk);
-				acc[0] = fma(x01.x, y.x, acc[0]); acc[1] = fma(x01.y, y.x, acc[1]);
-				acc[2] = fma(x23.x, y.x, acc[2]); acc[3] = fma(x23.y, y.x, acc[3]);
-				acc[4] = fma(x01.x, y.y, acc[4]); acc[5] = fma(x01.y, y.y, acc[5]);
-				acc[6] = fma(x23.x, y.y, acc[6]); acc[7] = fma(x23.y, y.y, acc[7]);
+				const double2 y01 = *(const double2 *)(aj + 4 * kk), y23 = *(const double2 *)(aj + 4 * kk + 2);
+				const double x[4] = {x01.x, x01.y, x23.x, x23.y}, y[4] = {y01.x, y01.y, y23.x, y23.y};
+#pragma unroll
+				for (int c = 0; c < 4; c++)
+#pragma unroll
+					for (int r = 0; r < 4; r++) acc[4 * c + r] = fma(x[r], y[c], acc[4 * c + r]);
 			}
 #pragma unroll
-			for (int c = 0; c < 2; c++)
+			for (int c = 0; c < 4; c++)
 #pragma unroll
 				for (int r = 0; r < 4; r++) {
-					const int i = 4 * ti + r, j = 4 * tj + 2 * q + c;
+					const int i = 4 * ti + r, j = 4 * tj + c;
 					W[i * W_LD + j] = acc[4 * c + r] + (i == j ? shift : 0.0);
 				}
 		}
-		if (lane == 0) *bad = 0;
+		if (li == 0) *bad = 0;
 		__syncwarp();
-		// 2. L = chol(S): lane i holds row i in FP64 registers
+		// 2. L = chol(S): lane i of the half holds row i in FP64 registers
 		{
 			double r[CM];
 #pragma unroll
-			for (int l = 0; l < CM; l++) r[l] = (lane < CM && l <= lane) ? W[lane * W_LD + l] : (l == lane ? 1.0 : 0.0);
-			DiagCol<0>::run(r, lane, CM, 0, dv, bad);
-			if (lane < CM) {
+			for (int l = 0; l < CM; l++) r[l] = (l <= li) ? W[li * W_LD + l] : 0.0;
+			DiagCol<0, double, 16>::run(r, li, CM, 0, dv, bad);
 #pragma unroll
-				for (int l = 0; l < CM; l++) W[lane * W_LD + l] = (l <= lane) ? r[l] : 0.0;
-			}
+			for (int l = 0; l < CM; l++) W[li * W_LD + l] = (l <= li) ? r[l] : 0.0;
 		}
 		__syncwarp();
-		// 3./4. X = R L^{-T} and D = C - X G^T, lane i owns row i
-		if (lane < CM) {
-			const int i = lane;
+		// 3./4. X = R L^{-T} and D = C - X G^T, lane i owns row i; G read four
+		// rows (one panel column) at a time
+		{
+			const int i = li;
 			double x[CM];
 #pragma unroll
 			for (int j = 0; j < CM; j++) {
@@ -164,28 +149,41 @@ __global__ void __launch_bounds__(CH_WARPS * 32) k_chain16(int batch, int k, dou
 				x[j] = s * dv[j];
 			}
 #pragma unroll
-			for (int j = 0; j < CM; j++) {
-				double s = 0.0;
+			for (int jp = 0; jp < CM / 4; jp++) {
+				double s[4] = {0.0, 0.0, 0.0, 0.0};
 #pragma unroll
-				for (int l = 0; l < CM; l++) s = fma(x[l], G[pm_idx16(j, l)], s);
-				Cm[pm_idx16(i, j)] = Cm[pm_idx16(i, j)] - s;
+				for (int l = 0; l < CM; l++) {
+					const double2 g01 = *(const double2 *)(G + jp * 4 * CM + 4 * l);
+					const double2 g23 = *(const double2 *)(G + jp * 4 * CM + 4 * l + 2);
+					s[0] = fma(x[l], g01.x, s[0]);
+					s[1] = fma(x[l], g01.y, s[1]);
+					s[2] = fma(x[l], g23.x, s[2]);
+					s[3] = fma(x[l], g23.y, s[3]);
+				}
+#pragma unroll
+				for (int q = 0; q < 4; q++) Cm[pm_idx16(i, 4 * jp + q)] -= s[q];
 			}
 #pragma unroll
 			for (int j = 0; j < CM; j++) R[pm_idx16(i, j)] = x[j];
 		}
 		__syncwarp();
 		// 5. outputs: L lower triangle (and its inverse diagonal), X, D
-		double *gL = pL + sl * b, *gX = pX + sx * b, *gD = pD + sd * b;
-		for (int e = lane; e < CM * CM; e += 32) {
-			const int j = (e & 63) >> 2, i = ((e >> 6) << 2) | (e & 3);
-			if (j <= i) gL[e] = W[i * W_LD + j];
+		if (act) {
+			double *gL = pL + sl * b, *gX = pX + sx * b, *gD = pD + sd * b;
+			for (int e = li; e < CM * CM; e += 16) {
+				const int j = (e & 63) >> 2, i = ((e >> 6) << 2) | (e & 3);
+				if (j <= i) gL[e] = W[i * W_LD + j];
+			}
+			(pLd + sl * b)[li] = dv[li];
+			for (int e = 2 * li; e < CM * CM; e += 32) {
+				*(double2 *)(gX + e) = *(const double2 *)(R + e);
+				*(double2 *)(gD + e) = *(const double2 *)(Cm + e);
+			}
+			if (li == 0 && info) info[b] = *bad;
 		}
-		if (lane < CM) (pLd + sl * b)[lane] = dv[lane];
-		for (int e = 2 * lane; e < CM * CM; e += 64) {
-			*(double2 *)(gX + e) = *(const double2 *)(R + e);
-			*(double2 *)(gD + e) = *(const double2 *)(Cm + e);
-		}
-		if (lane == 0 && info) info[b] = *bad;
+		// this pair's generic accesses to the slot are ordered before the next
+		// pair's bulk copies into it
+		fence_proxy_async_smem();
 		__syncwarp();
 	}
 }
@@ -215,13 +213,13 @@ int blasfeo_dsyrk_dpotrf_dtrsm_dgemm_batch(int batch, int m, int k, double shift
 	sX->use_dA = 0;
 	sD->use_dA = 0;
 	const ChainLayout lay = chain_layout(k);
-	const size_t smem = (size_t)lay.warp_bytes * CH_WARPS;
+	const size_t smem = (size_t)lay.half_bytes * 2 * CH_WARPS;
 	cudaFuncSetAttribute(k_chain16, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
 	int per_sm = 0;
 	cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_chain16, CH_WARPS * 32, smem);
 	if (per_sm < 1) per_sm = 1;
 	long long grid = (long long)bf::num_sms() * per_sm;
-	long long need = (batch + CH_WARPS - 1) / CH_WARPS;
+	long long need = ((long long)batch + 2 * CH_WARPS - 1) / (2 * CH_WARPS);
 	if (grid > need) grid = need;
 	k_chain16<<<(unsigned)grid, CH_WARPS * 32, smem, (cudaStream_t)stream>>>(
 	    batch, k, shift, sA->pA, sA->stride, sR->pA, sR->stride, sC->pA, sC->stride, sG->pA, sG->stride, sL->pA,

@@ -126,30 +126,35 @@ __device__ __forceinline__ void chol_pivot_rsqrt(double c, double &d, double &in
 // without branches so the compiler can overlap the column update with the
 // next pivot.  The terminal step records the first non-positive pivot
 // (c0 + j + 1) in *bad by one ballot over the rows.
-template <int J, typename T = double>
+// WIDTH = 16 factors two independent blocks per warp, one per half-warp:
+// `lane` is then the lane within the half (0..15), the shuffles stay inside
+// the half, and each half records its own dinv / bad (the caller passes the
+// half's pointers).  The whole warp executes the call.
+template <int J, typename T = double, int WIDTH = 32>
 struct DiagCol {
 	static __device__ __forceinline__ void run(T (&r)[CHOL_NB], int lane, int nbk, int c0, double *dinv, int *bad) {
-		const double cj = (double)__shfl_sync(0xffffffffu, r[J], J);
+		const double cj = (double)__shfl_sync(0xffffffffu, r[J], J, WIDTH);
 		const bool ok = cj > 0.0;
 		const double inv = ok ? rsqrt(cj) : 0.0;
 		r[J] = (lane == J) ? (T)(ok ? cj * inv : 0.0) : r[J] * (T)inv;
 		if (lane == J && J < nbk) dinv[c0 + J] = inv;
 #pragma unroll
 		for (int l = J + 1; l < CHOL_NB; l++) {
-			const T t = __shfl_sync(0xffffffffu, r[J], l);
+			const T t = __shfl_sync(0xffffffffu, r[J], l, WIDTH);
 			if (lane >= l) r[l] = fma(-r[J], t, r[l]);
 		}
-		DiagCol<J + 1, T>::run(r, lane, nbk, c0, dinv, bad);
+		DiagCol<J + 1, T, WIDTH>::run(r, lane, nbk, c0, dinv, bad);
 	}
 };
-template <typename T>
-struct DiagCol<CHOL_NB, T> {
+template <typename T, int WIDTH>
+struct DiagCol<CHOL_NB, T, WIDTH> {
 	static __device__ __forceinline__ void run(T (&r)[CHOL_NB], int lane, int nbk, int c0, double *, int *bad) {
 		T d = T(1);
 #pragma unroll
 		for (int l = 0; l < CHOL_NB; l++)
 			if (l == lane) d = r[l];
-		const unsigned m = __ballot_sync(0xffffffffu, lane < nbk && !(d > T(0)));
+		unsigned m = __ballot_sync(0xffffffffu, lane < nbk && !(d > T(0)));
+		if (WIDTH == 16) m = (m >> (threadIdx.x & 16)) & 0xffffu;  // this half-warp's rows
 		if (m && lane == 0 && *bad == 0) *bad = c0 + __ffs(m);
 	}
 };

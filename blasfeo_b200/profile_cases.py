@@ -5,6 +5,8 @@ Usage: python -m blasfeo_b200.profile_cases OP N BATCH REPS [NMIN]
   potrf N BATCH REPS       blasfeo_dpotrf_l_batch on C = G G^T / N + I, G ~ N(0,1)
   posv  N BATCH REPS NMIN  blasfeo_dposv_l_vbatch on the uneven SPD workload with n ~ U{NMIN..N}
   sposv N BATCH REPS NMIN  blasfeo_dsposv_l_vbatch (mixed precision), same inputs
+  ric   N BATCH REPS       blasfeo_dric_trf_batch, horizon N, nx = 12, nu = 4, BATCH problems
+                           (A = I + 0.1 N(0,1) scaled to spectral radius 0.95, B ~ N(0,1)/sqrt(12), Q = R = I)
 Each call goes through the C ABI; REPS calls back to back, then a check of info.
 """
 import ctypes as C, sys, os
@@ -45,6 +47,25 @@ elif op in ("posv", "sposv"):
         else:
             st = lib.blasfeo_dsposv_l_vbatch(batch, P(W.nvec), W.max_n, P(W.desc), P(W.bdesc), P(W.xdesc), 30, 1e-12, None, None, P(info), None, 0, None)
         assert st == 0
+    torch.cuda.synchronize()
+    assert bool((info == 0).all().item())
+elif op == "ric":
+    import numpy as np
+    N, nx, nu = n, 12, 4
+    g = torch.Generator(device=dev)
+    g.manual_seed(4)
+    A = torch.eye(nx, dtype=torch.float64, device=dev) + 0.1 * torch.randn((batch, nx, nx), generator=g, dtype=torch.float64, device=dev)
+    A = A * (0.95 / torch.linalg.eigvals(A.cpu()).abs().max(dim=1).values.to(dev))[:, None, None]
+    B = torch.randn((batch, nx, nu), generator=g, dtype=torch.float64, device=dev) / np.sqrt(nx)
+    BA = torch.zeros((batch, 16, nx), dtype=torch.float64, device=dev)
+    BA[:, :nu] = B.transpose(1, 2)
+    BA[:, nu:] = A.transpose(1, 2)
+    sBA, sRSQ, sL = bf.DMatBatch(16, nx, batch * N), bf.DMatBatch(16, 16, batch * (N + 1)), bf.DMatBatch(16, 16, batch * (N + 1))
+    fill_batch(sBA, BA[:, None].expand(batch, N, 16, nx).reshape(batch * N, 16, nx).contiguous())
+    fill_batch(sRSQ, torch.eye(16, dtype=torch.float64, device=dev).expand(batch * (N + 1), 16, 16).contiguous())
+    info = torch.zeros(batch, dtype=torch.int32, device=dev)
+    for _ in range(reps):
+        assert lib.blasfeo_dric_trf_batch(batch, N, nx, nu, sBA.ref, sRSQ.ref, sL.ref, P(info), None) == 0
     torch.cuda.synchronize()
     assert bool((info == 0).all().item())
 torch.cuda.synchronize()
