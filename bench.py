@@ -17,6 +17,9 @@ N(0,1) matrix and log10(lambda) ~ U[0,6], b ~ N(0,1); every system solved to
           (n = 64, 128, 256, inputs larger than L2) against the FP64 roofline
   fused_kernels : the fused n=16 chain (100,000 instances) and the batched
           Riccati factorization (4,096 problems, N=30), GB/s against HBM
+  learned_dispatch : the mixed-op stream (gemm/potrf/getrf/geqrf, sizes 4..384):
+          regret of the MLP cost model's variant picks against the exhaustive
+          autotuner, next to the built-in rule, and GFLOP/s of the stream
   cpu_baseline / --impl reference : the reference's own CPU path
           (blasfeo_dpotrf_l + blasfeo_dtrsv_lnn + blasfeo_dtrsv_ltn, BLASFEO
           compiled from source) on the host cores, threads over instances.
@@ -347,6 +350,12 @@ def main():
             others = other_configs(lib, torch, dev, stream, peak_bw)
         except Exception as ex:  # reported, never silently replaced
             others = {"error": repr(ex)}
+    dispatch = None
+    if not args.no_fp64 and rank == 0:
+        try:
+            dispatch = learned_dispatch()
+        except Exception as ex:  # reported, never silently replaced
+            dispatch = {"error": repr(ex)}
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         try:
@@ -364,7 +373,7 @@ def main():
             "refinement": {"mean_steps": float(it.mean()), "max_steps": int(it.max()), "max_berr": float(be.max()),
                            "sampled_host_residual": worst, "sampled_host_residual_plain": worst_plain},
             "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "clocks": clocks, "fp64_batched": fp64,
-            "fused_kernels": others,
+            "fused_kernels": others, "learned_dispatch": dispatch,
             "gpu_launches": (args.steps * nclass) * 2}
     if rank == 0:
         print(json.dumps(line), flush=True)
@@ -496,6 +505,39 @@ def other_configs(lib, torch, dev, stream, peak_bw):
                                         "gflops": 7.1e3 * N * nbt / ms / 1e6}
         del sBA, sRSQ, sL
     torch.cuda.empty_cache()
+    return out
+
+
+def learned_dispatch(nlaunch=64, ntrain=44, seed=5):
+    """Mixed-op stream (gemm_nt 40%, potrf_l 25%, getrf_rp 20%, geqrf 15%; sizes
+    log-uniform 4..384, geqrf m = 2n; batches log-uniform 256..8192; FP64): the
+    exhaustive autotuner times every kernel variant of `nlaunch` sampled
+    launches, the MLP cost model (CUDA training kernels) is trained on the
+    first `ntrain` launches and picks the variants of the held-out ones.  Reports
+    regret against the exhaustive best (mean per launch and on total time) for
+    the MLP, the built-in rule and a fixed variant, and the end-to-end GFLOP/s
+    of the held-out stream under each policy."""
+    from blasfeo_b200 import autotune as at
+    from blasfeo_b200.costmodel import CostModel
+    recs = at.sweep(nlaunch, seed=seed, bmin=256, bmax=8192, nmax=384, reps=3)
+    X, y = at.training_set(recs[:ntrain])
+    cm = CostModel(at.NFEAT, seed=0)
+    cm.fit(X, y, epochs=300, lr=2e-3, batch=128)
+    test = recs[ntrain:]
+    picks = [cm.pick(r["feat"]) for r in test]
+    fl = sum(r["flops"] for r in test)
+    t_best = sum(float(r["times"].min()) for r in test)
+    t_mlp = sum(float(r["times"][p]) for r, p in zip(test, picks))
+    t_rule = sum(float(r["heur"]) for r in test)
+    t_v0 = sum(float(r["times"][0]) for r in test)
+    out = {"launches": nlaunch, "train": ntrain, "test": len(test),
+           "ops_in_test": {op: sum(1 for r in test if r["op"] == op) for op in at.OPS},
+           "instances_in_test": int(sum(r["batch"] for r in test))}
+    for name, picks_ in (("mlp", picks), ("rule", [-1] * len(test)), ("variant0", [0] * len(test))):
+        mean, tot = at.regret(test, picks_)
+        out["regret_" + name] = {"mean_per_launch": mean, "total_time": tot}
+    out["gflops"] = {"exhaustive": fl / t_best / 1e6, "mlp": fl / t_mlp / 1e6, "rule": fl / t_rule / 1e6,
+                     "variant0": fl / t_v0 / 1e6}
     return out
 
 
