@@ -301,6 +301,36 @@ __device__ void chol_block_inverse(const T *S, int n, int K, const double *dinv,
 	for (int i = 0; i < CHOL_NB; i++) invL[i * CHOL_NB + c] = (T)x[i];
 }
 
+// Diagonal block K of the factor in S replaced by its inverse (lower
+// triangular, same tiles, working precision), from the factor in S and the
+// FP64 reciprocal pivots; lane c computes column c.  Only the real rows and
+// columns (< n) are written; the whole warp calls it.
+template <typename T>
+__device__ void chol_block_inverse_inplace(T *S, int n, int K, const double *dinv, int lane) {
+	const int c0 = 16 * K;
+	const int nbk = min(CHOL_NB, n - c0);
+	const int c = lane & 15;
+	double x[CHOL_NB];
+#pragma unroll
+	for (int i = 0; i < CHOL_NB; i++) {
+		double s = (i == c) ? 1.0 : 0.0;
+#pragma unroll
+		for (int l = 0; l < i; l++) {
+			const double lil = (i < nbk && l < nbk) ? (double)lp_at(S, c0 + i, c0 + l) : 0.0;
+			s = fma(-lil, x[l], s);
+		}
+		const double di = (i < nbk) ? dinv[c0 + i] : 1.0;
+		x[i] = (i < c) ? 0.0 : s * di;
+	}
+	__syncwarp();  // every lane has read the block before any lane overwrites it
+	if (lane < CHOL_NB && c < nbk) {
+#pragma unroll
+		for (int i = 0; i < CHOL_NB; i++)
+			if (i >= c && i < nbk) lp_at(S, c0 + i, c0 + c) = (T)x[i];
+	}
+	__syncwarp();
+}
+
 // rank-16 update of tile (ti,tj) with the panel at block column c0
 template <typename T>
 __device__ __forceinline__ void chol_tile_update(T *S, int ti, int tj, int c0) {
@@ -348,11 +378,12 @@ __device__ __forceinline__ void chol_tile_update(T *S, int ti, int tj, int c0) {
 
 // Full factorization of the n x n lower-panel matrix S by the whole CTA
 // (blockDim.x >= 64).  dinv: FP64 shared array of >= 4P entries; Lt: 16*17
-// entries of T; bad: shared int (0 on entry).  If invL_all is non-null the
-// explicit inverses of all diagonal blocks (256 entries each, row-major) are
-// formed at the end, all blocks in parallel.
+// entries of T; bad: shared int (0 on entry).  With inv_diag the diagonal
+// blocks of the factor are replaced at the end by their explicit inverses
+// (all blocks in parallel), for the blocked triangular solves; the blocks
+// below the diagonal keep L.
 template <typename T>
-__device__ void chol_smem(T *S, int n, double *dinv, T *Lt, int *bad, T *invL_all) {
+__device__ void chol_smem(T *S, int n, double *dinv, T *Lt, int *bad, bool inv_diag) {
 	const int P = (n + 3) >> 2;
 	const int NB = (n + 15) >> 4;
 	const int tid = threadIdx.x, nt = blockDim.x;
@@ -386,9 +417,9 @@ __device__ void chol_smem(T *S, int n, double *dinv, T *Lt, int *bad, T *invL_al
 		}
 		__syncthreads();
 	}
-	if (invL_all) {
+	if (inv_diag) {
 		const int nw = nt >> 5;
-		for (int K = warp; K < NB; K += nw) chol_block_inverse<T>(S, n, K, dinv, invL_all + (size_t)K * 256, lane);
+		for (int K = warp; K < NB; K += nw) chol_block_inverse_inplace<T>(S, n, K, dinv, lane);
 		__syncthreads();
 	}
 }

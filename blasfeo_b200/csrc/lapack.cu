@@ -103,7 +103,7 @@ __global__ void __launch_bounds__(NT, MINB)
 	else
 		load_lower_panels<T>(S, n, c);
 	__syncthreads();
-	chol_smem<T>(S, n, dinv, invL, bad, (T *)nullptr);
+	chol_smem<T>(S, n, dinv, invL, bad, false);
 	if ((d.ri & 3) == 0)
 		store_lp_vec<T, 4>(S, n, d.p + (size_t)d.ri * d.cn + 4 * d.cj, d.cn);
 	else

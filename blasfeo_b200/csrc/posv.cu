@@ -78,52 +78,66 @@ __global__ void k_posv_classify(int batch, const int *__restrict__ nvec, int max
 
 // shared-memory plan of the posv kernel
 struct PosvPlan {
-	size_t S_off, inv_off, dinv_off, scr_off, w_off, x_off, r_off, ybuf_off, asum_off, red_off, misc_off, total;
+	size_t S_off, dinv_off, scr_off, w_off, x_off, r_off, ybuf_off, asum_off, misc_off, total;
 };
-// CTA size of a size class (largest n of the class)
+// CTA size of a size class (largest n of the class).  The mixed kernel's
+// shared memory (FP32 lower panels: 63 KB at n = 176, 102 KB at n = 224,
+// 133 KB at n = 256) lets three 128-thread CTAs share an SM up to n = 176,
+// two 256-thread CTAs up to n = 224, one 512-thread CTA above
 __host__ __device__ inline int posv_threads(int upper) {
-	return upper <= 64 ? 64 : (upper <= 128 ? 128 : (upper <= 192 ? 256 : 512));
+	return upper <= 64 ? 64 : (upper <= 176 ? 128 : (upper <= 224 ? 256 : 512));
 }
+// Shared memory of one CTA: the lower panels S (the mixed solver overwrites
+// their diagonal blocks with the blocks' inverses after the factorization),
+// FP64 reciprocal pivots, the factorization's scratch (row-major copy of the
+// diagonal block; the mixed solver's first residual pass reuses it for the
+// row sums of |A|), the right-hand side / correction w in T and, for the
+// mixed solver, the FP64 solution x and residual r.
 template <typename T, bool MIXED>
 __host__ __device__ inline PosvPlan posv_plan(int max_n, int nt) {
+	(void)nt;
 	PosvPlan p;
 	const int P = (max_n + 3) / 4;
 	const int NB = (max_n + 15) / 16;
 	const int nv = NB * 16;
+	const size_t scr = (16 * 17 + 64) * sizeof(double);
+	const size_t asum = MIXED ? (size_t)nv * sizeof(double) : 0;
 	p.S_off = 0;
-	p.inv_off = p.S_off + a16((size_t)lp_size(max_n) * sizeof(T));
-	p.dinv_off = p.inv_off + a16((size_t)(MIXED ? NB : 1) * 256 * sizeof(T));
+	p.dinv_off = p.S_off + a16((size_t)lp_size(max_n) * sizeof(T));
 	p.scr_off = p.dinv_off + a16((size_t)4 * P * sizeof(double));
-	p.w_off = p.scr_off + a16((16 * 17 + 64) * sizeof(double));
+	p.asum_off = p.scr_off;
+	p.w_off = p.scr_off + a16(scr > asum ? scr : asum);
 	p.x_off = p.w_off + a16((size_t)nv * sizeof(T));
 	p.r_off = p.x_off + (MIXED ? a16((size_t)nv * sizeof(double)) : 0);
 	p.ybuf_off = p.r_off + (MIXED ? a16((size_t)nv * sizeof(double)) : 0);
-	p.asum_off = p.ybuf_off + a16(16 * sizeof(T));
-	p.red_off = p.asum_off + (MIXED ? a16((size_t)nv * sizeof(double)) : 0);
-	// residual: column partial sums of the upper half of the warps, 8 per lane
-	const int nw = nt / 32;
-	p.misc_off = p.red_off + (MIXED ? a16((size_t)(nw > 1 ? nw / 2 : 1) * 32 * 8 * sizeof(double)) : 0);
+	p.misc_off = p.ybuf_off + a16(16 * sizeof(T));
 	p.total = p.misc_off + 64 * sizeof(double);
 	return p;
 }
 
 // Forward substitution w := L^{-1} w on the lower panels, 16-row blocks.
-// With block inverses (invL_all != null) the diagonal block is a 16x16
-// product; otherwise warp 0 substitutes with the FP64 reciprocal pivots.
+// With inv_diag the diagonal blocks of S hold their inverses (chol_smem) and
+// the diagonal step is a 16x16 product; otherwise warp 0 substitutes with the
+// FP64 reciprocal pivots.
 template <typename T>
-__device__ void trsv_fwd(const T *S, int n, const T *invL_all, const double *dinv, T *w, T *ybuf) {
+__device__ void trsv_fwd(const T *S, int n, bool inv_diag, const double *dinv, T *w, T *ybuf) {
 	const int tid = threadIdx.x, nt = blockDim.x;
 	const int NB = (n + 15) >> 4;
 	for (int K = 0; K < NB; K++) {
 		const int c0 = 16 * K;
 		const int nbk = min(16, n - c0);
-		if (invL_all) {
+		if (inv_diag) {
 			if (tid < 16) {
-				const T *inv = invL_all + (size_t)K * 256;
+				// all 16 entries of row tid of the block are read (the lower
+				// panels of a class hold 16 * NB rows and columns) and the ones
+				// outside the lower triangle masked by a select, so the loads
+				// need no branches
 				T s = T(0);
 #pragma unroll
-				for (int l = 0; l < 16; l++)
-					if (l <= tid) s = fma(inv[tid * 16 + l], w[c0 + l], s);
+				for (int l = 0; l < 16; l++) {
+					const T v = lp_at(S, c0 + tid, c0 + l);
+					s = fma((l <= tid) ? v : T(0), w[c0 + l], s);
+				}
 				ybuf[tid] = (tid < nbk) ? s : T(0);
 			}
 		} else if (tid < 32) {
@@ -148,21 +162,22 @@ __device__ void trsv_fwd(const T *S, int n, const T *invL_all, const double *din
 	}
 }
 
-// Backward substitution w := L^{-T} w.
+// Backward substitution w := L^{-T} w (inv_diag as trsv_fwd).
 template <typename T>
-__device__ void trsv_bwd(const T *S, int n, const T *invL_all, const double *dinv, T *w, T *ybuf) {
+__device__ void trsv_bwd(const T *S, int n, bool inv_diag, const double *dinv, T *w, T *ybuf) {
 	const int tid = threadIdx.x, nt = blockDim.x;
 	const int NB = (n + 15) >> 4;
 	for (int K = NB - 1; K >= 0; K--) {
 		const int c0 = 16 * K;
 		const int nbk = min(16, n - c0);
-		if (invL_all) {
+		if (inv_diag) {
 			if (tid < 16) {
-				const T *inv = invL_all + (size_t)K * 256;
 				T s = T(0);
 #pragma unroll
-				for (int l = 0; l < 16; l++)
-					if (l >= tid && l < nbk) s = fma(inv[l * 16 + tid], w[c0 + l], s);
+				for (int l = 0; l < 16; l++) {
+					const T v = lp_at(S, c0 + l, c0 + tid);
+					s = fma((l >= tid && l < nbk) ? v : T(0), w[c0 + l], s);
+				}
 				ybuf[tid] = (tid < nbk) ? s : T(0);
 			}
 		} else if (tid < 32) {
@@ -214,11 +229,11 @@ __device__ double block_max(double v, double *red) {
 // Warp w takes tile rows ti = w, w + NW, ...; lane l the tiles tj = l, l + 32
 // of the row.  A tile adds A_tile x_tj to rows ti (row part, reduced over the
 // lanes by a shuffle tree) and, below the diagonal, A_tile^T x_ti to rows tj
-// (column part, kept per lane in registers and summed over the warps by a
-// fixed tree through shared memory), so the result does not depend on timing.
-// RES: the residual into r; NORM: the row sums of |A| into asum (same scheme).
-// red: (NW/2) * 32 * 8 doubles of shared memory.  n <= 256 (two tile
-// columns per lane).
+// (column part, kept per lane in registers); after all row parts are written
+// the warps subtract their column parts one after the other in warp order, so
+// the result does not depend on timing and needs no reduction buffer.
+// RES: the residual into r; NORM: the row sums of |A| into asum.
+// n <= 256 (two tile columns per lane).
 template <bool LP>
 __device__ __forceinline__ const double *res_tile(const double *base, int cn, int ti, int tj) {
 	return LP ? base + lp_off(ti) + 16 * tj : base + (size_t)(4 * ti) * cn + 16 * tj;
@@ -226,7 +241,7 @@ __device__ __forceinline__ const double *res_tile(const double *base, int cn, in
 
 template <bool LP, bool RES, bool NORM>
 __device__ void sym_residual(const double *base, int cn, int n, const double *b, const double *x, double *r,
-                             double *asum, double *red) {
+                             double *asum) {
 	const int tid = threadIdx.x, nt = blockDim.x;
 	const int lane = tid & 31, warp = tid >> 5, nw = nt >> 5;
 	const int P = (n + 3) >> 2;
@@ -300,45 +315,25 @@ __device__ void sym_residual(const double *base, int cn, int n, const double *b,
 			if (NORM) asum[i] = lane == 0 ? rabs[0] : (lane == 1 ? rabs[1] : (lane == 2 ? rabs[2] : rabs[3]));
 		}
 	}
-	// column parts: fixed-order tree over the warps (one tree per accumulated
-	// quantity), then warp 0 adds them to r / asum
+	__syncthreads();
+	// column parts: subtracted from r (added to asum) one warp after the
+	// other, in warp order
+	for (int wv = 0; wv < nw; wv++) {
+		if (warp == wv) {
 #pragma unroll
-	for (int pass = 0; pass < 2; pass++) {
-		if (pass == 0 ? !RES : !NORM) continue;
-		double(&acc)[2][4] = pass == 0 ? cacc : cabs;
-		for (int half = nw >> 1; half >= 1; half >>= 1) {
-			if (warp >= half && warp < 2 * half) {
-				double *d = red + ((size_t)(warp - half) * 32 + lane) * 8;
+			for (int m = 0; m < 2; m++) {
+				const int tj = lane + 32 * m;
+				if (tj < P) {
 #pragma unroll
-				for (int m = 0; m < 2; m++)
-#pragma unroll
-					for (int q = 0; q < 4; q++) d[4 * m + q] = acc[m][q];
-			}
-			__syncthreads();
-			if (warp < half) {
-				const double *d = red + ((size_t)warp * 32 + lane) * 8;
-#pragma unroll
-				for (int m = 0; m < 2; m++)
-#pragma unroll
-					for (int q = 0; q < 4; q++) acc[m][q] += d[4 * m + q];
-			}
-			__syncthreads();
-		}
-	}
-	if (warp == 0) {
-#pragma unroll
-		for (int m = 0; m < 2; m++) {
-			const int tj = lane + 32 * m;
-			if (tj < P) {
-#pragma unroll
-				for (int q = 0; q < 4; q++) {
-					if (RES) r[4 * tj + q] -= cacc[m][q];
-					if (NORM) asum[4 * tj + q] += cabs[m][q];
+					for (int q = 0; q < 4; q++) {
+						if (RES) r[4 * tj + q] -= cacc[m][q];
+						if (NORM) asum[4 * tj + q] += cabs[m][q];
+					}
 				}
 			}
 		}
+		__syncthreads();
 	}
-	__syncthreads();
 }
 
 template <typename T, bool MIXED, int NT, int MINB>
@@ -354,7 +349,6 @@ __global__ void __launch_bounds__(NT, MINB) k_posv(int cls, int max_n, PosvWs ws
 	double *slot = slots ? slots + (size_t)blockIdx.x * lp_size(max_n) : nullptr;
 	double *asum = (double *)(smem + pl.asum_off);
 	T *S = (T *)(smem + pl.S_off);
-	T *invL = (T *)(smem + pl.inv_off);
 	double *dinv = (double *)(smem + pl.dinv_off);
 	double *scratch = (double *)(smem + pl.scr_off);
 	T *w = (T *)(smem + pl.w_off);
@@ -362,7 +356,6 @@ __global__ void __launch_bounds__(NT, MINB) k_posv(int cls, int max_n, PosvWs ws
 	double *rs = (double *)(smem + pl.r_off);
 	T *ybuf = (T *)(smem + pl.ybuf_off);
 	double *misc = (double *)(smem + pl.misc_off);
-	double *red = (double *)(smem + pl.red_off);
 	int *s_bad = (int *)(misc + 40);
 	int *s_item = (int *)(misc + 41);
 	const int tid = threadIdx.x, nt = blockDim.x;
@@ -404,11 +397,11 @@ __global__ void __launch_bounds__(NT, MINB) k_posv(int cls, int max_n, PosvWs ws
 		if (MIXED)
 			for (int i = tid; i < nv; i += nt) xs[i] = 0.0;
 		__syncthreads();
-		chol_smem<T>(S, n, dinv, (T *)scratch, s_bad, MIXED ? invL : (T *)nullptr);
+		chol_smem<T>(S, n, dinv, (T *)scratch, s_bad, MIXED);
 
 		if (!MIXED) {
-			trsv_fwd<T>(S, n, nullptr, dinv, w, ybuf);
-			trsv_bwd<T>(S, n, nullptr, dinv, w, ybuf);
+			trsv_fwd<T>(S, n, false, dinv, w, ybuf);
+			trsv_bwd<T>(S, n, false, dinv, w, ybuf);
 			for (int i = tid; i < n; i += nt) xg[i] = (double)w[i];
 			if (tid == 0) {
 				if (info) info[sys] = *s_bad;
@@ -432,22 +425,22 @@ __global__ void __launch_bounds__(NT, MINB) k_posv(int cls, int max_n, PosvWs ws
 			__syncthreads();
 		}
 		for (;;) {
-			trsv_fwd<T>(S, n, invL, dinv, w, ybuf);
-			trsv_bwd<T>(S, n, invL, dinv, w, ybuf);
+			trsv_fwd<T>(S, n, true, dinv, w, ybuf);
+			trsv_bwd<T>(S, n, true, dinv, w, ybuf);
 			for (int i = tid; i < n; i += nt) xs[i] += (double)w[i] / scale;
 			__syncthreads();
 			// ||A||_inf (row sums of |A|) once, before the first residual
 			// (the first pass also accumulates the row sums of |A|: one read of A)
 			if (slot) {
 				if (it == 0)
-					sym_residual<true, true, true>(slot, 0, n, bg, xs, rs, asum, red);
+					sym_residual<true, true, true>(slot, 0, n, bg, xs, rs, asum);
 				else
-					sym_residual<true, true, false>(slot, 0, n, bg, xs, rs, asum, red);
+					sym_residual<true, true, false>(slot, 0, n, bg, xs, rs, asum);
 			} else {
 				if (it == 0)
-					sym_residual<false, true, true>(a.p, a.cn, n, bg, xs, rs, asum, red);
+					sym_residual<false, true, true>(a.p, a.cn, n, bg, xs, rs, asum);
 				else
-					sym_residual<false, true, false>(a.p, a.cn, n, bg, xs, rs, asum, red);
+					sym_residual<false, true, false>(a.p, a.cn, n, bg, xs, rs, asum);
 			}
 			// norms
 			double rm = 0.0, xm = 0.0;
@@ -582,7 +575,7 @@ PosvLayout posv_layout(int batch, int max_n, bool use_slots) {
 	PosvLayout L;
 	// size classes: shared memory and CTA size follow the largest member
 	const size_t smem_cap = bf::max_smem_optin();
-	const int uppers[] = {16, 32, 64, 96, 128, 160, 192, 256};
+	const int uppers[] = {16, 32, 64, 96, 128, 160, 176, 192, 224, 256};
 	int nc = 0;
 	int smem_limit_n = 0;  // largest n the shared-memory kernel takes
 	for (int v = 4; v <= 4096; v += 4)
@@ -681,7 +674,10 @@ int posv_run(int batch, const int *n, int max_n, const void *sA, const void *sb,
 			else if (cfg[c].upper <= 128)
 				st = launch_posv<T, MIXED, 128, 4>(c, cfg[c].upper, pl.total, batch, rslots, ws, n, sA, sb, sx,
 				                                   max_iter, tol, iters, berr, info, rs, s);
-			else if (cfg[c].upper <= 192)
+			else if (cfg[c].upper <= 176)
+				st = launch_posv<T, MIXED, 128, 3>(c, cfg[c].upper, pl.total, batch, rslots, ws, n, sA, sb, sx,
+				                                   max_iter, tol, iters, berr, info, rs, s);
+			else if (cfg[c].upper <= 224)
 				st = launch_posv<T, MIXED, 256, 2>(c, cfg[c].upper, pl.total, batch, rslots, ws, n, sA, sb, sx,
 				                                   max_iter, tol, iters, berr, info, rs, s);
 			else

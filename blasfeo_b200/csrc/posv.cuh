@@ -2,7 +2,7 @@
 #pragma once
 #include "common.cuh"
 
-constexpr int POSV_MAX_CLASSES = 10;
+constexpr int POSV_MAX_CLASSES = 12;
 
 // engine of the mixed solver when the caller asks for the default: 1 = the
 // tensor-core kernel (posv_tc.cu), 0 = the SIMT kernel (posv.cu)
