@@ -83,9 +83,11 @@ struct PosvPlan {
 // CTA size of a size class (largest n of the class).  The mixed kernel's
 // shared memory (FP32 lower panels: 63 KB at n = 176, 102 KB at n = 224,
 // 133 KB at n = 256) lets three 128-thread CTAs share an SM up to n = 176,
-// two 256-thread CTAs up to n = 224, one 512-thread CTA above
+// two up to n = 224, and one 256-thread CTA runs above (thread counts
+// measured: the work per system is latency-bound, and fewer threads make the
+// barriers cheaper, as long as the trailing updates keep enough warps)
 __host__ __device__ inline int posv_threads(int upper) {
-	return upper <= 64 ? 64 : (upper <= 176 ? 128 : (upper <= 224 ? 256 : 512));
+	return upper <= 64 ? 64 : (upper <= 224 ? 128 : 256);
 }
 // Shared memory of one CTA: the lower panels S (the mixed solver overwrites
 // their diagonal blocks with the blocks' inverses after the factorization),
@@ -678,10 +680,10 @@ int posv_run(int batch, const int *n, int max_n, const void *sA, const void *sb,
 				st = launch_posv<T, MIXED, 128, 3>(c, cfg[c].upper, pl.total, batch, rslots, ws, n, sA, sb, sx,
 				                                   max_iter, tol, iters, berr, info, rs, s);
 			else if (cfg[c].upper <= 224)
-				st = launch_posv<T, MIXED, 256, 2>(c, cfg[c].upper, pl.total, batch, rslots, ws, n, sA, sb, sx,
+				st = launch_posv<T, MIXED, 128, 2>(c, cfg[c].upper, pl.total, batch, rslots, ws, n, sA, sb, sx,
 				                                   max_iter, tol, iters, berr, info, rs, s);
 			else
-				st = launch_posv<T, MIXED, 512, 1>(c, cfg[c].upper, pl.total, batch, rslots, ws, n, sA, sb, sx,
+				st = launch_posv<T, MIXED, 256, 1>(c, cfg[c].upper, pl.total, batch, rslots, ws, n, sA, sb, sx,
 				                                   max_iter, tol, iters, berr, info, rs, s);
 			if (st) return st;
 		}
