@@ -63,6 +63,17 @@ class smat_batch(dmat_batch):
     pass
 
 
+class cm_dmat(C.Structure):
+    """struct blasfeo_cm_dmat (include/blasfeo_common.h:220-229 layout): pA is
+    column-major with leading dimension m."""
+    _fields_ = [("mem", C.c_void_p), ("pA", C.c_void_p), ("dA", C.c_void_p),
+                ("m", C.c_int), ("n", C.c_int), ("use_dA", C.c_int), ("memsize", C.c_int)]
+
+
+class cm_smat(cm_dmat):
+    """struct blasfeo_cm_smat (same layout, float pointers)."""
+
+
 P = C.POINTER
 _i, _d, _f, _vp, _sz = C.c_int, C.c_double, C.c_float, C.c_void_p, C.c_size_t
 _DM, _SM, _DV, _SV = P(dmat), P(smat), P(dvec), P(svec)
@@ -126,6 +137,14 @@ for p, M, V, R in (("d", _DM, _DV, _d), ("s", _SM, _SV, _f)):
     _sig("blasfeo_%strsm_rltu" % p, None, *_trsm_args(M, R))
     _sig("blasfeo_%spotrf_l_mn" % p, None, _i, _i, M, _i, _i, M, _i, _i)
     _sig("blasfeo_%sgetrf_np" % p, None, _i, _i, M, _i, _i, M, _i, _i)
+for p, R, M in (("d", _d, P(cm_dmat)), ("s", _f, P(cm_smat))):
+    _sig("blasfeo_cm_memsize_%smat" % p, _sz, _i, _i)
+    _sig("blasfeo_cm_create_%smat" % p, None, _i, _i, M, _vp)
+    _sig("blasfeo_cm_%sgemm_nt" % p, None, *_gemm_args(M, R))
+    _sig("blasfeo_cm_%strsm_rltn" % p, None, *_trsm_args(M, R))
+    _sig("blasfeo_cm_%spotrf_l" % p, None, _i, M, _i, _i, M, _i, _i)
+_sig("blasfeo_cm_dsyrk_ln", None, *_syrk_args(P(cm_dmat), _d))
+_sig("blasfeo_cm_dgetrf_rp", None, _i, _i, P(cm_dmat), _i, _i, P(cm_dmat), _i, _i, P(_i))
 _sig("blasfeo_dgemv_n", None, _i, _i, _d, _DM, _i, _i, _DV, _i, _d, _DV, _i, _DV, _i)
 _sig("blasfeo_dtrsv_lnn", None, _i, _DM, _i, _i, _DV, _i, _DV, _i)
 _sig("blasfeo_dtrsv_ltn", None, _i, _DM, _i, _i, _DV, _i, _DV, _i)

@@ -15,7 +15,7 @@ import ctypes as C
 
 import numpy as np
 
-from . import lib, dmat, smat, dvec, svec, dmat_batch, smat_batch, check
+from . import lib, dmat, smat, dvec, svec, dmat_batch, smat_batch, cm_dmat, cm_smat, check
 
 __all__ = [
     "DMat", "SMat", "DVec", "SVec", "DMatBatch", "SMatBatch", "device_buffer", "set_stream", "set_sync",
@@ -28,6 +28,9 @@ __all__ = [
     "blasfeo_dtrsv_ltn", "descriptor_array", "vector_array",
     "blasfeo_dsyrk_ln_mn", "blasfeo_dtrsm_rltu", "blasfeo_dpotrf_l_mn", "blasfeo_dgetrf_np",
     "blasfeo_ssyrk_ln_mn", "blasfeo_strsm_rltu", "blasfeo_spotrf_l_mn", "blasfeo_sgetrf_np",
+    "CmDMat", "CmSMat", "blasfeo_cm_dgemm_nt", "blasfeo_cm_dsyrk_ln", "blasfeo_cm_dtrsm_rltn",
+    "blasfeo_cm_dpotrf_l", "blasfeo_cm_dgetrf_rp", "blasfeo_cm_sgemm_nt", "blasfeo_cm_strsm_rltn",
+    "blasfeo_cm_spotrf_l",
 ]
 
 
@@ -238,11 +241,56 @@ def vector_array(vecs):
     return torch.frombuffer(bytearray(raw), dtype=torch.uint8).cuda()
 
 
+class _CmMat:
+    """A column-major device matrix (struct blasfeo_cm_dmat): m x n, leading
+    dimension m, created by blasfeo_cm_create_dmat on a device buffer."""
+    _prec = "d"
+    _np = np.float64
+    _desc = cm_dmat
+
+    def __init__(self, m, n):
+        self.m, self.n = m, n
+        nbytes = getattr(lib, "blasfeo_cm_memsize_%smat" % self._prec)(m, n)
+        self.buf = device_buffer(nbytes)
+        self.s = self._desc()
+        getattr(lib, "blasfeo_cm_create_%smat" % self._prec)(m, n, C.byref(self.s), C.c_void_p(self.buf.data_ptr()))
+
+    @property
+    def ref(self):
+        return C.byref(self.s)
+
+    def _view(self):
+        import torch
+        esz = np.dtype(self._np).itemsize
+        t = self.buf[: self.m * self.n * esz].view(torch.float64 if self._prec == "d" else torch.float32)
+        return t.view(self.n, self.m)  # row j of the view = column j of the matrix
+
+    def pack(self, A):
+        import torch
+        A = np.asarray(A, dtype=self._np)
+        assert A.shape == (self.m, self.n)
+        self._view().copy_(torch.from_numpy(np.ascontiguousarray(A.T)))
+        return self
+
+    def unpack(self):
+        return np.ascontiguousarray(self._view().cpu().numpy().T)
+
+
+class CmDMat(_CmMat):
+    pass
+
+
+class CmSMat(_CmMat):
+    _prec = "s"
+    _np = np.float32
+    _desc = cm_smat
+
+
 def _wrap(name):
     f = getattr(lib, name)
 
     def call(*args):
-        conv = [a.ref if isinstance(a, (_Mat, _Vec)) else a for a in args]
+        conv = [a.ref if isinstance(a, (_Mat, _Vec, _CmMat)) else a for a in args]
         r = f(*conv)
         check()
         return r
@@ -255,12 +303,13 @@ for _p in ("d", "s"):
                "rowsw", "syrk_ln_mn", "trsm_rltu", "potrf_l_mn", "getrf_np"):
         globals()["blasfeo_%s%s" % (_p, _r)] = _wrap("blasfeo_%s%s" % (_p, _r))
     globals()["blasfeo_%ssyrk_%spotrf_ln" % (_p, _p)] = _wrap("blasfeo_%ssyrk_%spotrf_ln" % (_p, _p))
-for _r in ("dgemv_n", "dtrsv_lnn", "dtrsv_ltn"):
+for _r in ("dgemv_n", "dtrsv_lnn", "dtrsv_ltn", "cm_dgemm_nt", "cm_dsyrk_ln", "cm_dtrsm_rltn", "cm_dpotrf_l",
+           "cm_sgemm_nt", "cm_strsm_rltn", "cm_spotrf_l"):
     globals()["blasfeo_" + _r] = _wrap("blasfeo_" + _r)
 
 
-def _getrf(prec):
-    f = getattr(lib, "blasfeo_%sgetrf_rp" % prec)
+def _getrf(prec, cm=False):
+    f = getattr(lib, "blasfeo_%s%sgetrf_rp" % ("cm_" if cm else "", prec))
 
     def call(m, n, sC, ci, cj, sD, di, dj, ipiv=None):
         mn = max(1, min(m, n))
@@ -285,5 +334,6 @@ def _geqrf(prec):
 
 blasfeo_dgetrf_rp = _getrf("d")
 blasfeo_sgetrf_rp = _getrf("s")
+blasfeo_cm_dgetrf_rp = _getrf("d", cm=True)
 blasfeo_dgeqrf = _geqrf("d")
 blasfeo_sgeqrf = _geqrf("s")

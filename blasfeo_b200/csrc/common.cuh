@@ -28,6 +28,9 @@ bool sync_mode();
 int finish_single();                      // launch check + optional stream sync, records error
 // library-owned device workspace (per device, grows; never shrinks)
 void *workspace(size_t bytes, cudaStream_t s);
+// a second buffer of the same kind, for the column-major routines' staging
+// (they call panel-major routines that use the first one)
+void *workspace_cm(size_t bytes, cudaStream_t s);
 int num_sms();
 size_t max_smem_optin();
 int posv_engine();                        // engine of the mixed SPD solver (BLASFEO_B200_POSV_*)

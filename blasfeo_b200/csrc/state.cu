@@ -46,14 +46,16 @@ struct Workspace {
 	size_t bytes = 0;
 };
 static std::mutex g_ws_mutex;
-static std::vector<Workspace> g_ws;
+// per device: [0] the general workspace, [1] the column-major staging buffer
+static std::vector<Workspace> g_ws[2];
 
-void *workspace(size_t bytes, cudaStream_t s) {
+static void *workspace_slot(int slot, size_t bytes, cudaStream_t s) {
 	int dev = 0;
 	if (cudaGetDevice(&dev) != cudaSuccess) return nullptr;
 	std::lock_guard<std::mutex> lock(g_ws_mutex);
-	if ((int)g_ws.size() <= dev) g_ws.resize(dev + 1);
-	Workspace &w = g_ws[dev];
+	std::vector<Workspace> &v = g_ws[slot];
+	if ((int)v.size() <= dev) v.resize(dev + 1);
+	Workspace &w = v[dev];
 	if (w.bytes >= bytes && w.ptr) return w.ptr;
 	// growing: wait for work that may still use the old buffer
 	if (w.ptr) {
@@ -73,6 +75,9 @@ void *workspace(size_t bytes, cudaStream_t s) {
 	w.bytes = want;
 	return w.ptr;
 }
+
+void *workspace(size_t bytes, cudaStream_t s) { return workspace_slot(0, bytes, s); }
+void *workspace_cm(size_t bytes, cudaStream_t s) { return workspace_slot(1, bytes, s); }
 
 int num_sms() {
 	static int sms[64] = {0};

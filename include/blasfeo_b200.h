@@ -85,6 +85,22 @@ struct blasfeo_smat_batch {
 	size_t memsize;
 };
 
+/* column-major descriptors, include/blasfeo_common.h:220-229 (same fields and
+ * order): pA is a column-major array in DEVICE memory whose leading dimension
+ * is m, element (i,j) at pA[i + j*m] (the reference's BLAS API sets m = lda). */
+struct blasfeo_cm_dmat {
+	double *mem; double *pA; double *dA;
+	int m, n;
+	int use_dA;
+	int memsize;
+};
+struct blasfeo_cm_smat {
+	float *mem; float *pA; float *dA;
+	int m, n;
+	int use_dA;
+	int memsize;
+};
+
 /* status codes */
 #define BLASFEO_B200_OK 0
 #define BLASFEO_B200_EINVAL 1      /* bad argument (size, NULL pointer, out of range) */
@@ -128,6 +144,40 @@ void blasfeo_pack_dvec(int m, double *x, int xi, struct blasfeo_dvec *sa, int ai
 void blasfeo_unpack_dvec(int m, struct blasfeo_dvec *sa, int ai, double *x, int xi);
 void blasfeo_pack_smat(int m, int n, float *A, int lda, struct blasfeo_smat *sA, int ai, int aj);
 void blasfeo_unpack_smat(int m, int n, struct blasfeo_smat *sA, int ai, int aj, float *A, int lda);
+
+/* ---- column-major drop-in (device-resident column-major matrices) ----
+ * storage: auxiliary/d_aux_common.c:111,121 (m*n elements, then min(m,n) for
+ * dA; the reference declares create with a struct blasfeo_pm_dmat pointer,
+ * include/blasfeo_d_aux.h:237, these take the column-major descriptor).
+ * Routines: include/blasfeo_d_blasfeo_api.h:321 (gemm_nt), :324 (syrk_ln,
+ * lower triangle of D written), :342 (trsm_rltn), :389 (potrf_l, lower
+ * triangle of D written), :391 (getrf_rp, ipiv: host array of min(m,n)
+ * 0-based absolute row indices); include/blasfeo_s_blasfeo_api.h:282, :295,
+ * :305.  Same arguments and results as the panel-major routines of the same
+ * name; dA / use_dA are neither read nor written (as in blasfeo_hp_cm/).
+ * Single-instance semantics as the panel-major drop-ins (stream, sync, last
+ * error). */
+size_t blasfeo_cm_memsize_dmat(int m, int n);
+void blasfeo_cm_create_dmat(int m, int n, struct blasfeo_cm_dmat *sA, void *memory);
+size_t blasfeo_cm_memsize_smat(int m, int n);
+void blasfeo_cm_create_smat(int m, int n, struct blasfeo_cm_smat *sA, void *memory);
+void blasfeo_cm_dgemm_nt(int m, int n, int k, double alpha, struct blasfeo_cm_dmat *sA, int ai, int aj,
+                         struct blasfeo_cm_dmat *sB, int bi, int bj, double beta, struct blasfeo_cm_dmat *sC, int ci,
+                         int cj, struct blasfeo_cm_dmat *sD, int di, int dj);
+void blasfeo_cm_dsyrk_ln(int m, int k, double alpha, struct blasfeo_cm_dmat *sA, int ai, int aj,
+                         struct blasfeo_cm_dmat *sB, int bi, int bj, double beta, struct blasfeo_cm_dmat *sC, int ci,
+                         int cj, struct blasfeo_cm_dmat *sD, int di, int dj);
+void blasfeo_cm_dtrsm_rltn(int m, int n, double alpha, struct blasfeo_cm_dmat *sA, int ai, int aj,
+                           struct blasfeo_cm_dmat *sB, int bi, int bj, struct blasfeo_cm_dmat *sD, int di, int dj);
+void blasfeo_cm_dpotrf_l(int m, struct blasfeo_cm_dmat *sC, int ci, int cj, struct blasfeo_cm_dmat *sD, int di, int dj);
+void blasfeo_cm_dgetrf_rp(int m, int n, struct blasfeo_cm_dmat *sC, int ci, int cj, struct blasfeo_cm_dmat *sD, int di,
+                          int dj, int *ipiv);
+void blasfeo_cm_sgemm_nt(int m, int n, int k, float alpha, struct blasfeo_cm_smat *sA, int ai, int aj,
+                         struct blasfeo_cm_smat *sB, int bi, int bj, float beta, struct blasfeo_cm_smat *sC, int ci,
+                         int cj, struct blasfeo_cm_smat *sD, int di, int dj);
+void blasfeo_cm_strsm_rltn(int m, int n, float alpha, struct blasfeo_cm_smat *sA, int ai, int aj,
+                           struct blasfeo_cm_smat *sB, int bi, int bj, struct blasfeo_cm_smat *sD, int di, int dj);
+void blasfeo_cm_spotrf_l(int m, struct blasfeo_cm_smat *sC, int ci, int cj, struct blasfeo_cm_smat *sD, int di, int dj);
 void blasfeo_pack_svec(int m, float *x, int xi, struct blasfeo_svec *sa, int ai);
 void blasfeo_unpack_svec(int m, struct blasfeo_svec *sa, int ai, float *x, int xi);
 /* include/blasfeo_d_aux.h:115 dgecp, :141 ddiare, :162 drowsw */

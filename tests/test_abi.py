@@ -91,3 +91,39 @@ def test_error_strings():
     import blasfeo_b200 as bf
     assert bf.lib.blasfeo_b200_error_string(0) == b"ok"
     assert b"invalid" in bf.lib.blasfeo_b200_error_string(1)
+
+
+def test_cm_descriptor_layout():
+    import blasfeo_b200 as bf
+    assert C.sizeof(bf.cm_dmat) == 40 and C.sizeof(bf.cm_smat) == 40
+    assert [f for f, _ in bf.cm_dmat._fields_] == ["mem", "pA", "dA", "m", "n", "use_dA", "memsize"]
+
+
+@pytest.mark.parametrize("mn", [(64, 64), (5, 3), (3, 5), (1, 1), (257, 13)])
+def test_cm_memsize_and_create_match_reference(mn):
+    """blasfeo_cm_memsize_dmat / blasfeo_cm_create_dmat (auxiliary/d_aux_common.c:111,121):
+    m*n elements then min(m,n) for dA, no rounding."""
+    import blasfeo_b200 as bf
+    m, n = mn
+    want = (m * n + min(m, n)) * 8
+    assert bf.lib.blasfeo_cm_memsize_dmat(m, n) == want
+    assert bf.lib.blasfeo_cm_memsize_smat(m, n) == want // 2
+    s = bf.cm_dmat()
+    base = 0x20000
+    bf.lib.blasfeo_cm_create_dmat(m, n, C.byref(s), C.c_void_p(base))
+    assert (s.m, s.n, s.use_dA, s.memsize) == (m, n, 0, want)
+    assert s.mem == base and s.pA == base and s.dA == base + m * n * 8
+    from oracle.pyoracle import ref_available, ref_lib
+    if ref_available("generic"):
+        r = ref_lib("generic")
+        r.blasfeo_cm_memsize_dmat.restype = C.c_size_t
+        assert r.blasfeo_cm_memsize_dmat(m, n) == want
+        # the reference's create takes a struct blasfeo_pm_dmat pointer
+        # (include/blasfeo_d_aux.h:237; include/blasfeo_common.h:173-185: mem,
+        # pA, dA, m, n, pm, cn, use_dA, ps, memsize): read its fields there
+        raw = (C.c_ubyte * 64)()
+        r.blasfeo_cm_create_dmat(m, n, raw, C.c_void_p(base))
+        b = bytes(raw)
+        q = lambda off: int.from_bytes(b[off:off + 8], "little")
+        i = lambda off: int.from_bytes(b[off:off + 4], "little", signed=True)
+        assert (q(8), q(16), i(24), i(28), i(40), i(48)) == (s.pA, s.dA, s.m, s.n, s.use_dA, s.memsize)
