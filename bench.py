@@ -350,6 +350,17 @@ def main():
             others = other_configs(lib, torch, dev, stream, peak_bw)
         except Exception as ex:  # reported, never silently replaced
             others = {"error": repr(ex)}
+    single = None
+    if not args.no_fp64 and rank == 0:
+        try:
+            single = single_dropin(torch, stream, fp64_peak, peak_bw)
+        except Exception as ex:  # reported, never silently replaced
+            single = {"error": repr(ex)}
+        if not args.no_cpu:
+            try:
+                single["cpu_reference"] = cpu_single_dropin()
+            except Exception as ex:
+                single["cpu_reference"] = {"error": repr(ex)}
     dispatch = None
     if not args.no_fp64 and rank == 0:
         try:
@@ -373,7 +384,7 @@ def main():
             "refinement": {"mean_steps": float(it.mean()), "max_steps": int(it.max()), "max_berr": float(be.max()),
                            "sampled_host_residual": worst, "sampled_host_residual_plain": worst_plain},
             "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "clocks": clocks, "fp64_batched": fp64,
-            "fused_kernels": others, "learned_dispatch": dispatch,
+            "fused_kernels": others, "single_dropin": single, "learned_dispatch": dispatch,
             "gpu_launches": (args.steps * nclass) * 2}
     if rank == 0:
         print(json.dumps(line), flush=True)
@@ -427,6 +438,129 @@ def fp64_batched(lib, torch, dev, stream, fp64_peak, peak_bw, sizes=(64, 128, 25
                                    "roofline_gflops": roof, "frac_of_roofline": g / roof}
         del w, A, B, D, Cm, L
         torch.cuda.empty_cache()
+    return out
+
+
+SINGLE_N = 64
+
+
+def _single_inputs():
+    """Config 1 inputs, seed 0: A, B 64x64 ~ U[-1,1]; S = G G^T / 64 + I with
+    G ~ N(0,1); R 64x64 ~ N(0,1), the trsm right-hand side."""
+    import numpy as np
+    n = SINGLE_N
+    rng = np.random.default_rng(0)
+    A = rng.uniform(-1, 1, (n, n))
+    B = rng.uniform(-1, 1, (n, n))
+    G = rng.standard_normal((n, n))
+    S = G @ G.T / n + np.eye(n)
+    R = rng.standard_normal((n, n))
+    return A, B, S, R
+
+
+def single_dropin(torch, stream, fp64_peak, peak_bw):
+    """Config 1: one 64x64 instance per call through the single-instance C ABI
+    (device-resident panel-major matrices): dgemm_nt 64x64x64 (alpha 1, beta 0),
+    dpotrf_l of S, dtrsm_rltn of R with that factor (which reuses the cached
+    inverse diagonal).  Microseconds per call: back-to-back asynchronous calls
+    timed with CUDA events (device time plus launch; the calls are made from
+    Python through ctypes), the same calls each synchronised (what a caller with
+    CPU semantics waits), and the three calls as one CUDA graph replay.  For
+    form: flops, algorithmic bytes and the roofline time max(flops / FP64 peak,
+    bytes / HBM bandwidth) of each call."""
+    import blasfeo_b200 as bf
+    from blasfeo_b200.api import DMat
+    n = SINGLE_N
+    A, B, S, R = _single_inputs()
+    dA, dB, dS, dL, dR, dX, dD = (DMat(n, n).pack(M) for M in (A, B, S, S, R, R, A))
+    lib = bf.lib
+    ref = lambda M: M.ref
+    calls = {
+        "dgemm_nt_64": lambda: lib.blasfeo_dgemm_nt(n, n, n, 1.0, ref(dA), 0, 0, ref(dB), 0, 0, 0.0, ref(dD), 0, 0,
+                                                    ref(dD), 0, 0),
+        "dpotrf_l_64": lambda: lib.blasfeo_dpotrf_l(n, ref(dS), 0, 0, ref(dL), 0, 0),
+        "dtrsm_rltn_64": lambda: lib.blasfeo_dtrsm_rltn(n, n, 1.0, ref(dL), 0, 0, ref(dR), 0, 0, ref(dX), 0, 0),
+    }
+    work = {"dgemm_nt_64": (2.0 * n ** 3, 3 * n * n * 8),
+            "dpotrf_l_64": (n ** 3 / 3 + n * n / 2 + n / 6, 2 * n * n * 8),
+            "dtrsm_rltn_64": (float(n ** 3), 3 * n * n * 8)}
+    bf.set_stream(stream)
+    out = {"n": n}
+    reps = 2000
+    try:
+        for name, f in calls.items():
+            bf.set_sync(False)
+            for _ in range(50):
+                f()
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            for _ in range(reps):
+                f()
+            e1.record(stream)
+            torch.cuda.synchronize()
+            us_async = e0.elapsed_time(e1) * 1e3 / reps
+            bf.set_sync(True)
+            t0 = time.perf_counter()
+            for _ in range(reps // 4):
+                f()
+            us_sync = (time.perf_counter() - t0) * 1e6 / (reps // 4)
+            fl, by = work[name]
+            roof_us = max(fl / (fp64_peak * 1e9), by / (peak_bw * 1e9)) * 1e6
+            out[name] = {"us_async": us_async, "us_sync": us_sync, "flops": fl, "bytes": by,
+                         "flop_per_byte": fl / by, "roofline_us": roof_us,
+                         "gflops_async": fl / (us_async * 1e-6) / 1e9}
+            assert lib.blasfeo_b200_last_error() == 0
+        # the three calls (factor, solve, update) as one graph
+        bf.set_sync(False)
+        g = torch.cuda.CUDAGraph()
+        cap = torch.cuda.Stream()
+        with torch.cuda.graph(g, stream=cap, capture_error_mode="relaxed"):
+            bf.set_stream(cap)
+            for f in calls.values():
+                f()
+        bf.set_stream(stream)
+        for _ in range(20):
+            g.replay()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(reps):
+            g.replay()
+        e1.record()
+        torch.cuda.synchronize()
+        out["graph_3calls_us"] = e0.elapsed_time(e1) * 1e3 / reps
+        del g
+    finally:
+        bf.set_sync(True)
+        bf.set_stream(None)
+    return out
+
+
+def cpu_single_dropin(reps=2000):
+    """Config 1 on the host: the same three calls through the compiled reference
+    (BLASFEO HP, Haswell build, one core), microseconds per call."""
+    import numpy as np
+    from oracle.pyoracle import Api, HostMat, ref_available
+    kind = "reference" if ref_available("haswell") else "port"
+    api = Api("hp", "haswell") if kind == "reference" else Api("oracle")
+    n = SINGLE_N
+    A, B, S, R = _single_inputs()
+    hA, hB, hS, hR = (HostMat(n, n).set(M) for M in (A, B, S, R))
+    hD, hL, hX = HostMat(n, n), HostMat(n, n), HostMat(n, n)
+    calls = {
+        "dgemm_nt_64": lambda: api.gemm_nt("d", n, n, n, 1.0, hA, 0, 0, hB, 0, 0, 0.0, hD, 0, 0, hD, 0, 0),
+        "dpotrf_l_64": lambda: api.potrf_l("d", n, hS, 0, 0, hL, 0, 0),
+        "dtrsm_rltn_64": lambda: api.trsm_rltn("d", n, n, 1.0, hL, 0, 0, hR, 0, 0, hX, 0, 0),
+    }
+    out = {"kind": kind, "cores": 1}
+    for name, f in calls.items():
+        for _ in range(50):
+            f()
+        t0 = time.perf_counter()
+        for _ in range(reps):
+            f()
+        out[name + "_us"] = (time.perf_counter() - t0) * 1e6 / reps
     return out
 
 
