@@ -1,7 +1,6 @@
 // Library state: error recording, the stream of the single-instance entry
 // points, the synchronous/asynchronous switch, and the library-owned device
 // workspace used when a caller passes no workspace.
-#include <mutex>
 #include <vector>
 
 #include "common.cuh"
@@ -44,18 +43,37 @@ int finish_single() {
 struct Workspace {
 	void *ptr = nullptr;
 	size_t bytes = 0;
+	int dev = 0;
 };
-static std::mutex g_ws_mutex;
-// per device: [0] the general workspace, [1] the column-major staging buffer
-static std::vector<Workspace> g_ws[2];
+// One set per host thread, like the stream of the single-instance calls: two
+// threads that work on their own streams never share scratch.  Per thread and
+// device: [0] the general workspace, [1] the column-major staging buffer.
+// Freed when the thread ends (at process exit the runtime may already be gone;
+// the failed cudaFree is then harmless).
+struct ThreadWorkspaces {
+	std::vector<Workspace> slot[2];
+	~ThreadWorkspaces() {
+		int cur = 0;
+		const bool have = cudaGetDevice(&cur) == cudaSuccess;
+		for (auto &v : slot)
+			for (auto &w : v)
+				if (w.ptr) {
+					cudaSetDevice(w.dev);
+					cudaFree(w.ptr);
+				}
+		if (have) cudaSetDevice(cur);
+		cudaGetLastError();
+	}
+};
+static thread_local ThreadWorkspaces g_ws;
 
 static void *workspace_slot(int slot, size_t bytes, cudaStream_t s) {
 	int dev = 0;
 	if (cudaGetDevice(&dev) != cudaSuccess) return nullptr;
-	std::lock_guard<std::mutex> lock(g_ws_mutex);
-	std::vector<Workspace> &v = g_ws[slot];
+	std::vector<Workspace> &v = g_ws.slot[slot];
 	if ((int)v.size() <= dev) v.resize(dev + 1);
 	Workspace &w = v[dev];
+	w.dev = dev;
 	if (w.bytes >= bytes && w.ptr) return w.ptr;
 	// growing: wait for work that may still use the old buffer
 	if (w.ptr) {

@@ -383,7 +383,8 @@ int blasfeo_dgeqrf_vbatch_variant(int batch, const int *m, const int *n, int max
  *           or max_iter refinement steps; iters[b] / berr[b] (device, may be NULL)
  *           receive the step count and final backward error; info[b] = -1 when
  *           refinement did not reach tol.
- * work/work_bytes: device workspace; NULL uses a library-owned workspace.
+ * work/work_bytes: device workspace; NULL uses a library-owned workspace (one
+ * per host thread and device, like the stream of the single-instance calls).
  * blasfeo_dposv_worksize_n(batch, max_n, mixed) gives its size for a call
  * (mixed = 1: dsposv); blasfeo_dposv_worksize(batch) is the size when every
  * system fits a shared-memory kernel (dsposv with n <= 256, dposv with
