@@ -166,6 +166,85 @@ __global__ void k_trsm_rltn(SizeArg sz, T alpha, MatArg<T> A, MatArg<T> B, MatAr
 	}
 }
 
+// The same solve for n <= NMAX (16, 32, 64): the lower triangle of A and its
+// inverse diagonal are staged in shared memory once per CTA, and each row of
+// the right-hand side lives in registers, updated right-looking (after d_ij:
+// c_ik -= d_ij a_kj for k > j, A's column j read by every thread at once).
+// TPR threads share a row (columns interleaved, k = TPR q + h), so a row of 64
+// doubles fits in registers; the thread that owns column j passes d_ij to its
+// partner by a shuffle within the pair.  Element (i,k) sees exactly the
+// operations of k_trsm_rltn, in the same order (alpha b_ik, then the FMAs over
+// l = 0..k-1), so the results are identical; nothing is re-read from global
+// memory inside the recurrence.  64 rows per CTA, blockDim.x = 64 TPR.
+template <typename T, bool UNIT, int NMAX, int TPR>
+__global__ void __launch_bounds__(64 * TPR) k_trsm_rltn_reg(SizeArg sz, T alpha, MatArg<T> A, MatArg<T> B,
+                                                             MatArg<T> D) {
+	constexpr int NQ = NMAX / TPR;
+	__shared__ T sa[NMAX * NMAX];  // sa[j * NMAX + k] = a(k, j), k > j
+	__shared__ T sinv[NMAX];
+	const int b = blockIdx.x;
+	const int m = sz.M(b), n = sz.N(b);
+	const PMat<T> a = A.get(b), bb = B.get(b), d = D.get(b);
+	{
+		// thread t stages row t % 64 of the columns j = t / 64 (mod TPR); the
+		// loop is unrolled so every load is in flight at once
+		const int k = threadIdx.x & 63, j0 = threadIdx.x >> 6;
+#pragma unroll
+		for (int jj = 0; jj < NQ; jj++) {
+			const int j = jj * TPR + j0;
+			if (j < n && k < n && k > j) sa[j * NMAX + k] = a.at(k, j);
+		}
+		if (!UNIT && threadIdx.x < n) sinv[threadIdx.x] = a.d[threadIdx.x];
+	}
+	__syncthreads();
+	const int h = threadIdx.x % TPR;
+	const int i = blockIdx.y * 64 + threadIdx.x / TPR;
+	if (i >= m) return;  // both threads of a pair leave together
+	const int lane = threadIdx.x & 31;
+	const unsigned pair = (TPR == 1) ? (1u << lane) : (3u << (lane & ~1));
+	T c[NQ];
+#pragma unroll
+	for (int q = 0; q < NQ; q++) {
+		const int k = q * TPR + h;
+		c[q] = (k < n) ? alpha * bb.at(i, k) : T(0);
+	}
+#pragma unroll
+	for (int j = 0; j < NMAX; j++) {
+		if (j >= n) break;
+		const int qj = j / TPR, hj = j % TPR;
+		T dj = T(0);
+		if (h == hj) dj = UNIT ? c[qj] : c[qj] * sinv[j];
+		if (TPR > 1) dj = __shfl_sync(pair, dj, (lane & ~(TPR - 1)) | hj);
+		if (h == hj) c[qj] = dj;
+#pragma unroll
+		for (int q = 0; q < NQ; q++) {
+			const int k = q * TPR + h;
+			if (k > j && k < n) c[q] = fma(-dj, sa[j * NMAX + k], c[q]);
+		}
+	}
+#pragma unroll
+	for (int q = 0; q < NQ; q++) {
+		const int k = q * TPR + h;
+		if (k < n) d.at(i, k) = c[q];
+	}
+}
+
+template <typename T, bool UNIT>
+void trsm_rltn_kernel(int batch, SizeArg sz, int m, int n, T alpha, MatArg<T> A, MatArg<T> B, MatArg<T> D,
+                      cudaStream_t s) {
+	const dim3 grid(batch, cdiv(m, 64));
+	// a row of 64 doubles takes two threads (registers); everything else one
+	constexpr int TPR64 = sizeof(T) == 8 ? 2 : 1;
+	if (n <= 16)
+		k_trsm_rltn_reg<T, UNIT, 16, 1><<<grid, 64, 0, s>>>(sz, alpha, A, B, D);
+	else if (n <= 32)
+		k_trsm_rltn_reg<T, UNIT, 32, 1><<<grid, 64, 0, s>>>(sz, alpha, A, B, D);
+	else if (n <= 64)
+		k_trsm_rltn_reg<T, UNIT, 64, TPR64><<<grid, 64 * TPR64, 0, s>>>(sz, alpha, A, B, D);
+	else
+		k_trsm_rltn<T, UNIT><<<grid, 64, 0, s>>>(sz, alpha, A, B, D);
+}
+
 // D = alpha * B * A, A lower non-unit (blasfeo_hp_pm/d_blas3_lib4.c:4893).
 // D must not alias B.
 template <typename T>
@@ -224,7 +303,7 @@ int trsm_core(int batch, int m, int n, T alpha, MatArg<T> A, int ai, int aj, int
               cudaStream_t s, bool unit = false) {
 	SizeArg sz = uniform_sizes(m, n, 0);
 	if (unit) {
-		k_trsm_rltn<T, true><<<dim3(batch, cdiv(m, 64)), 64, 0, s>>>(sz, alpha, A, B, D);
+		trsm_rltn_kernel<T, true>(batch, sz, m, n, alpha, A, B, D, s);
 		return bf::check_launch();
 	}
 	// inverse diagonal of A into A's dA, reused when already valid
@@ -233,7 +312,7 @@ int trsm_core(int batch, int m, int n, T alpha, MatArg<T> A, int ai, int aj, int
 		k_invdiag<T><<<dim3(batch, cdiv(n, 128)), 128, 0, s>>>(sz, A);
 		*use_dA = (ai == 0 && aj == 0) ? n : 0;
 	}
-	k_trsm_rltn<T, false><<<dim3(batch, cdiv(m, 64)), 64, 0, s>>>(sz, alpha, A, B, D);
+	trsm_rltn_kernel<T, false>(batch, sz, m, n, alpha, A, B, D, s);
 	return bf::check_launch();
 }
 
