@@ -127,3 +127,31 @@ def test_cm_memsize_and_create_match_reference(mn):
         q = lambda off: int.from_bytes(b[off:off + 8], "little")
         i = lambda off: int.from_bytes(b[off:off + 4], "little", signed=True)
         assert (q(8), q(16), i(24), i(28), i(40), i(48)) == (s.pA, s.dA, s.m, s.n, s.use_dA, s.memsize)
+
+
+def test_cm_bad_arguments_rejected_without_gpu():
+    """The column-major entry points check their descriptors before any device
+    work: a NULL descriptor or pA records EINVAL; empty sizes are no-ops."""
+    import blasfeo_b200 as bf
+    lib = bf.lib
+    EINVAL = 1
+    lib.blasfeo_b200_last_error()  # clear
+    good = bf.cm_dmat()
+    lib.blasfeo_cm_create_dmat(8, 8, C.byref(good), C.c_void_p(0x3000))
+    empty = bf.cm_dmat()  # pA NULL
+    lib.blasfeo_cm_dpotrf_l(8, None, 0, 0, C.byref(good), 0, 0)
+    assert lib.blasfeo_b200_last_error() == EINVAL
+    lib.blasfeo_cm_dpotrf_l(8, C.byref(empty), 0, 0, C.byref(good), 0, 0)
+    assert lib.blasfeo_b200_last_error() == EINVAL
+    lib.blasfeo_cm_dgemm_nt(4, 4, -1, 1.0, C.byref(good), 0, 0, C.byref(good), 0, 0, 0.0, C.byref(good), 0, 0,
+                            C.byref(good), 0, 0)
+    assert lib.blasfeo_b200_last_error() == EINVAL
+    lib.blasfeo_cm_dgetrf_rp(4, 4, C.byref(good), 0, 0, C.byref(good), 0, 0, None)
+    assert lib.blasfeo_b200_last_error() == EINVAL
+    s = bf.cm_smat()
+    lib.blasfeo_cm_strsm_rltn(4, 4, 1.0, None, 0, 0, C.byref(s), 0, 0, C.byref(s), 0, 0)
+    assert lib.blasfeo_b200_last_error() == EINVAL
+    # empty sizes: nothing happens, nothing is recorded
+    lib.blasfeo_cm_dpotrf_l(0, None, 0, 0, None, 0, 0)
+    lib.blasfeo_cm_dgemm_nt(0, 4, 4, 1.0, None, 0, 0, None, 0, 0, 0.0, None, 0, 0, None, 0, 0)
+    assert lib.blasfeo_b200_last_error() == 0
