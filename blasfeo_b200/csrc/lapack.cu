@@ -31,8 +31,10 @@ namespace {
 __host__ __device__ inline size_t align16(size_t x) { return (x + 15) / 16 * 16; }
 
 // shared-memory plan of the potrf kernel for matrices up to max_n
+// (lower panels, FP64 reciprocal pivots, the 16x17 row-major copy of the
+// diagonal block that chol_smem's panel solve reads, the bad-pivot flag)
 struct PotrfSmem {
-	size_t s_bytes, dinv_off, invl_off, scratch_off, bad_off, total;
+	size_t s_bytes, dinv_off, lt_off, bad_off, total;
 };
 template <typename T>
 __host__ __device__ inline PotrfSmem potrf_smem_plan(int max_n) {
@@ -40,9 +42,8 @@ __host__ __device__ inline PotrfSmem potrf_smem_plan(int max_n) {
 	int P = (max_n + 3) / 4;
 	p.s_bytes = align16((size_t)lp_size(max_n) * sizeof(T));
 	p.dinv_off = p.s_bytes;
-	p.invl_off = p.dinv_off + align16((size_t)4 * P * sizeof(double));
-	p.scratch_off = p.invl_off + align16(16 * 17 * sizeof(T));
-	p.bad_off = p.scratch_off + align16((16 * 17 + 64) * sizeof(double));
+	p.lt_off = p.dinv_off + align16((size_t)4 * P * sizeof(double));
+	p.bad_off = p.lt_off + align16(16 * 17 * sizeof(T));
 	p.total = p.bad_off + 16;
 	return p;
 }
@@ -93,8 +94,7 @@ __global__ void __launch_bounds__(NT, MINB)
 	PotrfSmem pl = potrf_smem_plan<T>(max_n);
 	T *S = (T *)smem;
 	double *dinv = (double *)(smem + pl.dinv_off);
-	T *invL = (T *)(smem + pl.invl_off);
-	double *scratch = (double *)(smem + pl.scratch_off);
+	T *Lt = (T *)(smem + pl.lt_off);
 	int *bad = (int *)(smem + pl.bad_off);
 	const PMat<T> c = C.get(b), d = D.get(b);
 	if (threadIdx.x == 0) *bad = 0;
@@ -103,7 +103,7 @@ __global__ void __launch_bounds__(NT, MINB)
 	else
 		load_lower_panels<T>(S, n, c);
 	__syncthreads();
-	chol_smem<T>(S, n, dinv, invL, bad, false);
+	chol_smem<T>(S, n, dinv, Lt, bad, false);
 	if ((d.ri & 3) == 0)
 		store_lp_vec<T, 4>(S, n, d.p + (size_t)d.ri * d.cn + 4 * d.cj, d.cn);
 	else
