@@ -11,7 +11,9 @@ Two libraries share one calling convention (the BLASFEO panel-major C API with
   (symbols ``oracle_d_*`` / ``oracle_s_*``);
 * ``_ref/libblasfeo_ref_{generic,haswell}.so`` - BLASFEO 0.1.4.2 compiled from
   its own sources by oracle/Makefile (symbols ``blasfeo_*`` for the HP panel-major
-  path and ``blasfeo_ref_*`` for its REFERENCE backend).
+  path and ``blasfeo_ref_*`` for its REFERENCE backend);
+* ``_ref/libblasfeo_ref_cm_generic.so`` - the GENERIC build plus the reference's
+  column-major ``blasfeo_cm_d*`` routines (blasfeo_hp_cm/, BLAS_API).
 
 Host matrices are numpy arrays in column-major order; :class:`HostMat` packs
 them into panel-major storage (panel size 4) owned by a numpy buffer.
@@ -47,6 +49,38 @@ def oracle_lib():
 
 def ref_lib(target="generic"):
     return _lib(os.path.join(HERE, "_ref", "libblasfeo_ref_%s.so" % target))
+
+
+def ref_cm_lib():
+    """The GENERIC build plus the reference's column-major blasfeo_cm_d* routines."""
+    return _lib(os.path.join(HERE, "_ref", "libblasfeo_ref_cm_generic.so"))
+
+
+def ref_cm_available():
+    return os.path.exists(os.path.join(HERE, "_ref", "libblasfeo_ref_cm_generic.so"))
+
+
+class CmDMat(C.Structure):
+    """struct blasfeo_cm_dmat (include/blasfeo_common.h:220-229)."""
+    _fields_ = [("mem", C.c_void_p), ("pA", C.c_void_p), ("dA", C.c_void_p),
+                ("m", C.c_int), ("n", C.c_int), ("use_dA", C.c_int), ("memsize", C.c_int)]
+
+
+class HostCmMat:
+    """A column-major host matrix (leading dimension m) with a cm descriptor."""
+
+    def __init__(self, data):
+        self.a = np.asfortranarray(np.array(data, dtype=np.float64))
+        self.m, self.n = self.a.shape
+        self.dA = np.zeros(max(self.m, self.n) + 8)
+        self.desc = CmDMat()
+        self.desc.mem = self.desc.pA = self.a.ctypes.data
+        self.desc.dA = self.dA.ctypes.data
+        self.desc.m, self.desc.n = self.m, self.n
+
+    @property
+    def ref(self):
+        return C.byref(self.desc)
 
 
 def ref_available(target="generic"):

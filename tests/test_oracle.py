@@ -10,7 +10,7 @@ import os
 import numpy as np
 import pytest
 
-from tests.helpers import oracle_api, relfro
+from tests.helpers import oracle_api, relfro, spd
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 GOLD = os.path.join(HERE, "golden")
@@ -291,3 +291,128 @@ def test_reference_pack_tran_semantics(shape):
         out = np.asfortranarray(np.zeros((n, m)))
         lib.blasfeo_unpack_tran_dmat(m, n, h.ref, ai, aj, out.ctypes.data_as(C.c_void_p), n)
         assert np.array_equal(out, h.get()[ai:ai + m, aj:aj + n].T)
+
+
+# ---- the reference's column-major routines vs the panel-major oracle ----
+# The column-major drop-in stages each block into panel-major storage, runs the
+# panel-major routine and writes back the block (or the lower triangle for
+# syrk_ln / potrf_l).  These tests pin that equivalence on the reference's own
+# column-major code (blasfeo_hp_cm/, GENERIC build): same numbers as the
+# panel-major restatement on the same blocks, and nothing written outside.
+
+def _cm_ref():
+    from oracle.pyoracle import ref_cm_available, ref_cm_lib
+    if not ref_cm_available():
+        pytest.skip("column-major reference not built (make -C oracle cm)")
+    lib = ref_cm_lib()
+    return lib
+
+
+def _outside_same(got, before, r0, c0, m, n, lower=False):
+    mask = np.ones(got.shape, dtype=bool)
+    blk = np.tril(np.ones((m, n), dtype=bool)) if lower else np.ones((m, n), dtype=bool)
+    mask[r0:r0 + m, c0:c0 + n] &= ~blk
+    return np.array_equal(got[mask], before[mask])
+
+
+@pytest.mark.parametrize("case", [(17, 13, 9, 1, 2, 3, 1), (64, 64, 64, 0, 0, 0, 0), (5, 3, 7, 2, 0, 1, 4)])
+@pytest.mark.parametrize("ab", [(1.0, 0.0), (1.5, -0.5)])
+def test_cm_reference_gemm_nt_is_panel_major_gemm_on_blocks(case, ab):
+    import ctypes as C
+    from oracle.pyoracle import HostCmMat, HostMat
+    lib = _cm_ref()
+    orc = oracle_api()
+    m, n, k, ai, bi, ci, di = case
+    alpha, beta = ab
+    rng = np.random.default_rng(m + 7 * n + k)
+    A = rng.uniform(-1, 1, (m + ai + 2, k + 3))
+    B = rng.uniform(-1, 1, (n + bi + 1, k + 3))
+    Cm = rng.uniform(-1, 1, (m + ci + 3, n + 2))
+    D0 = rng.uniform(-1, 1, (m + di + 1, n + 4))
+    cA, cB, cC, cD = HostCmMat(A), HostCmMat(B), HostCmMat(Cm), HostCmMat(D0)
+    lib.blasfeo_cm_dgemm_nt(m, n, k, C.c_double(alpha), cA.ref, ai, 1, cB.ref, bi, 2, C.c_double(beta), cC.ref, ci, 1,
+                            cD.ref, di, 3)
+    pD = HostMat(*D0.shape).set(D0)
+    orc.gemm_nt("d", m, n, k, alpha, HostMat(*A.shape).set(A), ai, 1, HostMat(*B.shape).set(B), bi, 2, beta,
+                HostMat(*Cm.shape).set(Cm), ci, 1, pD, di, 3)
+    assert relfro(cD.a, pD.get()) <= 1e-13
+    assert _outside_same(cD.a, D0, di, 3, m, n)
+
+
+@pytest.mark.parametrize("mk", [(16, 32, 0), (13, 7, 1)])
+def test_cm_reference_syrk_ln_writes_lower_block(mk):
+    import ctypes as C
+    from oracle.pyoracle import HostCmMat, HostMat
+    lib = _cm_ref()
+    orc = oracle_api()
+    m, k, off = mk
+    rng = np.random.default_rng(m + 100 * k)
+    A = rng.standard_normal((m + off + 1, k))
+    Cm = rng.standard_normal((m + off, m + off))
+    D0 = rng.standard_normal((m + off + 2, m + off + 1))
+    cA, cC, cD = HostCmMat(A), HostCmMat(Cm), HostCmMat(D0)
+    lib.blasfeo_cm_dsyrk_ln(m, k, C.c_double(0.7), cA.ref, off, 0, cA.ref, off + 1, 0, C.c_double(1.3), cC.ref, off,
+                            off, cD.ref, off + 1, off)
+    hA, pD = HostMat(*A.shape).set(A), HostMat(*D0.shape).set(D0)
+    orc.syrk_ln("d", m, k, 0.7, hA, off, 0, hA, off + 1, 0, 1.3, HostMat(*Cm.shape).set(Cm), off, off, pD, off + 1, off)
+    assert relfro(cD.a, pD.get()) <= 1e-13
+    assert _outside_same(cD.a, D0, off + 1, off, m, m, lower=True)
+
+
+@pytest.mark.parametrize("mn", [(13, 21), (40, 7), (64, 64)])
+def test_cm_reference_trsm_rltn_is_panel_major_trsm(mn):
+    import ctypes as C
+    from oracle.pyoracle import HostCmMat, HostMat
+    lib = _cm_ref()
+    orc = oracle_api()
+    m, n = mn
+    rng = np.random.default_rng(m * 3 + n)
+    Abig = rng.standard_normal((n + 2, n + 1))
+    Abig[2:2 + n, 1:1 + n] = np.linalg.cholesky(spd(rng, n))
+    B = rng.standard_normal((m + 1, n + 3))
+    D0 = rng.standard_normal((m + 3, n + 2))
+    cA, cB, cD = HostCmMat(Abig), HostCmMat(B), HostCmMat(D0)
+    lib.blasfeo_cm_dtrsm_rltn(m, n, C.c_double(1.0), cA.ref, 2, 1, cB.ref, 1, 3, cD.ref, 3, 2)
+    pD = HostMat(*D0.shape).set(D0)
+    orc.trsm_rltn("d", m, n, 1.0, HostMat(*Abig.shape).set(Abig), 2, 1, HostMat(*B.shape).set(B), 1, 3, pD, 3, 2)
+    assert relfro(cD.a, pD.get()) <= 1e-12
+    assert _outside_same(cD.a, D0, 3, 2, m, n)
+
+
+@pytest.mark.parametrize("n", [1, 5, 16, 33, 64])
+def test_cm_reference_potrf_l_writes_lower_block_only(n):
+    from oracle.pyoracle import HostCmMat, HostMat
+    lib = _cm_ref()
+    orc = oracle_api()
+    rng = np.random.default_rng(n + 7)
+    big = rng.standard_normal((n + 3, n + 2))
+    big[1:1 + n, 2:2 + n] = spd(rng, n)
+    D0 = rng.standard_normal((n + 2, n + 4))
+    cC, cD = HostCmMat(big), HostCmMat(D0)
+    lib.blasfeo_cm_dpotrf_l(n, cC.ref, 1, 2, cD.ref, 2, 1)
+    pD = HostMat(*D0.shape).set(D0)
+    orc.potrf_l("d", n, HostMat(*big.shape).set(big), 1, 2, pD, 2, 1)
+    got, want = np.tril(cD.a[2:2 + n, 1:1 + n]), np.tril(pD.get()[2:2 + n, 1:1 + n])
+    assert relfro(got, want) <= 1e-13
+    assert _outside_same(cD.a, D0, 2, 1, n, n, lower=True)
+    assert cD.desc.use_dA == 0
+
+
+@pytest.mark.parametrize("mn", [(37, 20), (20, 37), (64, 64)])
+def test_cm_reference_getrf_rp_pivots_match(mn):
+    import ctypes as C
+    from oracle.pyoracle import HostCmMat, HostMat
+    lib = _cm_ref()
+    orc = oracle_api()
+    m, n = mn
+    rng = np.random.default_rng(m + 3 * n)
+    big = rng.standard_normal((m + 2, n + 1))
+    D0 = rng.standard_normal((m + 1, n + 3))
+    cC, cD = HostCmMat(big), HostCmMat(D0)
+    piv = np.zeros(min(m, n) + 8, dtype=np.int32)
+    lib.blasfeo_cm_dgetrf_rp(m, n, cC.ref, 2, 1, cD.ref, 1, 3, piv.ctypes.data_as(C.POINTER(C.c_int)))
+    pD = HostMat(*D0.shape).set(D0)
+    ppiv = orc.getrf_rp("d", m, n, HostMat(*big.shape).set(big), 2, 1, pD, 1, 3)
+    assert np.array_equal(piv[:min(m, n)], ppiv)
+    assert relfro(cD.a, pD.get()) <= 1e-12
+    assert _outside_same(cD.a, D0, 1, 3, m, n)
