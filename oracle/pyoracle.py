@@ -67,12 +67,13 @@ class CmDMat(C.Structure):
 
 
 class HostCmMat:
-    """A column-major host matrix (leading dimension m) with a cm descriptor."""
+    """A column-major host matrix (leading dimension m) with a cm descriptor
+    (struct blasfeo_cm_dmat, or blasfeo_cm_smat for float32: same layout)."""
 
-    def __init__(self, data):
-        self.a = np.asfortranarray(np.array(data, dtype=np.float64))
+    def __init__(self, data, dtype=np.float64):
+        self.a = np.asfortranarray(np.array(data, dtype=dtype))
         self.m, self.n = self.a.shape
-        self.dA = np.zeros(max(self.m, self.n) + 8)
+        self.dA = np.zeros(max(self.m, self.n) + 8, dtype=dtype)
         self.desc = CmDMat()
         self.desc.mem = self.desc.pA = self.a.ctypes.data
         self.desc.dA = self.dA.ctypes.data

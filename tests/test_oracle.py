@@ -315,9 +315,19 @@ def _outside_same(got, before, r0, c0, m, n, lower=False):
     return np.array_equal(got[mask], before[mask])
 
 
+CM_NP = {"d": np.float64, "s": np.float32}
+CM_TOL = {"d": 1e-13, "s": 2e-5}
+
+
+def _cm_real(prec, v):
+    import ctypes as C
+    return C.c_double(v) if prec == "d" else C.c_float(v)
+
+
+@pytest.mark.parametrize("prec", ["d", "s"])
 @pytest.mark.parametrize("case", [(17, 13, 9, 1, 2, 3, 1), (64, 64, 64, 0, 0, 0, 0), (5, 3, 7, 2, 0, 1, 4)])
 @pytest.mark.parametrize("ab", [(1.0, 0.0), (1.5, -0.5)])
-def test_cm_reference_gemm_nt_is_panel_major_gemm_on_blocks(case, ab):
+def test_cm_reference_gemm_nt_is_panel_major_gemm_on_blocks(prec, case, ab):
     import ctypes as C
     from oracle.pyoracle import HostCmMat, HostMat
     lib = _cm_ref()
@@ -325,17 +335,18 @@ def test_cm_reference_gemm_nt_is_panel_major_gemm_on_blocks(case, ab):
     m, n, k, ai, bi, ci, di = case
     alpha, beta = ab
     rng = np.random.default_rng(m + 7 * n + k)
-    A = rng.uniform(-1, 1, (m + ai + 2, k + 3))
-    B = rng.uniform(-1, 1, (n + bi + 1, k + 3))
-    Cm = rng.uniform(-1, 1, (m + ci + 3, n + 2))
-    D0 = rng.uniform(-1, 1, (m + di + 1, n + 4))
-    cA, cB, cC, cD = HostCmMat(A), HostCmMat(B), HostCmMat(Cm), HostCmMat(D0)
-    lib.blasfeo_cm_dgemm_nt(m, n, k, C.c_double(alpha), cA.ref, ai, 1, cB.ref, bi, 2, C.c_double(beta), cC.ref, ci, 1,
-                            cD.ref, di, 3)
-    pD = HostMat(*D0.shape).set(D0)
-    orc.gemm_nt("d", m, n, k, alpha, HostMat(*A.shape).set(A), ai, 1, HostMat(*B.shape).set(B), bi, 2, beta,
-                HostMat(*Cm.shape).set(Cm), ci, 1, pD, di, 3)
-    assert relfro(cD.a, pD.get()) <= 1e-13
+    t = CM_NP[prec]
+    A = rng.uniform(-1, 1, (m + ai + 2, k + 3)).astype(t)
+    B = rng.uniform(-1, 1, (n + bi + 1, k + 3)).astype(t)
+    Cm = rng.uniform(-1, 1, (m + ci + 3, n + 2)).astype(t)
+    D0 = rng.uniform(-1, 1, (m + di + 1, n + 4)).astype(t)
+    cA, cB, cC, cD = HostCmMat(A, t), HostCmMat(B, t), HostCmMat(Cm, t), HostCmMat(D0, t)
+    getattr(lib, "blasfeo_cm_%sgemm_nt" % prec)(m, n, k, _cm_real(prec, alpha), cA.ref, ai, 1, cB.ref, bi, 2,
+                                                _cm_real(prec, beta), cC.ref, ci, 1, cD.ref, di, 3)
+    H = lambda M: HostMat(*M.shape, dtype=t).set(M)
+    pD = H(D0)
+    orc.gemm_nt(prec, m, n, k, alpha, H(A), ai, 1, H(B), bi, 2, beta, H(Cm), ci, 1, pD, di, 3)
+    assert relfro(cD.a, pD.get()) <= CM_TOL[prec]
     assert _outside_same(cD.a, D0, di, 3, m, n)
 
 
@@ -359,41 +370,49 @@ def test_cm_reference_syrk_ln_writes_lower_block(mk):
     assert _outside_same(cD.a, D0, off + 1, off, m, m, lower=True)
 
 
+@pytest.mark.parametrize("prec", ["d", "s"])
 @pytest.mark.parametrize("mn", [(13, 21), (40, 7), (64, 64)])
-def test_cm_reference_trsm_rltn_is_panel_major_trsm(mn):
+def test_cm_reference_trsm_rltn_is_panel_major_trsm(prec, mn):
     import ctypes as C
     from oracle.pyoracle import HostCmMat, HostMat
     lib = _cm_ref()
     orc = oracle_api()
     m, n = mn
     rng = np.random.default_rng(m * 3 + n)
+    t = CM_NP[prec]
     Abig = rng.standard_normal((n + 2, n + 1))
     Abig[2:2 + n, 1:1 + n] = np.linalg.cholesky(spd(rng, n))
-    B = rng.standard_normal((m + 1, n + 3))
-    D0 = rng.standard_normal((m + 3, n + 2))
-    cA, cB, cD = HostCmMat(Abig), HostCmMat(B), HostCmMat(D0)
-    lib.blasfeo_cm_dtrsm_rltn(m, n, C.c_double(1.0), cA.ref, 2, 1, cB.ref, 1, 3, cD.ref, 3, 2)
-    pD = HostMat(*D0.shape).set(D0)
-    orc.trsm_rltn("d", m, n, 1.0, HostMat(*Abig.shape).set(Abig), 2, 1, HostMat(*B.shape).set(B), 1, 3, pD, 3, 2)
-    assert relfro(cD.a, pD.get()) <= 1e-12
+    Abig = Abig.astype(t)
+    B = rng.standard_normal((m + 1, n + 3)).astype(t)
+    D0 = rng.standard_normal((m + 3, n + 2)).astype(t)
+    cA, cB, cD = HostCmMat(Abig, t), HostCmMat(B, t), HostCmMat(D0, t)
+    getattr(lib, "blasfeo_cm_%strsm_rltn" % prec)(m, n, _cm_real(prec, 1.0), cA.ref, 2, 1, cB.ref, 1, 3, cD.ref, 3, 2)
+    H = lambda M: HostMat(*M.shape, dtype=t).set(M)
+    pD = H(D0)
+    orc.trsm_rltn(prec, m, n, 1.0, H(Abig), 2, 1, H(B), 1, 3, pD, 3, 2)
+    assert relfro(cD.a, pD.get()) <= CM_TOL[prec] * 10
     assert _outside_same(cD.a, D0, 3, 2, m, n)
 
 
+@pytest.mark.parametrize("prec", ["d", "s"])
 @pytest.mark.parametrize("n", [1, 5, 16, 33, 64])
-def test_cm_reference_potrf_l_writes_lower_block_only(n):
+def test_cm_reference_potrf_l_writes_lower_block_only(prec, n):
     from oracle.pyoracle import HostCmMat, HostMat
     lib = _cm_ref()
     orc = oracle_api()
     rng = np.random.default_rng(n + 7)
+    t = CM_NP[prec]
     big = rng.standard_normal((n + 3, n + 2))
     big[1:1 + n, 2:2 + n] = spd(rng, n)
-    D0 = rng.standard_normal((n + 2, n + 4))
-    cC, cD = HostCmMat(big), HostCmMat(D0)
-    lib.blasfeo_cm_dpotrf_l(n, cC.ref, 1, 2, cD.ref, 2, 1)
-    pD = HostMat(*D0.shape).set(D0)
-    orc.potrf_l("d", n, HostMat(*big.shape).set(big), 1, 2, pD, 2, 1)
+    big = big.astype(t)
+    D0 = rng.standard_normal((n + 2, n + 4)).astype(t)
+    cC, cD = HostCmMat(big, t), HostCmMat(D0, t)
+    getattr(lib, "blasfeo_cm_%spotrf_l" % prec)(n, cC.ref, 1, 2, cD.ref, 2, 1)
+    H = lambda M: HostMat(*M.shape, dtype=t).set(M)
+    pD = H(D0)
+    orc.potrf_l(prec, n, H(big), 1, 2, pD, 2, 1)
     got, want = np.tril(cD.a[2:2 + n, 1:1 + n]), np.tril(pD.get()[2:2 + n, 1:1 + n])
-    assert relfro(got, want) <= 1e-13
+    assert relfro(got, want) <= CM_TOL[prec]
     assert _outside_same(cD.a, D0, 2, 1, n, n, lower=True)
     assert cD.desc.use_dA == 0
 
