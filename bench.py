@@ -27,6 +27,14 @@ N(0,1) matrix and log10(lambda) ~ U[0,6], b ~ N(0,1); every system solved to
 Usage: python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 For N > 1 launch one process per GPU with torch.distributed.run; every rank
 solves its own batch (weak scaling, no data-path collective).
+
+Single-routine cases for profiling one kernel under ncu (small, seeded; every
+call goes through the C ABI, REPS calls back to back, then a check of info):
+  python bench.py --case gemm  N BATCH REPS        blasfeo_dgemm_nt_batch, m = n = k = N, A, B ~ U[-1,1], beta = 0
+  python bench.py --case potrf N BATCH REPS        blasfeo_dpotrf_l_batch on C = G G^T / N + I, G ~ N(0,1)
+  python bench.py --case posv  N BATCH REPS NMIN   blasfeo_dposv_l_vbatch, uneven SPD systems n ~ U{NMIN..N}
+  python bench.py --case sposv N BATCH REPS NMIN   blasfeo_dsposv_l_vbatch (mixed precision), same inputs
+  python bench.py --case ric   N BATCH REPS        blasfeo_dric_trf_batch, horizon N, nx = 12, nu = 4
 """
 import argparse
 import ctypes as C
@@ -61,7 +69,80 @@ def parse():
     ap.add_argument("--cpu-sample", type=int, default=4000)
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--no-fp64", action="store_true", help="skip the FP64 batched dgemm/dpotrf roofline legs")
+    ap.add_argument("--case", nargs="+", metavar="ARG",
+                    help="run one profiling case instead of the benchmark: OP N BATCH REPS [NMIN]")
     return ap.parse_args()
+
+
+def run_case(argv):
+    """One routine on a small seeded workload, for an ncu capture of its kernel."""
+    import torch
+    import blasfeo_b200 as bf
+    from blasfeo_b200.workloads import fill_batch, to_panel_major, spd_config3
+    lib = bf.lib
+    dev = torch.device("cuda")
+    op, n, batch, reps = argv[0], int(argv[1]), int(argv[2]), int(argv[3])
+    P = lambda t: C.c_void_p(t.data_ptr())
+    if op == "gemm":
+        A, B, D = bf.DMatBatch(n, n, batch), bf.DMatBatch(n, n, batch), bf.DMatBatch(n, n, batch)
+        fill_batch(A, torch.rand((batch, n, n), dtype=torch.float64, device=dev) * 2 - 1)
+        fill_batch(B, torch.rand((batch, n, n), dtype=torch.float64, device=dev) * 2 - 1)
+        for _ in range(reps):
+            bf.check(lib.blasfeo_dgemm_nt_batch(batch, n, n, n, 1.0, A.ref, 0, 0, B.ref, 0, 0, 0.0, D.ref, 0, 0,
+                                                D.ref, 0, 0, None))
+    elif op == "potrf":
+        Cm, L = bf.DMatBatch(n, n, batch), bf.DMatBatch(n, n, batch)
+        pm, cn, st = Cm.s.pm, Cm.s.cn, Cm.s.stride
+        for s0 in range(0, batch, 4096):
+            s1 = min(batch, s0 + 4096)
+            G = torch.randn((s1 - s0, n, n), dtype=torch.float64, device=dev)
+            S = G @ G.transpose(1, 2) / n + torch.eye(n, dtype=torch.float64, device=dev)
+            Cm.buf[s0 * st * 8: s1 * st * 8].view(torch.float64).view(s1 - s0, st)[:, : pm * cn] = \
+                to_panel_major(S, pm, cn)
+        info = torch.zeros(batch, dtype=torch.int32, device=dev)
+        for _ in range(reps):
+            bf.check(lib.blasfeo_dpotrf_l_batch(batch, n, Cm.ref, 0, 0, L.ref, 0, 0, P(info), None))
+        torch.cuda.synchronize()
+        assert bool((info == 0).all().item())
+    elif op in ("posv", "sposv"):
+        lo = int(argv[4]) if len(argv) > 4 else n
+        W = spd_config3(batch, nmin=lo, nmax=n, seed=3, device="cuda")
+        info = torch.zeros(batch, dtype=torch.int32, device=dev)
+        for _ in range(reps):
+            if op == "posv":
+                st = lib.blasfeo_dposv_l_vbatch(batch, P(W.nvec), W.max_n, P(W.desc), P(W.bdesc), P(W.xdesc),
+                                                P(info), None, 0, None)
+            else:
+                st = lib.blasfeo_dsposv_l_vbatch(batch, P(W.nvec), W.max_n, P(W.desc), P(W.bdesc), P(W.xdesc), 30,
+                                                 1e-12, None, None, P(info), None, 0, None)
+            bf.check(st)
+        torch.cuda.synchronize()
+        assert bool((info == 0).all().item())
+    elif op == "ric":
+        N, nx, nu = n, 12, 4
+        g = torch.Generator(device=dev)
+        g.manual_seed(4)
+        A = torch.eye(nx, dtype=torch.float64, device=dev) + 0.1 * torch.randn((batch, nx, nx), generator=g,
+                                                                              dtype=torch.float64, device=dev)
+        A = A * (0.95 / torch.linalg.eigvals(A.cpu()).abs().max(dim=1).values.to(dev))[:, None, None]
+        B = torch.randn((batch, nx, nu), generator=g, dtype=torch.float64, device=dev) / np.sqrt(nx)
+        BA = torch.zeros((batch, 16, nx), dtype=torch.float64, device=dev)
+        BA[:, :nu] = B.transpose(1, 2)
+        BA[:, nu:] = A.transpose(1, 2)
+        sBA = bf.DMatBatch(16, nx, batch * N)
+        sRSQ, sL = bf.DMatBatch(16, 16, batch * (N + 1)), bf.DMatBatch(16, 16, batch * (N + 1))
+        fill_batch(sBA, BA[:, None].expand(batch, N, 16, nx).reshape(batch * N, 16, nx).contiguous())
+        fill_batch(sRSQ, torch.eye(16, dtype=torch.float64, device=dev).expand(batch * (N + 1), 16, 16).contiguous())
+        info = torch.zeros(batch, dtype=torch.int32, device=dev)
+        for _ in range(reps):
+            bf.check(lib.blasfeo_dric_trf_batch(batch, N, nx, nu, sBA.ref, sRSQ.ref, sL.ref, P(info), None))
+        torch.cuda.synchronize()
+        assert bool((info == 0).all().item())
+    else:
+        raise SystemExit("unknown case %r" % op)
+    torch.cuda.synchronize()
+    print("ok", op, n, batch, flush=True)
+    return 0
 
 
 # ---------------------------------------------------------------------------
@@ -219,6 +300,8 @@ class Clocks:
 
 def main():
     args = parse()
+    if args.case:
+        return run_case(args.case)
     if args.impl == "reference":
         return run_reference(args)
     import torch

@@ -109,6 +109,9 @@ _sig("blasfeo_b200_set_posv_engine", _i, _i)
 _sig("blasfeo_b200_get_posv_engine", _i)
 _sig("blasfeo_b200_version", _i)
 _sig("blasfeo_b200_measure_fma_peak", _d, C.c_char, _i)
+_sig("blasfeo_b200_set_wait_limit", None, C.c_uint)
+_sig("blasfeo_b200_get_wait_limit", C.c_uint)
+_sig("blasfeo_b200_check_wait_timeout", _i, _vp, _vp)
 for p, M, V, R in (("d", _DM, _DV, _d), ("s", _SM, _SV, _f)):
     _sig("blasfeo_memsize_%smat" % p, _sz, _i, _i)
     _sig("blasfeo_memsize_diag_%smat" % p, _sz, _i, _i)

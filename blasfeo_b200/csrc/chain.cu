@@ -49,7 +49,7 @@ __global__ void __launch_bounds__(CH_WARPS * 32) k_chain16(int batch, int k, dou
                                                            const double *__restrict__ pC, long long sc,
                                                            const double *__restrict__ pG, long long sg, double *pL,
                                                            double *pLd, long long sl, double *pX, long long sx,
-                                                           double *pD, long long sd, int *info) {
+                                                           double *pD, long long sd, int *info, uint32_t wait_limit) {
 	extern __shared__ __align__(128) unsigned char smem[];
 	const ChainLayout lay = chain_layout(k);
 	const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -86,12 +86,12 @@ __global__ void __launch_bounds__(CH_WARPS * 32) k_chain16(int batch, int k, dou
 		}
 		bool ok = true;
 		if (act) {
-			ok = mbar_wait(bar, phase);
+			ok = mbar_wait(bar, phase, wait_limit);
 			phase ^= 1u;
 		}
 		if (!__all_sync(0xffffffffu, ok)) {  // a bulk copy did not complete in time
 			if (act && li == 0 && info) info[b] = -3;
-			if (act) mbar_wait(bar, phase ^ 1u);
+			if (act) mbar_wait(bar, phase ^ 1u, BF_DRAIN_LIMIT);  // drain the copy still in flight
 			return;
 		}
 		const double *A = buf;
@@ -223,7 +223,7 @@ int blasfeo_dsyrk_dpotrf_dtrsm_dgemm_batch(int batch, int m, int k, double shift
 	if (grid > need) grid = need;
 	k_chain16<<<(unsigned)grid, CH_WARPS * 32, smem, (cudaStream_t)stream>>>(
 	    batch, k, shift, sA->pA, sA->stride, sR->pA, sR->stride, sC->pA, sC->stride, sG->pA, sG->stride, sL->pA,
-	    sL->dA, sL->stride, sX->pA, sX->stride, sD->pA, sD->stride, info);
+	    sL->dA, sL->stride, sX->pA, sX->stride, sD->pA, sD->stride, info, bf::wait_limit());
 	return bf::check_launch();
 }
 

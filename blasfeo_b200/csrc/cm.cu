@@ -123,6 +123,16 @@ bool bad(const M *a) {
 	return !a || !a->pA || a->m < 0;
 }
 
+// the r x c block at (i, j) lies inside the descriptor's m x n matrix (m is
+// the leading dimension, so this also keeps every column inside its stride):
+// an out-of-range block would make the gather read, and the scatter write,
+// outside the caller's buffer
+template <typename M>
+bool bad_block(const M *a, int i, int j, int r, int c) {
+	return bad(a) || a->n < 0 || i < 0 || j < 0 || r < 0 || c < 0 || (long long)i + r > a->m ||
+	       (long long)j + c > a->n;
+}
+
 // the panel-major drop-ins, by precision
 inline void pm_gemm_nt(int m, int n, int k, double al, blasfeo_dmat *A, blasfeo_dmat *B, double be, blasfeo_dmat *C) {
 	blasfeo_dgemm_nt(m, n, k, al, A, 0, 0, B, 0, 0, be, C, 0, 0, C, 0, 0);
@@ -152,7 +162,8 @@ void cm_gemm(int m, int n, int k, T alpha, typename CmT<T>::cm *sA, int ai, int 
              int bj, T beta, typename CmT<T>::cm *sC, int ci, int cj, typename CmT<T>::cm *sD, int di, int dj,
              bool syrk) {
 	if (m <= 0 || n <= 0) return;
-	if (bad(sA) || bad(sB) || bad(sC) || bad(sD) || k < 0) {
+	if (k < 0 || bad_block(sA, ai, aj, m, k) || bad_block(sB, bi, bj, n, k) ||
+	    (beta != T(0) && bad_block(sC, ci, cj, m, n)) || (beta == T(0) && bad(sC)) || bad_block(sD, di, dj, m, n)) {
 		bf::set_error(BLASFEO_B200_EINVAL);
 		return;
 	}
@@ -186,7 +197,7 @@ template <typename T>
 void cm_trsm_rltn(int m, int n, T alpha, typename CmT<T>::cm *sA, int ai, int aj, typename CmT<T>::cm *sB, int bi,
                   int bj, typename CmT<T>::cm *sD, int di, int dj) {
 	if (m <= 0 || n <= 0) return;
-	if (bad(sA) || bad(sB) || bad(sD)) {
+	if (bad_block(sA, ai, aj, n, n) || bad_block(sB, bi, bj, m, n) || bad_block(sD, di, dj, m, n)) {
 		bf::set_error(BLASFEO_B200_EINVAL);
 		return;
 	}
@@ -210,7 +221,7 @@ void cm_trsm_rltn(int m, int n, T alpha, typename CmT<T>::cm *sA, int ai, int aj
 template <typename T>
 void cm_potrf_l(int m, typename CmT<T>::cm *sC, int ci, int cj, typename CmT<T>::cm *sD, int di, int dj) {
 	if (m <= 0) return;
-	if (bad(sC) || bad(sD)) {
+	if (bad_block(sC, ci, cj, m, m) || bad_block(sD, di, dj, m, m)) {
 		bf::set_error(BLASFEO_B200_EINVAL);
 		return;
 	}
@@ -232,7 +243,7 @@ void cm_potrf_l(int m, typename CmT<T>::cm *sC, int ci, int cj, typename CmT<T>:
 // 0-based absolute row indices (blasfeo_hp_cm/dgetrf.c:263)
 void cm_dgetrf_rp(int m, int n, blasfeo_cm_dmat *sC, int ci, int cj, blasfeo_cm_dmat *sD, int di, int dj, int *ipiv) {
 	if (m <= 0 || n <= 0) return;
-	if (bad(sC) || bad(sD) || !ipiv) {
+	if (bad_block(sC, ci, cj, m, n) || bad_block(sD, di, dj, m, n) || !ipiv) {
 		bf::set_error(BLASFEO_B200_EINVAL);
 		return;
 	}

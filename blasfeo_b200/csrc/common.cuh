@@ -34,6 +34,7 @@ void *workspace_cm(size_t bytes, cudaStream_t s);
 int num_sms();
 size_t max_smem_optin();
 int posv_engine();                        // engine of the mixed SPD solver (BLASFEO_B200_POSV_*)
+unsigned int wait_limit();                // polls of a bounded mbarrier wait (blasfeo_b200_set_wait_limit)
 
 template <typename T> struct MatT;
 template <> struct MatT<double> { typedef struct blasfeo_dmat type; typedef struct blasfeo_dmat_batch batch; typedef struct blasfeo_dvec vec; };

@@ -23,18 +23,25 @@
 //     use, so consecutive calls need no clearing by the caller;
 //   - the first call on a device looks up the device address of the array
 //     (cudaGetSymbolAddress with that device current) and caches it; make that
-//     first call on each device before any stream capture.
+//     first call on each device before any stream capture.  The cached address
+//     belongs to the device's primary context: after cudaDeviceReset the
+//     library's module is loaded again at another address, so a process that
+//     resets a device must not call this entry point on it afterwards.
 #include <mutex>
 
 #include "common.cuh"
+#include "posv.cuh"
 
 namespace {
 
 constexpr int kMaxBatch = BLASFEO_B200_NOALLOC_MAX_BATCH;
 constexpr int kMaxN = 256;
 // scratch of the fused solver for kMaxBatch systems: the work list (one int
-// per system) followed by four 16-byte-aligned tables of 10 ints
-constexpr size_t kScratchBytes = (size_t)kMaxBatch * sizeof(int) + 4 * 48;
+// per system) followed by four 16-byte-aligned tables of POSV_MAX_CLASSES
+// ints, the layout blasfeo_dposv_worksize(kMaxBatch) sizes
+constexpr size_t kScratchBytes = posv_list_bytes((size_t)kMaxBatch);
+static_assert(kScratchBytes == (size_t)kMaxBatch * sizeof(int) + 4 * posv_a16(POSV_MAX_CLASSES * sizeof(int)),
+              "work list followed by four class tables");
 
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kScratchBytes];
 

@@ -606,7 +606,7 @@ PosvLayout posv_layout(int batch, int max_n, bool use_slots) {
 	// workspace: work list and class tables, global-path factor slots,
 	// mapped-path refinement slots
 	L.gslots = L.need_global ? 4 * bf::num_sms() : 0;
-	L.need = a16((size_t)batch * sizeof(int)) + 4 * a16(POSV_MAX_CLASSES * sizeof(int));
+	L.need = posv_list_bytes((size_t)batch);
 	L.slots_off = L.need;
 	L.need += (size_t)L.gslots * posv_slot_elems(max_n) * sizeof(double);
 	L.rslots_off = a16(L.need);
@@ -698,7 +698,7 @@ extern "C" {
 
 size_t blasfeo_dposv_worksize(int batch) {
 	// list + class tables (enough for every system that takes a shared-memory kernel)
-	return a16((size_t)(batch > 0 ? batch : 0) * sizeof(int)) + 4 * a16(POSV_MAX_CLASSES * sizeof(int));
+	return posv_list_bytes((size_t)(batch > 0 ? batch : 0));
 }
 
 size_t blasfeo_dposv_worksize_n(int batch, int max_n, int mixed) {

@@ -4,6 +4,14 @@
 
 constexpr int POSV_MAX_CLASSES = 12;
 
+// bytes of the work list and class tables of one call of `batch` systems: the
+// list (one int per system), then the start, count and claim-counter tables
+// and a spare one, each 16-byte aligned
+constexpr size_t posv_a16(size_t x) { return (x + 15) / 16 * 16; }
+constexpr size_t posv_list_bytes(size_t batch) {
+	return posv_a16(batch * sizeof(int)) + 4 * posv_a16(POSV_MAX_CLASSES * sizeof(int));
+}
+
 // engine of the mixed solver when the caller asks for the default: 1 = the
 // tensor-core kernel (posv_tc.cu), 0 = the SIMT kernel (posv.cu)
 #define POSV_TENSOR_DEFAULT 0

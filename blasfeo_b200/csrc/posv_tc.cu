@@ -397,7 +397,7 @@ template <int NT>
 __global__ void __launch_bounds__(NT, 1)
     k_posv_tc(int cls, int U, PosvWs ws, const int *__restrict__ nvec, const DevDesc<double> *__restrict__ sA,
               const DevVec<double> *__restrict__ sb, const DevVec<double> *__restrict__ sx, int max_iter, double tol,
-              int *iters, double *berr, int *info, uint32_t tmem_cols) {
+              int *iters, double *berr, int *info, uint32_t tmem_cols, uint32_t wait_limit) {
 	extern __shared__ __align__(1024) unsigned char smem[];
 	const TcPlan pl = tc_plan(U);
 	float *Ph = (float *)(smem + pl.ph);
@@ -501,7 +501,7 @@ __global__ void __launch_bounds__(NT, 1)
 		for (int K = 0; K < NB; K++) {
 			const int c0 = 16 * K;
 			if (K > 0) {
-				if (!mbar_wait(mbar, phase)) *s_err = 1;
+				if (!mbar_wait(mbar, phase, wait_limit)) *s_err = 1;
 				phase ^= 1u;
 				tc_fence_after();
 			}
@@ -624,7 +624,7 @@ __global__ void __launch_bounds__(NT, 1)
 
 	// teardown: tensor-core work finished (every commit was waited for, or a
 	// last bounded wait after a timeout), then free the tensor memory
-	if (*s_err) mbar_wait(mbar, phase ^ 1u);
+	if (*s_err) mbar_wait(mbar, phase ^ 1u, BF_DRAIN_LIMIT);
 	tc_fence_before();
 	__syncthreads();
 	tc_fence_after();
@@ -657,7 +657,7 @@ int launch_tc(int cls, int U, int batch, PosvWs ws, const int *n, const void *sA
 	int grid = bf::num_sms() * per_sm;
 	if (grid > batch) grid = batch;
 	kern<<<grid, NT, smem, s>>>(cls, U, ws, n, (const DevDesc<double> *)sA, (const DevVec<double> *)sb,
-	                            (const DevVec<double> *)sx, max_iter, tol, iters, berr, info, cols);
+	                            (const DevVec<double> *)sx, max_iter, tol, iters, berr, info, cols, bf::wait_limit());
 	return bf::check_launch();
 }
 

@@ -55,7 +55,7 @@ __device__ __forceinline__ int pm_idx(int i, int j, int cn) { return (i & ~3) * 
 template <typename T>
 __global__ void __launch_bounds__(RIC_WARPS * 32) k_ric_trf(int batch, int N, int nx, int nu, const T *__restrict__ pBA,
                                                            long long sba, const T *__restrict__ pRSQ, long long srsq,
-                                                           T *pL, T *pLd, long long sl, int *info) {
+                                                           T *pL, T *pLd, long long sl, int *info, uint32_t wait_limit) {
 	extern __shared__ __align__(128) unsigned char smem[];
 	const RicLayout<T> lay = ric_layout<T>(nx);
 	const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -100,10 +100,11 @@ __global__ void __launch_bounds__(RIC_WARPS * 32) k_ric_trf(int batch, int N, in
 				else if (b + nw < batch)
 					issue(b + nw, N, slot ^ 1);
 			}
-			if (!mbar_wait(&bar[slot], phase[slot])) {
+			if (!mbar_wait(&bar[slot], phase[slot], wait_limit)) {
 				if (lane == 0 && info) info[b] = -3;
-				mbar_wait(&bar[slot], phase[slot]);
-				mbar_wait(&bar[slot ^ 1], phase[slot ^ 1]);
+				// drain both slots' copies before the warp leaves
+				mbar_wait(&bar[slot], phase[slot], BF_DRAIN_LIMIT);
+				mbar_wait(&bar[slot ^ 1], phase[slot ^ 1], BF_DRAIN_LIMIT);
 				return;
 			}
 			phase[slot] ^= 1u;
@@ -196,7 +197,7 @@ int ric_run(int batch, int N, int nx, int nu, BT *sBA, BT *sRSQ, BT *sL, int *in
 	if (grid > need) grid = need;
 	k_ric_trf<T><<<(unsigned)grid, RIC_WARPS * 32, smem, (cudaStream_t)stream>>>(
 	    batch, N, nx, nu, N > 0 ? sBA->pA : nullptr, N > 0 ? sBA->stride : 0, sRSQ->pA, sRSQ->stride, sL->pA, sL->dA,
-	    sL->stride, info);
+	    sL->stride, info, bf::wait_limit());
 	return bf::check_launch();
 }
 

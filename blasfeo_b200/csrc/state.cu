@@ -1,6 +1,7 @@
 // Library state: error recording, the stream of the single-instance entry
 // points, the synchronous/asynchronous switch, and the library-owned device
 // workspace used when a caller passes no workspace.
+#include <atomic>
 #include <vector>
 
 #include "common.cuh"
@@ -11,6 +12,8 @@ static thread_local int g_last_error = BLASFEO_B200_OK;
 static thread_local cudaStream_t g_stream = nullptr;
 static thread_local int g_sync = 1;
 static thread_local int g_posv_engine = BLASFEO_B200_POSV_DEFAULT;
+// polls of a bounded mbarrier wait in the kernels that use bulk copies (process-wide)
+static std::atomic<unsigned int> g_wait_limit{1u << 24};
 
 void set_error(int status) {
 	if (status != BLASFEO_B200_OK) g_last_error = status;
@@ -27,6 +30,7 @@ int check_launch() {
 
 cudaStream_t cur_stream() { return g_stream; }
 int posv_engine() { return g_posv_engine; }
+unsigned int wait_limit() { return g_wait_limit.load(std::memory_order_relaxed); }
 bool sync_mode() { return g_sync != 0; }
 
 int finish_single() {
@@ -154,5 +158,7 @@ int blasfeo_b200_set_posv_engine(int engine) {
 }
 int blasfeo_b200_get_posv_engine(void) { return bf::g_posv_engine; }
 int blasfeo_b200_version(void) { return 100; }
+void blasfeo_b200_set_wait_limit(unsigned int polls) { bf::g_wait_limit.store(polls ? polls : (1u << 24)); }
+unsigned int blasfeo_b200_get_wait_limit(void) { return bf::wait_limit(); }
 
 }  // extern "C"

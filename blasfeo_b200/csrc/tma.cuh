@@ -2,12 +2,19 @@
 //
 // Only untiled bulk copies from this GPU's own global memory into the
 // issuing CTA's shared memory are used (no cluster multicast).  Every wait on
-// an mbarrier is bounded: after BF_WAIT_LIMIT polls it gives up and reports
-// a timeout to the caller, which records an error and returns.
+// an mbarrier is bounded: after `limit` polls (a kernel argument, set per
+// process by blasfeo_b200_set_wait_limit, default BF_WAIT_LIMIT, about one
+// second) it gives up and reports a timeout to the caller, which records
+// info = -3 and returns.  Before returning, a kernel whose copies may still be
+// in flight waits for them once more with the fixed BF_DRAIN_LIMIT (about four
+// seconds), so that no copy lands in the shared memory of an exited block
+// unless it is stuck for that long too: the drain is best effort, bounded like
+// every other wait.
 #pragma once
 #include <stdint.h>
 
 #define BF_WAIT_LIMIT (1u << 24)
+#define BF_DRAIN_LIMIT (1u << 26)
 
 __device__ __forceinline__ uint32_t smem_u32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
 
@@ -44,9 +51,9 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity) {
 	return ok != 0;
 }
 
-// bounded wait for phase `parity` of bar; false on timeout
-__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity) {
-	for (uint32_t it = 0; it < BF_WAIT_LIMIT; it++) {
+// bounded wait for phase `parity` of bar; false after `limit` polls
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, uint32_t limit) {
+	for (uint32_t it = 0; it < limit; it++) {
 		if (mbar_try_wait(bar, parity)) return true;
 		if (it > 64) __nanosleep(64);
 	}

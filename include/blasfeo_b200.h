@@ -118,6 +118,19 @@ int blasfeo_b200_version(void);
 /* measured FMA throughput (GFLOP/s) of the current device, prec 'd' or 's';
  * the roofline denominator of the SIMT kernels (no reference counterpart) */
 double blasfeo_b200_measure_fma_peak(char prec, int iters);
+/* Polls of every bounded mbarrier wait of the kernels that use bulk copies
+ * (the fused n=16 chain, the batched Riccati factorization, the tensor-memory
+ * engine of the mixed solver), process-wide; 0 restores the default (2^24
+ * polls, about one second).  A wait that runs out sets the instance's
+ * info = -3 and the kernel returns after draining its copies (no reference
+ * counterpart: the reference has no asynchronous copies). */
+void blasfeo_b200_set_wait_limit(unsigned int polls);
+unsigned int blasfeo_b200_get_wait_limit(void);
+/* Self-check of that timeout path: one warp waits, with the current limit, on
+ * an mbarrier armed for data that no copy delivers; *status (device int)
+ * receives -3 when the wait ran out (0 if it did not).  Asynchronous on
+ * `stream`. */
+int blasfeo_b200_check_wait_timeout(int *status, void *stream);
 
 /* ---- storage: auxiliary/d_aux_lib4.c:1519,1548,1575,1588 / include/blasfeo_d_aux.h ---- */
 size_t blasfeo_memsize_dmat(int m, int n);

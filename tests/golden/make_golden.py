@@ -8,8 +8,10 @@ Every output stored here comes from the reference library itself (its
 LA=HIGH_PERFORMANCE panel-major routines ``blasfeo_*``, TARGET=GENERIC so the
 single-precision layout is the ps=4 one used on the device), called on the
 seeded inputs that are stored next to them.  The oracle restatement and the GPU
-kernels are both checked against these files (tests/test_oracle.py,
-tests/test_gpu_golden.py); tests/golden/manifest.json records their SHA-256.
+kernels are both checked against these files (the oracle in
+tests/test_oracle.py; the GPU kernels in tests/test_gpu_chain.py,
+tests/test_gpu_riccati.py and tests/test_gpu_adjacent.py);
+tests/golden/manifest.json records their SHA-256.
 """
 import hashlib
 import json

@@ -155,3 +155,61 @@ def test_cm_bad_arguments_rejected_without_gpu():
     lib.blasfeo_cm_dpotrf_l(0, None, 0, 0, None, 0, 0)
     lib.blasfeo_cm_dgemm_nt(0, 4, 4, 1.0, None, 0, 0, None, 0, 0, 0.0, None, 0, 0, None, 0, 0)
     assert lib.blasfeo_b200_last_error() == 0
+
+
+def test_cm_out_of_range_blocks_rejected_without_gpu():
+    """Every operand block of the column-major entry points must lie inside its
+    descriptor's m x n matrix (m is the leading dimension): a negative offset
+    or a block that runs past the last row or column records EINVAL before any
+    staging kernel could read or write outside the caller's buffer."""
+    import blasfeo_b200 as bf
+    lib = bf.lib
+    EINVAL = 1
+    lib.blasfeo_b200_last_error()  # clear
+    a = bf.cm_dmat()
+    lib.blasfeo_cm_create_dmat(8, 6, C.byref(a), C.c_void_p(0x3000))
+    A = C.byref(a)
+    bad_calls = [
+        # gemm_nt: A m x k at (ai, aj), B n x k, C and D m x n
+        lambda: lib.blasfeo_cm_dgemm_nt(4, 4, 4, 1.0, A, -1, 0, A, 0, 0, 0.0, A, 0, 0, A, 0, 0),
+        lambda: lib.blasfeo_cm_dgemm_nt(4, 4, 4, 1.0, A, 5, 0, A, 0, 0, 0.0, A, 0, 0, A, 0, 0),
+        lambda: lib.blasfeo_cm_dgemm_nt(4, 4, 4, 1.0, A, 0, 3, A, 0, 0, 0.0, A, 0, 0, A, 0, 0),
+        lambda: lib.blasfeo_cm_dgemm_nt(4, 4, 4, 1.0, A, 0, 0, A, 0, -2, 0.0, A, 0, 0, A, 0, 0),
+        lambda: lib.blasfeo_cm_dgemm_nt(4, 4, 4, 1.0, A, 0, 0, A, 0, 0, 1.0, A, 6, 0, A, 0, 0),
+        lambda: lib.blasfeo_cm_dgemm_nt(4, 4, 4, 1.0, A, 0, 0, A, 0, 0, 0.0, A, 0, 0, A, 0, 3),
+        lambda: lib.blasfeo_cm_dgemm_nt(9, 4, 4, 1.0, A, 0, 0, A, 0, 0, 0.0, A, 0, 0, A, 0, 0),
+        # syrk_ln: D m x m
+        lambda: lib.blasfeo_cm_dsyrk_ln(7, 2, 1.0, A, 0, 0, A, 0, 0, 0.0, A, 0, 0, A, 0, 0),
+        # trsm_rltn: A n x n, B and D m x n
+        lambda: lib.blasfeo_cm_dtrsm_rltn(4, 6, 1.0, A, 3, 0, A, 0, 0, A, 0, 0),
+        lambda: lib.blasfeo_cm_dtrsm_rltn(4, 4, 1.0, A, 0, 0, A, 0, 0, A, 0, -1),
+        # potrf_l: m x m
+        lambda: lib.blasfeo_cm_dpotrf_l(6, A, 0, 1, A, 0, 0),
+        lambda: lib.blasfeo_cm_dpotrf_l(6, A, 0, 0, A, 3, 0),
+        # getrf_rp: m x n
+        lambda: lib.blasfeo_cm_dgetrf_rp(8, 6, A, 1, 0, A, 0, 0, (C.c_int * 8)()),
+        lambda: lib.blasfeo_cm_dgetrf_rp(8, 7, A, 0, 0, A, 0, 0, (C.c_int * 8)()),
+    ]
+    for i, call in enumerate(bad_calls):
+        call()
+        assert lib.blasfeo_b200_last_error() == EINVAL, i
+    s = bf.cm_smat()
+    lib.blasfeo_cm_create_smat(8, 6, C.byref(s), C.c_void_p(0x3000))
+    lib.blasfeo_cm_strsm_rltn(4, 6, 1.0, C.byref(s), 3, 0, C.byref(s), 0, 0, C.byref(s), 0, 0)
+    assert lib.blasfeo_b200_last_error() == EINVAL
+    lib.blasfeo_cm_spotrf_l(7, C.byref(s), 0, 0, C.byref(s), 0, 0)
+    assert lib.blasfeo_b200_last_error() == EINVAL
+    lib.blasfeo_cm_sgemm_nt(4, 4, 7, 1.0, C.byref(s), 0, 0, C.byref(s), 0, 0, 0.0, C.byref(s), 0, 0, C.byref(s), 0, 0)
+    assert lib.blasfeo_b200_last_error() == EINVAL
+
+
+def test_wait_limit_setting():
+    import blasfeo_b200 as bf
+    lib = bf.lib
+    default = lib.blasfeo_b200_get_wait_limit()
+    assert default == 1 << 24
+    lib.blasfeo_b200_set_wait_limit(1000)
+    assert lib.blasfeo_b200_get_wait_limit() == 1000
+    lib.blasfeo_b200_set_wait_limit(0)
+    assert lib.blasfeo_b200_get_wait_limit() == default
+    assert lib.blasfeo_b200_check_wait_timeout(None, None) == 1

@@ -8,7 +8,7 @@ import os
 import numpy as np
 import pytest
 
-from tests.helpers import oracle_api, relfro
+from tests.helpers import oracle_api, relfro, tol
 
 pytestmark = pytest.mark.gpu
 NP = {"d": np.float64, "s": np.float32}
@@ -57,24 +57,24 @@ def test_adjacent_vs_golden(bf, prec):
     fn(bf, prec, "syrk_ln_mn")(m, n, k, 0.5, dev(bf, m, k, prec, A), 0, 0, dev(bf, n, k, prec, B), 0, 0, -1.5,
                                dev(bf, m, n, prec, Cm), 0, 0, dD, 0, 0)
     want = g[prec + "_syrkmn_D"]
-    assert relfro(np.tril(dD.unpack()), np.tril(want)) <= TOL[prec] * 10
+    assert relfro(np.tril(dD.unpack()), np.tril(want)) <= tol(prec, 10)
     dY = dev(bf, m, n, prec)
     fn(bf, prec, "trsm_rltu")(m, n, 1.25, dev(bf, n, n, prec, g[prec + "_trsmu_L"]), 0, 0,
                               dev(bf, m, n, prec, g[prec + "_trsmu_X"]), 0, 0, dY, 0, 0)
-    assert relfro(dY.unpack(), g[prec + "_trsmu_Y"]) <= TOL[prec] * 10
+    assert relfro(dY.unpack(), g[prec + "_trsmu_Y"]) <= tol(prec, 10)
     dP = dev(bf, m, m, prec)
     fn(bf, prec, "potrf_l_mn")(m, n, dev(bf, m, m, prec, g[prec + "_potrfmn_S"]), 0, 0, dP, 0, 0)
     Lw = g[prec + "_potrfmn_L"]
-    assert relfro(np.tril(dP.unpack())[:, :n], np.tril(Lw)[:, :n]) <= TOL[prec] * 10
-    assert relfro(dP.diag_array(n), g[prec + "_potrfmn_dA"]) <= TOL[prec] * 10
+    assert relfro(np.tril(dP.unpack())[:, :n], np.tril(Lw)[:, :n]) <= tol(prec, 10)
+    assert relfro(dP.diag_array(n), g[prec + "_potrfmn_dA"]) <= tol(prec, 10)
     assert dP.use_dA == 1
     for tag in ("sq", "rect"):
         M = g[prec + "_lunp_%s_in" % tag]
         r, c = M.shape
         dLU = dev(bf, r, c, prec)
         fn(bf, prec, "getrf_np")(r, c, dev(bf, r, c, prec, M), 0, 0, dLU, 0, 0)
-        assert relfro(dLU.unpack(), g[prec + "_lunp_%s" % tag]) <= TOL[prec] * 10, tag
-        assert relfro(dLU.diag_array(min(r, c)), g[prec + "_lunp_%s_dA" % tag]) <= TOL[prec] * 10, tag
+        assert relfro(dLU.unpack(), g[prec + "_lunp_%s" % tag]) <= tol(prec, 10), tag
+        assert relfro(dLU.diag_array(min(r, c)), g[prec + "_lunp_%s_dA" % tag]) <= tol(prec, 10), tag
 
 
 @pytest.mark.parametrize("prec", ["d", "s"])
@@ -110,9 +110,9 @@ def test_adjacent_offsets_vs_oracle(bf, orc, prec, off):
     fn(bf, prec, "getrf_np")(m, n, dev(bf, m + oi, n + oj, prec, M), oi, oj, dLU, od, od)
     # untouched parts (upper part of the trapezoids, columns >= n of the potrf target) keep D0
     for name, d, h in (("syrk", dD, hD), ("trsm", dY, hY), ("potrf", dP, hP), ("getrf", dLU, hLU)):
-        assert relfro(d.unpack(), h.get()) <= TOL[prec] * 10, name
-    assert relfro(dP.diag_array(n), hP.diag(n)) <= TOL[prec] * 10
-    assert relfro(dLU.diag_array(n), hLU.diag(n)) <= TOL[prec] * 10
+        assert relfro(d.unpack(), h.get()) <= tol(prec, 10), name
+    assert relfro(dP.diag_array(n), hP.diag(n)) <= tol(prec, 10)
+    assert relfro(dLU.diag_array(n), hLU.diag(n)) <= tol(prec, 10)
     assert dP.use_dA == (1 if od == 0 else 0) and dLU.use_dA == (1 if od == 0 else 0)
 
 
@@ -155,14 +155,14 @@ def test_adjacent_batches_vs_oracle(bf, orc, prec):
         hD = host(m, n, prec, np.zeros((m, n)))
         orc.syrk_ln_mn(prec, m, n, k, 2.0, host(m, k, prec, A[b]), 0, 0, host(n, k, prec, B[b]), 0, 0, -1.0,
                        host(m, n, prec, Cm[b]), 0, 0, hD, 0, 0)
-        assert relfro(gD[b], hD.get()) <= TOL[prec] * 10
+        assert relfro(gD[b], hD.get()) <= tol(prec, 10)
         hY = host(m, n, prec)
         orc.trsm_rltu(prec, m, n, 1.0, host(n, n, prec, L[b]), 0, 0, host(m, n, prec, X[b]), 0, 0, hY, 0, 0)
-        assert relfro(gY[b], hY.get()) <= TOL[prec] * 10
+        assert relfro(gY[b], hY.get()) <= tol(prec, 10)
         hP = host(m, m, prec)
         orc.potrf_l_mn(prec, m, n, host(m, m, prec, S[b]), 0, 0, hP, 0, 0)
         if b != 4:
-            assert relfro(np.tril(gP[b])[:, :n], np.tril(hP.get())[:, :n]) <= TOL[prec] * 10
+            assert relfro(np.tril(gP[b])[:, :n], np.tril(hP.get())[:, :n]) <= tol(prec, 10)
         hLU = host(m, n, prec)
         orc.getrf_np(prec, m, n, host(m, n, prec, M[b]), 0, 0, hLU, 0, 0)
-        assert relfro(gLU[b], hLU.get()) <= TOL[prec] * 10
+        assert relfro(gLU[b], hLU.get()) <= tol(prec, 10)

@@ -62,8 +62,8 @@ def test_chain_random_batch_vs_oracle_and_inverse_diag(bf):
         assert relfro(np.tril(L[b]), Lr) <= 1e-13
         assert relfro(dg[b], 1 / np.diag(Lr)) <= 1e-13
         Xr = np.linalg.solve(Lr, R[b].T).T
-        assert relfro(X[b], Xr) <= 1e-12
-        assert relfro(D[b], Cm[b] - Xr @ G[b].T) <= 1e-12
+        assert relfro(X[b], Xr) <= 1e-13
+        assert relfro(D[b], Cm[b] - Xr @ G[b].T) <= 1e-13
     # upper triangle of L untouched (left as allocated: zeros)
     assert np.abs(np.triu(L, 1)).max() == 0.0
 
@@ -93,12 +93,12 @@ def test_chain_odd_k_and_graph_of_unfused_calls(bf):
     graph.replay()
     torch.cuda.synchronize()
     assert relfro(np.tril(dL.unpack_all()), np.tril(uL.unpack_all())) <= 1e-13
-    assert relfro(dX.unpack_all(), uX.unpack_all()) <= 1e-12
-    assert relfro(dD.unpack_all(), uD.unpack_all()) <= 1e-12
+    assert relfro(dX.unpack_all(), uX.unpack_all()) <= 1e-13
+    assert relfro(dD.unpack_all(), uD.unpack_all()) <= 1e-13
     # replaying again gives the same result (every output is written from unchanged inputs)
     graph.replay()
     torch.cuda.synchronize()
-    assert relfro(dD.unpack_all(), uD.unpack_all()) <= 1e-12
+    assert relfro(dD.unpack_all(), uD.unpack_all()) <= 1e-13
 
 
 def test_chain_rejects_unsupported(bf):

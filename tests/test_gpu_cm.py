@@ -7,7 +7,7 @@ leave everything outside the block (or triangle) it writes untouched."""
 import numpy as np
 import pytest
 
-from tests.helpers import oracle_api, relfro, spd
+from tests.helpers import oracle_api, relfro, spd, tol
 
 pytestmark = pytest.mark.gpu
 
@@ -113,7 +113,7 @@ def test_cm_trsm_rltn(bf, orc, prec, mn):
     assert np.array_equal(got[3:3 + m, 2:2 + n], pD.unpack()[3:3 + m, 2:2 + n])
     hA, hB, hD = host(prec, Abig), host(prec, B), host(prec, D0)
     orc.trsm_rltn(prec, m, n, 1.0, hA, 2, 1, hB, 1, 3, hD, 3, 2)
-    assert relfro(got, hD.get()) <= TOL[prec] * 10
+    assert relfro(got, hD.get()) <= tol(prec, 10)
     assert outside_unchanged(got, D0, 3, 2, m, n)
 
 
@@ -134,7 +134,7 @@ def test_cm_potrf_l(bf, orc, prec, n):
     assert np.array_equal(got[2:2 + n, 1:1 + n][blk], pD.unpack()[2:2 + n, 1:1 + n][blk])
     hC, hD = host(prec, big), host(prec, D0)
     orc.potrf_l(prec, n, hC, 1, 2, hD, 2, 1)
-    assert relfro(np.tril(got[2:2 + n, 1:1 + n]), np.tril(hD.get()[2:2 + n, 1:1 + n])) <= TOL[prec] * (10 if n > 100 else 1)
+    assert relfro(np.tril(got[2:2 + n, 1:1 + n]), np.tril(hD.get()[2:2 + n, 1:1 + n])) <= tol(prec, 10 if n > 100 else 1)
     assert outside_unchanged(got, D0, 2, 1, n, n, lower=True)
 
 
@@ -172,5 +172,5 @@ def test_cm_getrf_rp(bf, orc, mn):
     hC, hD = host("d", big), host("d", D0)
     hpiv = orc.getrf_rp("d", m, n, hC, 2, 1, hD, 1, 3)
     assert np.array_equal(piv, hpiv)
-    assert relfro(got, hD.get()) <= 1e-12
+    assert relfro(got, hD.get()) <= 1e-13
     assert outside_unchanged(got, D0, 1, 3, m, n)

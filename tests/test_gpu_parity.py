@@ -8,7 +8,7 @@ tolerances of this port: relative Frobenius error <= 1e-13 in FP64 and
 import numpy as np
 import pytest
 
-from tests.helpers import oracle_api, relfro, spd
+from tests.helpers import oracle_api, relfro, spd, tol
 
 pytestmark = pytest.mark.gpu
 
@@ -44,7 +44,9 @@ def dev(bf, m, n, prec, data=None):
 
 
 GEMM_CASES = [(64, 64, 64, 0, 0, 0, 0), (16, 16, 16, 0, 0, 0, 0), (17, 13, 9, 0, 0, 0, 0), (5, 3, 7, 1, 2, 3, 1),
-              (1, 1, 1, 0, 0, 0, 0), (33, 70, 21, 2, 1, 0, 3), (130, 65, 40, 0, 0, 0, 0), (8, 8, 0, 0, 0, 0, 0)]
+              (1, 1, 1, 0, 0, 0, 0), (33, 70, 21, 2, 1, 0, 3), (130, 65, 40, 0, 0, 0, 0), (8, 8, 0, 0, 0, 0, 0),
+              # the mixed-op stream's largest sizes (m, n, k up to 384)
+              (384, 384, 384, 0, 0, 0, 0), (300, 384, 211, 0, 0, 0, 0), (384, 97, 384, 3, 0, 1, 2)]
 
 
 @pytest.mark.parametrize("prec", ["d", "s"])
@@ -81,7 +83,7 @@ def test_syrk_ln(bf, orc, prec, mk):
     assert relfro(dD.unpack(), hD.get()) <= TOL[prec]
 
 
-POTRF_N = [1, 2, 3, 4, 5, 7, 13, 16, 17, 31, 33, 60, 64, 100, 129, 200, 257]
+POTRF_N = [1, 2, 3, 4, 5, 7, 13, 16, 17, 31, 33, 60, 64, 100, 129, 200, 257, 300, 384]
 
 
 @pytest.mark.parametrize("prec", ["d", "s"])
@@ -94,8 +96,8 @@ def test_potrf_l(bf, orc, prec, n):
     orc.potrf_l(prec, n, hC, 0, 0, hD, 0, 0)
     dC, dD = dev(bf, n, n, prec, S), dev(bf, n, n, prec, D0)
     getattr(bf, "blasfeo_%spotrf_l" % prec)(n, dC, 0, 0, dD, 0, 0)
-    assert relfro(dD.unpack(), hD.get()) <= TOL[prec] * (10 if n > 100 else 1)
-    assert relfro(dD.diag_array(n), hD.diag(n)) <= TOL[prec] * 10
+    assert relfro(dD.unpack(), hD.get()) <= tol(prec, 10 if n > 100 else 1)
+    assert relfro(dD.diag_array(n), hD.diag(n)) <= tol(prec, 10)
     assert dD.use_dA == n
 
 
@@ -128,12 +130,13 @@ def test_potrf_l_not_spd(bf, orc, prec):
     getattr(bf, "blasfeo_%spotrf_l" % prec)(n, dC, 0, 0, dD, 0, 0)
     got, ref = dD.unpack(), hD.get()
     assert np.all(np.isfinite(got) == np.isfinite(ref))
-    assert relfro(np.nan_to_num(got), np.nan_to_num(ref)) <= TOL[prec] * 100
+    assert relfro(np.nan_to_num(got), np.nan_to_num(ref)) <= tol(prec, 100)
     assert dD.diag_array(n)[5] == 0.0
 
 
 @pytest.mark.parametrize("prec", ["d", "s"])
-@pytest.mark.parametrize("mn", [(64, 64, 0, 0), (16, 16, 0, 0), (19, 13, 0, 0), (7, 30, 2, 1), (1, 1, 0, 0)])
+@pytest.mark.parametrize("mn", [(64, 64, 0, 0), (16, 16, 0, 0), (19, 13, 0, 0), (7, 30, 2, 1), (1, 1, 0, 0),
+                                (100, 130, 0, 0), (64, 384, 1, 3), (384, 200, 0, 0)])
 @pytest.mark.parametrize("alpha", [1.0, -2.0])
 def test_trsm_rltn(bf, orc, prec, mn, alpha):
     m, n, bi, di = mn
@@ -148,7 +151,7 @@ def test_trsm_rltn(bf, orc, prec, mn, alpha):
     getattr(bf, "blasfeo_%spotrf_l" % prec)(n, dS, 0, 0, dL, 0, 0)
     dB, dD = dev(bf, m + bi, n, prec, X), dev(bf, m + di, n, prec, np.zeros((m + di, n)))
     getattr(bf, "blasfeo_%strsm_rltn" % prec)(m, n, alpha, dL, 0, 0, dB, bi, 0, dD, di, 0)
-    assert relfro(dD.unpack(), hD.get()) <= TOL[prec] * 10
+    assert relfro(dD.unpack(), hD.get()) <= tol(prec, 10)
 
 
 @pytest.mark.parametrize("prec", ["d", "s"])
@@ -162,13 +165,14 @@ def test_trsm_rltn_uncached_diag(bf, orc, prec):
     orc.trsm_rltn(prec, m, n, 1.0, hL, 0, 0, hB, 0, 0, hD, 0, 0)
     dL, dB, dD = dev(bf, n, n, prec, L), dev(bf, m, n, prec, X), dev(bf, m, n, prec, np.zeros((m, n)))
     getattr(bf, "blasfeo_%strsm_rltn" % prec)(m, n, 1.0, dL, 0, 0, dB, 0, 0, dD, 0, 0)
-    assert relfro(dD.unpack(), hD.get()) <= TOL[prec] * 10
+    assert relfro(dD.unpack(), hD.get()) <= tol(prec, 10)
     assert dL.use_dA == n
     assert relfro(dL.diag_array(n), hL.diag(n)) <= TOL[prec]
 
 
 @pytest.mark.parametrize("prec", ["d", "s"])
-@pytest.mark.parametrize("mn", [(64, 64), (16, 16), (1, 1), (5, 5), (37, 37), (40, 23), (23, 40), (130, 130)])
+@pytest.mark.parametrize("mn", [(64, 64), (16, 16), (1, 1), (5, 5), (37, 37), (40, 23), (23, 40), (130, 130),
+                                (300, 300), (384, 384), (384, 250)])
 def test_getrf_rp(bf, orc, prec, mn):
     m, n = mn
     rng = np.random.default_rng(m * 3 + n)
@@ -178,7 +182,7 @@ def test_getrf_rp(bf, orc, prec, mn):
     dC, dD = dev(bf, m, n, prec, M), dev(bf, m, n, prec)
     piv = getattr(bf, "blasfeo_%sgetrf_rp" % prec)(m, n, dC, 0, 0, dD, 0, 0)
     assert np.array_equal(piv, piv_ref)
-    tol = TOL[prec] * (100 if prec == "s" else 10)
+    tol = tol(prec, 100)
     assert relfro(dD.unpack(), hD.get()) <= tol
     k = min(m, n)
     assert relfro(dD.diag_array(k), hD.diag(k)) <= tol
@@ -199,7 +203,8 @@ def test_getrf_rp_ties_and_zero_pivot(bf, orc, prec):
 
 
 @pytest.mark.parametrize("prec", ["d", "s"])
-@pytest.mark.parametrize("mn", [(128, 64), (32, 16), (9, 9), (5, 3), (3, 5), (1, 1), (200, 100)])
+@pytest.mark.parametrize("mn", [(128, 64), (32, 16), (9, 9), (5, 3), (3, 5), (1, 1), (200, 100), (300, 150),
+                                (384, 192)])
 def test_geqrf(bf, orc, prec, mn):
     m, n = mn
     rng = np.random.default_rng(m + 7 * n)
@@ -208,7 +213,7 @@ def test_geqrf(bf, orc, prec, mn):
     orc.geqrf(prec, m, n, hC, 0, 0, hD, 0, 0)
     dC, dD = dev(bf, m, n, prec, M), dev(bf, m, n, prec)
     getattr(bf, "blasfeo_%sgeqrf" % prec)(m, n, dC, 0, 0, dD, 0, 0)
-    tol = TOL[prec] * (50 if prec == "s" else 10)
+    tol = tol(prec, 50)
     assert relfro(dD.unpack(), hD.get()) <= tol
     k = min(m, n)
     assert relfro(dD.diag_array(k), hD.diag(k)) <= tol

@@ -61,4 +61,64 @@ def test_noalloc_rejects_oversize_requests():
                                                None) == ENOTSUP
     assert lib.blasfeo_dsposv_l_vbatch_noalloc(10, None, 257, None, None, None, 30, 1e-12, None, None, None,
                                                None) == ENOTSUP
-    assert lib.blasfeo_dsposv_noalloc_scratch_bytes() == 65536 * 4 + 4 * 48
+    # the static array is exactly the scratch the allocating entry point asks for at the limit
+    assert lib.blasfeo_dsposv_noalloc_scratch_bytes() == lib.blasfeo_dposv_worksize(65536)
+
+
+def _noalloc_call(lib, W, num, berr, info):
+    P = lambda t: C.c_void_p(t.data_ptr())
+    return lib.blasfeo_dsposv_l_vbatch_noalloc(num, P(W.nvec), W.max_n, P(W.desc), P(W.bdesc), P(W.xdesc), 30, 1e-12,
+                                               None, P(berr), P(info), None)
+
+
+def test_noalloc_largest_size_and_tensor_engine_allocate_nothing():
+    """Systems up to the documented limit n = 256, on both engines of the
+    solver, from a host thread that has never called the library (so it owns no
+    library workspace): the device's free memory is the same before and after
+    the calls, and the results match the allocating entry point."""
+    import threading
+    import torch
+    import blasfeo_b200 as bf
+    from blasfeo_b200.workloads import spd_config3
+    lib = bf.lib
+    P = lambda t: C.c_void_p(t.data_ptr())
+    num = 120
+    W = spd_config3(num, seed=13, nmin=200, nmax=256)  # seed 13 draws n = 256 twice
+    assert W.max_n == 256
+    info = torch.full((num,), -9, dtype=torch.int32, device="cuda")
+    berr = torch.zeros(num, dtype=torch.float64, device="cuda")
+    assert lib.blasfeo_dsposv_l_vbatch(num, P(W.nvec), W.max_n, P(W.desc), P(W.bdesc), P(W.xdesc), 30, 1e-12, None,
+                                       P(berr), P(info), None, 0, None) == 0
+    torch.cuda.synchronize()
+    x_ref = W.x.clone()
+    # first call on this device (looks up the static array's address; loads the module)
+    assert _noalloc_call(lib, W, num, berr, info) == 0
+    torch.cuda.synchronize()
+    out = {}
+
+    def worker():
+        try:
+            torch.cuda.set_device(0)
+            free0 = torch.cuda.mem_get_info()[0]
+            for engine in (1, 2):  # SIMT, then the tensor-memory engine (the setting is per host thread)
+                assert lib.blasfeo_b200_set_posv_engine(engine) == 0
+                W.x.zero_()
+                info.fill_(-9)
+                st = _noalloc_call(lib, W, num, berr, info)
+                torch.cuda.synchronize()
+                out[engine] = (st, info.cpu().numpy().copy(), berr.cpu().numpy().copy(),
+                               ((W.x - x_ref).norm() / x_ref.norm()).item())
+            out["free"] = (free0, torch.cuda.mem_get_info()[0])
+        except Exception as ex:  # reported by the main thread
+            out["error"] = repr(ex)
+
+    t = threading.Thread(target=worker)
+    t.start()
+    t.join()
+    assert "error" not in out, out.get("error")
+    for engine in (1, 2):
+        st, inf, be, diff = out[engine]
+        assert st == 0 and (inf == 0).all() and (be <= 1e-12).all(), engine
+        assert diff <= 1e-10, (engine, diff)  # both engines are backward stable to 1e-12 (cond <= 1e6)
+    free0, free1 = out["free"]
+    assert free0 == free1, (free0, free1)
