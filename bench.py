@@ -66,7 +66,6 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--num", type=int, default=NUM)
-    ap.add_argument("--cpu-sample", type=int, default=4000)
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--no-fp64", action="store_true", help="skip the FP64 batched dgemm/dpotrf roofline legs")
     ap.add_argument("--case", nargs="+", metavar="ARG",
@@ -171,84 +170,197 @@ def cpu_library():
     return pyoracle.oracle_lib(), "oracle_d_", "port", "oracle restatement (C, scalar loops)"
 
 
-def cpu_sample_systems(num, seed=1):
+def physical_cpus():
+    """One logical CPU per physical core among the CPUs this process may run
+    on (sysfs topology: core_id and physical_package_id), so that P threads of
+    the CPU baseline land on P different cores."""
+    allowed = sorted(os.sched_getaffinity(0))
+    seen, pick = set(), []
+    for c in allowed:
+        base = "/sys/devices/system/cpu/cpu%d/topology/" % c
+        try:
+            core = open(base + "core_id").read().strip()
+            pkg = open(base + "physical_package_id").read().strip()
+        except OSError:
+            return allowed
+        if (pkg, core) not in seen:
+            seen.add((pkg, core))
+            pick.append(c)
+    return pick
+
+
+def gen_config3(num, seed, device):
+    """The benchmark's systems: n ~ U{4..256} (numpy, seeded); per size,
+    A = Q diag(lambda) Q^T with Q from the QR of an N(0,1) matrix and
+    log10(lambda) ~ U[0,6] (torch generator with the same seed, on `device`);
+    b ~ N(0,1).  Returns (ns, {n: (indices, A tensor)}, [b]).  Both arms call
+    this with the same seed, so the GPU arm and the reference arm solve the
+    same systems."""
+    import torch
     rng = np.random.default_rng(seed)
-    ns = rng.integers(4, 257, size=num)
-    mats, rhs = [], []
-    for n in ns:
-        q, _ = np.linalg.qr(rng.standard_normal((n, n)))
-        lam = 10.0 ** rng.uniform(0, 6, n)
-        a = (q * lam) @ q.T
-        mats.append(0.5 * (a + a.T))
-        rhs.append(rng.standard_normal(n))
+    ns = rng.integers(4, 257, size=num).astype(np.int32)
+    g = torch.Generator(device=device)
+    g.manual_seed(seed)
+    mats = {}
+    for n in np.unique(ns):
+        idx = np.nonzero(ns == n)[0]
+        G = torch.randn((len(idx), int(n), int(n)), generator=g, dtype=torch.float64, device=device)
+        Q, _ = torch.linalg.qr(G)
+        lam = 10.0 ** (torch.rand((len(idx), int(n)), generator=g, dtype=torch.float64, device=device) * 6.0)
+        A = (Q * lam[:, None, :]) @ Q.transpose(1, 2)
+        mats[int(n)] = (idx, 0.5 * (A + A.transpose(1, 2)))
+    rhs = [rng.standard_normal(int(n)) for n in ns]
     return ns, mats, rhs
 
 
-class CpuRun:
-    def __init__(self, num, threads=None):
-        from oracle.pyoracle import HostMat, HostVec
-        self.lib, self.prefix, self.kind, self.name = cpu_library()
-        d = os.path.join(ROOT, "oracle")
-        so = os.path.join(d, "libcpu_bench.so")
-        if not os.path.exists(so):
-            subprocess.run(["make", "-s", "-C", d, "cpubench"], check=True)
-        self.drv = C.CDLL(so)
-        self.drv.cpu_posv_batch.restype = C.c_double
-        self.threads = threads or len(os.sched_getaffinity(0))
-        self.ns, mats, self.rhs = cpu_sample_systems(num)
-        self.mats = mats
-        self.hA = [HostMat(int(n), int(n)).set(a) for n, a in zip(self.ns, mats)]
-        self.hb = [HostVec(int(n)).set(b) for n, b in zip(self.ns, self.rhs)]
-        self.hx = [HostVec(int(n)) for n in self.ns]
+def _memsize_dmat(m, n):
+    """blasfeo_memsize_dmat (auxiliary/d_aux_lib4.c:1519): pm*cn + dA rounded to 16, in bytes, 64-byte rounded."""
+    pm, cn = (m + 3) // 4 * 4, (n + 3) // 4 * 4
+    return ((pm * cn + (min(m, n) + 15) // 16 * 16) * 8 + 63) // 64 * 64
+
+
+class HostSystems:
+    """The systems of gen_config3 in host memory, each matrix laid out as
+    blasfeo_create_dmat lays it out (panel-major, panel size 4), with BLASFEO
+    descriptors for the CPU library."""
+
+    def __init__(self, ns, mats, rhs):
+        import torch
         from oracle.pyoracle import DMat, DVec
-        self.A = (DMat * num)(*[h.desc for h in self.hA])
-        self.b = (DVec * num)(*[h.desc for h in self.hb])
-        self.x = (DVec * num)(*[h.desc for h in self.hx])
-        self.n = (C.c_int * num)(*[int(v) for v in self.ns])
-        f = lambda s: C.cast(getattr(self.lib, self.prefix + s), C.c_void_p)
-        self.fp = (f("potrf_l"), f("trsv_lnn"), f("trsv_ltn"))
+        self.ns = np.asarray(ns, dtype=np.int32)
+        num = len(ns)
+        size = {int(n): _memsize_dmat(int(n), int(n)) // 8 for n in np.unique(self.ns)}
+        offs = np.zeros(num, dtype=np.int64)
+        acc = 0
+        for i, n in enumerate(self.ns):
+            offs[i] = acc
+            acc += size[int(n)]
+        self.slab = np.zeros(acc + 8)
+        for n, (idx, X) in mats.items():
+            pm = (n + 3) // 4 * 4
+            pad = torch.zeros((len(idx), pm, pm), dtype=torch.float64, device=X.device)
+            pad[:, :n, :n] = X
+            P = pad.reshape(len(idx), pm // 4, 4, pm).permute(0, 1, 3, 2).reshape(len(idx), pm * pm).cpu().numpy()
+            for r, i in enumerate(idx):
+                self.slab[offs[i]:offs[i] + pm * pm] = P[r]
+        self.mats_by_n = mats
+        vlen = (self.ns + 3) // 4 * 4
+        voff = np.concatenate([[0], np.cumsum(vlen)[:-1]]).astype(np.int64)
+        self.b = np.zeros(int(vlen.sum()) + 4)
+        self.x = np.zeros_like(self.b)
+        for i, r in enumerate(rhs):
+            self.b[voff[i]:voff[i] + len(r)] = r
+        self.rhs, self.voff = rhs, voff
+        base, bb, xb = self.slab.ctypes.data, self.b.ctypes.data, self.x.ctypes.data
+        A, bv, xv = (DMat * num)(), (DVec * num)(), (DVec * num)()
+        for i, n in enumerate(self.ns):
+            n = int(n)
+            pm = (n + 3) // 4 * 4
+            a = A[i]
+            a.mem = a.pA = base + int(offs[i]) * 8
+            a.dA = a.pA + pm * pm * 8
+            a.m = a.n = n
+            a.pm = a.cn = pm
+            a.use_dA = 0
+            a.memsize = size[n] * 8
+            for v, p in ((bv[i], bb), (xv[i], xb)):
+                v.mem = v.pa = p + int(voff[i]) * 8
+                v.m, v.pm, v.memsize = n, pm, pm * 8
+        self.A, self.bv, self.xv = A, bv, xv
+        self.nvec = (C.c_int * num)(*[int(v) for v in self.ns])
         self.num = num
 
-    def run(self):
-        return self.drv.cpu_posv_batch(self.threads, self.num, int(self.ns.max()), self.n, self.A, self.b, self.x,
-                                       *self.fp)
+    def backward_error(self, i):
+        n = int(self.ns[i])
+        idx, X = self.mats_by_n[n]
+        a = X[int(np.nonzero(idx == i)[0][0])].cpu().numpy()
+        x = self.x[self.voff[i]:self.voff[i] + n]
+        b = self.rhs[i]
+        return float(np.abs(b - a @ x).max() / (np.abs(a).sum(1).max() * np.abs(x).max()))
+
+
+class CpuRun:
+    """The reference's CPU path (dpotrf_l + dtrsv_lnn + dtrsv_ltn per system,
+    oracle/cpu_bench.c) over HostSystems with P threads on P physical cores."""
+
+    def __init__(self, systems):
+        self.lib, self.prefix, self.kind, self.name = cpu_library()
+        self.drv = cpu_driver()
+        self.sys = systems
+        f = lambda s: C.cast(getattr(self.lib, self.prefix + s), C.c_void_p)
+        self.fp = (f("potrf_l"), f("trsv_lnn"), f("trsv_ltn"))
+        self.cpus = physical_cpus()
+
+    def run(self, threads):
+        S = self.sys
+        old = os.sched_getaffinity(0)
+        os.sched_setaffinity(0, self.cpus[:max(1, threads)])
+        try:
+            return self.drv.cpu_posv_batch(threads, S.num, int(S.ns.max()), S.nvec, S.A, S.bv, S.xv, *self.fp)
+        finally:
+            os.sched_setaffinity(0, old)
 
     def check(self, k=8):
-        worst = 0.0
-        for i in range(0, self.num, max(1, self.num // k)):
-            x = self.hx[i].get()
-            a, b = self.mats[i], self.rhs[i]
-            worst = max(worst, np.abs(b - a @ x).max() / (np.abs(a).sum(1).max() * np.abs(x).max()))
-        return worst
+        return max(self.sys.backward_error(i) for i in range(0, self.sys.num, max(1, self.sys.num // k)))
 
 
-def cpu_baseline(sample, budget_s=10.0):
-    cr = CpuRun(sample)
-    t = cr.run()
-    reps = max(1, min(20, int(budget_s / max(t, 1e-3))))
-    ts = [cr.run() for _ in range(reps)]
-    t = float(np.median(ts))
-    return {"value": sample / t, "unit": UNIT, "cores": cr.threads, "kind": cr.kind,
-            "sample": "%d systems of the same distribution (seeded), %s, dpotrf_l+dtrsv_lnn+dtrsv_ltn per system, "
-                      "median of %d passes, worst sampled residual %.1e" % (sample, cr.name, reps, cr.check())}
+def cpu_driver():
+    d = os.path.join(ROOT, "oracle")
+    so = os.path.join(d, "libcpu_bench.so")
+    if not os.path.exists(so):
+        subprocess.run(["make", "-s", "-C", d, "cpubench"], check=True)
+    drv = C.CDLL(so)
+    for f in ("cpu_posv_batch", "cpu_chain_batch", "cpu_ric_trf_batch"):
+        getattr(drv, f).restype = C.c_double
+    drv.cpu_chain_batch.argtypes = [C.c_int, C.c_int, C.c_int, C.c_double] + [C.c_void_p, C.c_longlong] * 7 + \
+        [C.c_void_p] * 5
+    drv.cpu_ric_trf_batch.argtypes = [C.c_int] * 5 + [C.c_void_p, C.c_longlong] * 3 + [C.c_void_p] * 3
+    return drv
+
+
+def cpu_baseline(systems, passes=5, p1_passes=3):
+    """Median wall time of `passes` passes over all systems with one thread per
+    physical core, and of `p1_passes` passes on one core."""
+    cr = CpuRun(systems)
+    P = len(cr.cpus)
+    cr.run(P)
+    tp = float(np.median([cr.run(P) for _ in range(passes)]))
+    t1 = float(np.median([cr.run(1) for _ in range(p1_passes)]))
+    n = systems.num
+    return {"value": n / tp, "unit": UNIT, "cores": P, "kind": cr.kind,
+            "sample": "the same %d systems as the GPU arm (seed 1000), %s, dpotrf_l+dtrsv_lnn+dtrsv_ltn per system, "
+                      "one thread per physical core (%d of %d logical CPUs), median of %d passes; worst sampled "
+                      "backward error %.1e" % (n, cr.name, P, len(os.sched_getaffinity(0)), passes, cr.check()),
+            "p1": {"value": n / t1, "cores": 1, "sample": "same systems, one core, median of %d passes" % p1_passes},
+            "ms_per_pass": 1e3 * tp}
 
 
 def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
-    cr = CpuRun(args.cpu_sample)
+    import torch
+    dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", "0"))) if torch.cuda.is_available() else "cpu"
+    # the GPU arm's systems (seed 1000 for rank 0); the device only generates them
+    systems = HostSystems(*gen_config3(args.num, 1000, dev))
+    cr = CpuRun(systems)
+    P = len(cr.cpus)
     for _ in range(args.warmup):
-        cr.run()
-    ts = [cr.run() for _ in range(args.steps)]
+        cr.run(P)
+    ts = [cr.run(P) for _ in range(args.steps)]
     total = float(np.sum(ts))
-    val = args.cpu_sample * args.steps / total
+    val = args.num * args.steps / total
+    t1 = float(np.median([cr.run(1) for _ in range(2)]))
     line = {"metric": METRIC, "value": val, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": 1e3 * total / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic", "impl": "reference",
-            "config": {"workload": WORKLOAD, "sample_systems": args.cpu_sample, "library": cr.name},
-            "cpu_baseline": {"value": val, "unit": UNIT, "cores": cr.threads, "kind": cr.kind,
-                             "sample": "%d systems per step, %s" % (args.cpu_sample, cr.name)},
+            "config": {"workload": WORKLOAD, "systems": args.num, "seed": 1000, "library": cr.name,
+                       "same_systems_as_gpu_arm": True},
+            "cpu_baseline": {"value": val, "unit": UNIT, "cores": P, "kind": cr.kind,
+                             "sample": "all %d systems per step (the GPU arm's, seed 1000), %s, one thread per "
+                                       "physical core; median pass %.1f ms; worst sampled backward error %.1e"
+                                       % (args.num, cr.name, 1e3 * float(np.median(ts)), cr.check()),
+                             "p1": {"value": args.num / t1, "cores": 1}},
             "e2e": {"value": val, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
     return 0
@@ -314,11 +426,15 @@ def main():
         import datetime
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300), device_id=torch.device("cuda", local))
     import blasfeo_b200 as bf
-    from blasfeo_b200.workloads import spd_config3
+    from blasfeo_b200.workloads import SpdBatch
     lib = bf.lib
     P = lambda t: C.c_void_p(t.data_ptr())
     dev = torch.device("cuda", local)
-    W = spd_config3(args.num, seed=1000 + rank, device=dev)
+    systems = gen_config3(args.num, 1000 + rank, dev)
+    W = SpdBatch(*systems, device=dev)
+    # the CPU baseline solves the very same systems from host memory
+    host_sys = HostSystems(*systems) if (rank == 0 and world == 1 and not args.no_cpu) else None
+    del systems
     info = torch.zeros(args.num, dtype=torch.int32, device=dev)
     iters = torch.zeros(args.num, dtype=torch.int32, device=dev)
     berr = torch.zeros(args.num, dtype=torch.float64, device=dev)
@@ -430,7 +546,7 @@ def main():
     others = None
     if not args.no_fp64:
         try:
-            others = other_configs(lib, torch, dev, stream, peak_bw)
+            others = other_configs(lib, torch, dev, stream, peak_bw, cpu=(rank == 0 and not args.no_cpu))
         except Exception as ex:  # reported, never silently replaced
             others = {"error": repr(ex)}
     single = None
@@ -453,7 +569,7 @@ def main():
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         try:
-            cpu = cpu_baseline(args.cpu_sample)
+            cpu = cpu_baseline(host_sys)
         except Exception as ex:
             cpu = {"value": None, "error": repr(ex)}
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -647,7 +763,7 @@ def cpu_single_dropin(reps=2000):
     return out
 
 
-def other_configs(lib, torch, dev, stream, peak_bw):
+def other_configs(lib, torch, dev, stream, peak_bw, cpu=True):
     """The two fused HBM-bound kernels on their own workloads (seeded, inputs
     larger than L2), per instance: algorithmic bytes (inputs read once, outputs
     written once) and flops as in the design record.
@@ -692,10 +808,36 @@ def other_configs(lib, torch, dev, stream, peak_bw):
     out["chain_n16"] = {"instances": nb, "ms": ms, "instances_per_s": nb / ms * 1e3, "gbs": by / ms / 1e6,
                         "frac_of_hbm": by / ms / 1e6 / peak_bw, "gflops": fl / ms / 1e6,
                         "bytes_per_instance": 15424, "flops_per_instance": 22.8e3}
+    if cpu:
+        try:
+            out["chain_n16"]["cpu_reference"] = cpu_chain_leg(nb, slabs, L, X, D)
+        except Exception as ex:  # reported, never silently replaced
+            out["chain_n16"]["cpu_reference"] = {"error": repr(ex)}
     del slabs, L, X, D
     torch.cuda.empty_cache()
 
     nbt, N, nx, nu = 4096, 30, 12, 4
+    out.update(riccati_legs(lib, torch, dev, stream, peak_bw, g, tm, nbt, N, nx, nu, cpu))
+    torch.cuda.empty_cache()
+    return out
+
+
+def riccati_legs(lib, torch, dev, stream, peak_bw, g, tm, nbt, N, nx, nu, cpu):
+    """Config 4: 4,096 LQR problems, N = 30, nx = 12, nu = 4; A = I + 0.1 N(0,1)
+    scaled to spectral radius 0.95, B ~ N(0,1)/sqrt(nx), Q = R = I, S = 0,
+    P_N = I; for the solves, linear terms rq_k ~ N(0,1), b_k ~ N(0,1).
+      riccati_d_N30 / riccati_s_N30: the backward factorization in one launch
+        (FP64 / FP32);
+      lq_solve_d_N30: FP64 factorization + Riccati solve (ux_k, pi_k);
+      lq_solve_mixed_N30: FP32 factorization + FP64 refinement on the KKT residual;
+    errors of P_0, K_k (all stages) and of the refined solution against the
+    FP64 reference (the compiled reference's factors when the CPU leg runs,
+    else this library's FP64 factors)."""
+    from blasfeo_b200.api import DMatBatch, SMatBatch
+    from blasfeo_b200.workloads import fill_batch
+    P = lambda t: C.c_void_p(t.data_ptr())
+    sh = C.c_void_p(stream.cuda_stream)
+    out = {}
     A = torch.eye(nx, dtype=torch.float64, device=dev) + 0.1 * torch.randn((nbt, nx, nx), generator=g,
                                                                           dtype=torch.float64, device=dev)
     rho = torch.linalg.eigvals(A.cpu()).abs().max(dim=1).values.to(dev)
@@ -706,13 +848,21 @@ def other_configs(lib, torch, dev, stream, peak_bw):
     BA[:, nu:nu + nx] = A.transpose(1, 2)
     BAs = BA[:, None].expand(nbt, N, 16, nx).reshape(nbt * N, 16, nx)
     RSQ = torch.eye(16, dtype=torch.float64, device=dev).expand(nbt * (N + 1), 16, 16)
+    m = nx + nu
+    b = torch.zeros((nbt, N, 16), dtype=torch.float64, device=dev)
+    b[:, :, :nx] = torch.randn((nbt, N, nx), generator=g, dtype=torch.float64, device=dev)
+    rq = torch.zeros((nbt, N + 1, 16), dtype=torch.float64, device=dev)
+    rq[:, :N, :m] = torch.randn((nbt, N, m), generator=g, dtype=torch.float64, device=dev)
+    rq[:, N, :nx] = torch.randn((nbt, nx), generator=g, dtype=torch.float64, device=dev)
+    Ls = {}
+    slabs = {}
     for prec, Bt, dt in (("d", DMatBatch, torch.float64), ("s", SMatBatch, torch.float32)):
         sBA, sRSQ, sL = Bt(16, nx, nbt * N), Bt(16, 16, nbt * (N + 1)), Bt(16, 16, nbt * (N + 1))
         fill_batch(sBA, BAs.to(dt).contiguous())
         fill_batch(sRSQ, RSQ.to(dt).contiguous())
         info = torch.zeros(nbt, dtype=torch.int32, device=dev)
         f = lib.blasfeo_dric_trf_batch if prec == "d" else lib.blasfeo_sric_trf_batch
-        ms = tm(lambda: f(nbt, N, nx, nu, sBA.ref, sRSQ.ref, sL.ref, C.c_void_p(info.data_ptr()), sh))
+        ms = tm(lambda: f(nbt, N, nx, nu, sBA.ref, sRSQ.ref, sL.ref, P(info), sh))
         if not bool((info == 0).all().item()):
             raise RuntimeError("Riccati factorization reported a non-positive pivot")
         esz = 8 if prec == "d" else 4
@@ -720,9 +870,158 @@ def other_configs(lib, torch, dev, stream, peak_bw):
         out["riccati_%s_N30" % prec] = {"problems": nbt, "ms": ms, "problems_per_s": nbt / ms * 1e3,
                                         "gbs": by / ms / 1e6, "frac_of_hbm": by / ms / 1e6 / peak_bw,
                                         "gflops": 7.1e3 * N * nbt / ms / 1e6}
-        del sBA, sRSQ, sL
-    torch.cuda.empty_cache()
+        Ls[prec] = sL.unpack_all().reshape(nbt, N + 1, 16, 16)
+        slabs[prec] = (sBA, sRSQ, sL)
+    sBA, sRSQ, sL = slabs["d"]
+    if cpu:
+        try:
+            out["riccati_d_N30"]["cpu_reference"], Ls["ref"] = cpu_riccati_leg(nbt, N, nx, nu, sBA, sRSQ, sL)
+        except Exception as ex:  # reported, never silently replaced
+            out["riccati_d_N30"]["cpu_reference"] = {"error": repr(ex)}
+    # FP64 factorization + solve
+    bflat, rqflat = b.reshape(-1).contiguous(), rq.reshape(-1).contiguous()
+    ux = torch.zeros(nbt * (N + 1) * 16, dtype=torch.float64, device=dev)
+    pi = torch.zeros(nbt * N * 16, dtype=torch.float64, device=dev)
+    info = torch.zeros(nbt, dtype=torch.int32, device=dev)
+
+    def solve64():
+        lib.blasfeo_dric_trf_batch(nbt, N, nx, nu, sBA.ref, sRSQ.ref, sL.ref, P(info), sh)
+        return lib.blasfeo_dric_trs_batch(nbt, N, nx, nu, sBA.ref, sL.ref, P(bflat), 16, P(rqflat), 16, P(ux), 16,
+                                          P(pi), 16, sh)
+    ms64 = tm(solve64)
+    ux64, pi64 = ux.clone(), pi.clone()
+    ms_trs = tm(lambda: lib.blasfeo_dric_trs_batch(nbt, N, nx, nu, sBA.ref, sL.ref, P(bflat), 16, P(rqflat), 16,
+                                                   P(ux), 16, P(pi), 16, sh))
+    out["lq_solve_d_N30"] = {"problems": nbt, "ms": ms64, "problems_per_s": nbt / ms64 * 1e3, "trs_ms": ms_trs}
+    # mixed: FP32 factorization + FP64 refinement
+    iters = torch.zeros(nbt, dtype=torch.int32, device=dev)
+    res = torch.zeros(nbt, dtype=torch.float64, device=dev)
+    TOLR = 1e-13
+    msm = tm(lambda: lib.blasfeo_dsric_sv_batch(nbt, N, nx, nu, sBA.ref, sRSQ.ref, P(bflat), 16, P(rqflat), 16, P(ux),
+                                                16, P(pi), 16, 20, TOLR, P(iters), P(res), P(info), None, 0, sh))
+    torch.cuda.synchronize()
+    rel = lambda a_, b_: float((a_ - b_).norm().item() / b_.norm().item())
+    out["lq_solve_mixed_N30"] = {
+        "problems": nbt, "ms": msm, "problems_per_s": nbt / msm * 1e3, "vs_fp64_solve": ms64 / msm,
+        "converged": bool((info == 0).all().item()), "tol_rel_kkt_residual": TOLR,
+        "mean_refinement_steps": float(iters.double().mean().item()), "max_rel_kkt_residual": float(res.max().item()),
+        "solution_relfro_vs_fp64": {"ux": rel(ux, ux64), "pi": rel(pi, pi64)}}
+    ref = Ls.get("ref", Ls["d"])
+    for prec in ("d", "s"):
+        out["riccati_%s_N30" % prec]["error_vs_fp64_reference"] = riccati_errors(Ls[prec], ref, nx, nu, N)
+    out["riccati_d_N30"]["error_reference"] = "compiled reference (CPU)" if "ref" in Ls else "this library's FP64"
     return out
+
+
+def riccati_gains(L, nx, nu):
+    """From a stage factor L = [[Luu, 0], [Lxu, Lxx]] (problems x 16 x 16):
+    P = Lxx Lxx^T and K = -Luu^{-T} Lxu^T (the feedback u = K x)."""
+    Luu, Lxu, Lxx = L[:, :nu, :nu], L[:, nu:nu + nx, :nu], L[:, nu:nu + nx, nu:nu + nx]
+    P = np.tril(Lxx) @ np.transpose(np.tril(Lxx), (0, 2, 1))
+    K = -np.linalg.solve(np.transpose(np.tril(Luu), (0, 2, 1)), np.transpose(Lxu, (0, 2, 1)))
+    return P, K
+
+
+def riccati_errors(L, ref, nx, nu, N):
+    """Max over problems of the relative Frobenius error of P_0, and of K_k
+    over all problems and stages k < N."""
+    e = lambda a, b: float((np.linalg.norm(a - b, axis=(1, 2)) / np.linalg.norm(b, axis=(1, 2))).max())
+    P, _ = riccati_gains(np.asarray(L[:, 0], dtype=np.float64), nx, nu)
+    Pr, _ = riccati_gains(ref[:, 0], nx, nu)
+    kerr = 0.0
+    for k in range(N):
+        _, K = riccati_gains(np.asarray(L[:, k], dtype=np.float64), nx, nu)
+        _, Kr = riccati_gains(ref[:, k], nx, nu)
+        kerr = max(kerr, e(K, Kr))
+    return {"P0_relfro_max": e(P, Pr), "K_relfro_max_all_stages": kerr}
+
+
+def _host_slab(B):
+    """Host copy of a device uniform-batch slab (same layout): (array, pointer to instance 0, stride)."""
+    h = np.ascontiguousarray(B.buf.cpu().numpy()).view(np.float64)
+    off = (B.s.pA - B.buf.data_ptr()) // 8
+    return h, h.ctypes.data + 8 * off, B.s.stride
+
+
+def _cpu_times(fn, passes=5, p1_passes=3):
+    cpus = physical_cpus()
+    old = os.sched_getaffinity(0)
+    try:
+        os.sched_setaffinity(0, cpus)
+        fn(len(cpus))
+        tp = float(np.median([fn(len(cpus)) for _ in range(passes)]))
+        os.sched_setaffinity(0, cpus[:1])
+        t1 = float(np.median([fn(1) for _ in range(p1_passes)]))
+    finally:
+        os.sched_setaffinity(0, old)
+    return len(cpus), tp, t1
+
+
+def cpu_chain_leg(nb, slabs, L, X, D):
+    """The n = 16 chain through the compiled reference (dsyrk_ln + ddiare +
+    dpotrf_l + dtrsm_rltn + dgemm_nt per instance) on host copies of the GPU
+    leg's input slabs; instances/s at P = all physical cores and P = 1, and the
+    GPU results' relative error against the reference's."""
+    lib, prefix, kind, name = cpu_library()
+    drv = cpu_driver()
+    f = lambda s_: C.cast(getattr(lib, prefix + s_), C.c_void_p)
+    hin = {k: _host_slab(v) for k, v in slabs.items()}
+    hout = {k: _host_slab(v) for k, v in (("L", L), ("X", X), ("D", D))}
+    for h, _, _ in hout.values():
+        h[:] = 0.0
+    args = [hin[k][1:] for k in "ARCG"] + [hout[k][1:] for k in "LXD"]
+    flat = [a for pr in args for a in pr]
+
+    def run(P):
+        return drv.cpu_chain_batch(P, nb, 32, 16.0, *flat, f("syrk_ln"), f("diare"), f("potrf_l"), f("trsm_rltn"),
+                                   f("gemm_nt"))
+    P, tp, t1 = _cpu_times(run)
+    errs = {}
+    for k, B in (("L", L), ("X", X), ("D", D)):
+        g = B.unpack_all()
+        h = hout[k][0]
+        pm, cn, st = B.s.pm, B.s.cn, B.s.stride
+        off = (B.s.pA - B.buf.data_ptr()) // 8
+        r = h[off: off + nb * st].reshape(nb, st)[:, :pm * cn].reshape(nb, pm // 4, cn, 4).transpose(0, 1, 3, 2)
+        r = r.reshape(nb, pm, cn)[:, :16, :16]
+        if k == "L":
+            g, r = np.tril(g), np.tril(r)
+        errs[k] = float(np.linalg.norm(g - r) / np.linalg.norm(r))
+    return {"kind": kind, "library": name, "instances_per_s": nb / tp, "cores": P,
+            "p1_instances_per_s": nb / t1, "median_pass_ms": 1e3 * tp,
+            "sample": "the GPU leg's %d instances (host copies of its slabs)" % nb,
+            "gpu_vs_reference_relfro": errs}
+
+
+def cpu_riccati_leg(nbt, N, nx, nu, sBA, sRSQ, sL):
+    """The Riccati factorization through the compiled reference
+    (examples/example_d_riccati_recursion.c:115-143: dpotrf_l, then per stage
+    dtrmm_rlnn + dsyrk_dpotrf_ln) on host copies of the GPU leg's FP64 slabs;
+    problems/s at P = all physical cores and P = 1; returns (report, the
+    reference's L as problems x (N+1) x 16 x 16)."""
+    lib, prefix, kind, name = cpu_library()
+    drv = cpu_driver()
+    f = lambda s_: C.cast(getattr(lib, prefix + s_), C.c_void_p)
+    hBA, hRSQ, hL = _host_slab(sBA), _host_slab(sRSQ), _host_slab(sL)
+    hL[0][:] = 0.0
+
+    def run(P):
+        return drv.cpu_ric_trf_batch(P, nbt, N, nx, nu, *hBA[1:], *hRSQ[1:], *hL[1:], f("potrf_l"), f("trmm_rlnn"),
+                                     f("syrk_potrf_ln") if prefix == "oracle_d_" else f("syrk_dpotrf_ln"))
+    P, tp, t1 = _cpu_times(run)
+    pm, cn, st = sL.s.pm, sL.s.cn, sL.s.stride
+    off = (sL.s.pA - sL.buf.data_ptr()) // 8
+    tot = nbt * (N + 1)
+    r = hL[0][off: off + tot * st].reshape(tot, st)[:, :pm * cn].reshape(tot, pm // 4, cn, 4).transpose(0, 1, 3, 2)
+    Lref = r.reshape(tot, pm, cn)[:, :16, :16].reshape(nbt, N + 1, 16, 16)
+    g = sL.unpack_all().reshape(nbt, N + 1, 16, 16)
+    m = nu + nx
+    err = float(np.linalg.norm(np.tril(g[:, :N, :m, :m]) - np.tril(Lref[:, :N, :m, :m])) /
+                np.linalg.norm(np.tril(Lref[:, :N, :m, :m])))
+    rep = {"kind": kind, "library": name, "problems_per_s": nbt / tp, "cores": P, "p1_problems_per_s": nbt / t1,
+           "median_pass_ms": 1e3 * tp, "sample": "the GPU leg's %d problems (host copies of its FP64 slabs)" % nbt,
+           "gpu_fp64_vs_reference_relfro": err}
+    return rep, Lref
 
 
 def learned_dispatch(nlaunch=64, ntrain=44, seed=5):

@@ -186,6 +186,12 @@ _sig("blasfeo_dsposv_l_vbatch_mapped", _i, _i, _vp, _i, _vp, _vp, _vp, _i, _d, _
 _sig("blasfeo_dsyrk_dpotrf_dtrsm_dgemm_batch", _i, _i, _i, _i, _d, _DB, _DB, _DB, _DB, _DB, _DB, _DB, _vp, _vp)
 _sig("blasfeo_dric_trf_batch", _i, _i, _i, _i, _i, _DB, _DB, _DB, _vp, _vp)
 _sig("blasfeo_sric_trf_batch", _i, _i, _i, _i, _i, _SB, _SB, _SB, _vp, _vp)
+_LL = C.c_longlong
+_sig("blasfeo_dric_trs_batch", _i, _i, _i, _i, _i, _DB, _DB, _vp, _LL, _vp, _LL, _vp, _LL, _vp, _LL, _vp)
+_sig("blasfeo_dric_gains_batch", _i, _i, _i, _i, _i, _DB, _DB, _vp)
+_sig("blasfeo_dsric_sv_worksize", _sz, _i, _i, _i)
+_sig("blasfeo_dsric_sv_batch", _i, _i, _i, _i, _i, _DB, _DB, _vp, _LL, _vp, _LL, _vp, _LL, _vp, _LL, _i, _d, _vp, _vp,
+     _vp, _vp, _sz, _vp)
 _sig("blasfeo_b200_mlp_param_count", _i, _i, _i)
 _sig("blasfeo_b200_mlp_work_bytes", _sz, _i, _i)
 _sig("blasfeo_b200_mlp_forward", _i, _i, _i, _vp, _i, _vp, _vp, _vp, _vp)

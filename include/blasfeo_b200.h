@@ -453,6 +453,45 @@ int blasfeo_dric_trf_batch(int batch, int N, int nx, int nu, struct blasfeo_dmat
 int blasfeo_sric_trf_batch(int batch, int N, int nx, int nu, struct blasfeo_smat_batch *sBAbt,
 	struct blasfeo_smat_batch *sRSQ, struct blasfeo_smat_batch *sL, int *info, void *stream);
 
+/* Batched Riccati solve (no reference counterpart for the batch; per problem
+ * the sequence d_back_ric_trs_libstr of examples/example_d_riccati_recursion.c:203-270:
+ * blasfeo_dtrmv_ltn / dtrmv_lnn / dgemv_n / dtrsv_lnn_mn backward, dtrsv_ltn_mn /
+ * dgemv_t / dtrmv_ltn / dtrmv_lnn forward) on the factors of
+ * blasfeo_dric_trf_batch: the LQ problem
+ *   min sum_k 1/2 [u;x]_k^T RSQ_k [u;x]_k + rq_k^T [u;x]_k + 1/2 x_N^T Q_N x_N + q_N^T x_N,
+ *   x_{k+1} = BAbt_k^T [u;x]_k + b_k  (x_0 free).
+ * Vectors are strided arrays of doubles: b_k of problem p at b + sb*(p*N + k)
+ * (nx entries), rq_k at rq + srq*(p*(N+1) + k) (nu + nx entries; stage N: nx),
+ * ux_k = [u_k; x_k] at ux + sux*(p*(N+1) + k) (stage N: x_N), pi_k (the
+ * dynamics multipliers) at pi + spi*(p*N + k).  sBAbt, sL as for
+ * blasfeo_dric_trf_batch.  N >= 1, nu + nx <= 16. */
+int blasfeo_dric_trs_batch(int batch, int N, int nx, int nu, struct blasfeo_dmat_batch *sBAbt,
+	struct blasfeo_dmat_batch *sL, const double *b, long long sb, const double *rq, long long srq, double *ux,
+	long long sux, double *pi, long long spi, void *stream);
+/* Feedback gains K_k = -(R + B^T P B)^{-1} (S + B^T P A) = -Luu^{-T} Lxu^T of
+ * every stage k < N from the factors L_k = [[Luu, 0], [Lxu, Lxx]] of
+ * blasfeo_dric_trf_batch (u_k = K_k x_k for the homogeneous problem): sK
+ * holds batch*N instances of nu x nx (problem p, stage k at p*N + k). */
+int blasfeo_dric_gains_batch(int batch, int N, int nx, int nu, struct blasfeo_dmat_batch *sL,
+	struct blasfeo_dmat_batch *sK, void *stream);
+/* Mixed-precision LQ solve: the Riccati factorization in FP32
+ * (blasfeo_sric_trf_batch on FP32 copies of BAbt_k and RSQ_k), then iterative
+ * refinement in FP64 on the KKT residual
+ *   RSQ_k ux_k + rq_k + BAbt_k pi_k - [0; pi_{k-1}],  Q_N x_N + q_N - pi_{N-1},
+ *   BAbt_k^T ux_k + b_k - x_{k+1}
+ * with corrections from the FP32 factors (the solve of blasfeo_dric_trs_batch),
+ * until ||residual||_inf <= tol * ||(rq, b)||_inf or max_iter corrections.
+ * Arguments as blasfeo_dric_trs_batch plus sRSQ (FP64, as for the
+ * factorization); iters[p], res[p] (relative residual) and info[p] (device,
+ * may be NULL): info = the factorization's pivot report, else 0, or -1 when
+ * refinement did not reach tol.  work: blasfeo_dsric_sv_worksize(batch, N, nx)
+ * bytes of device memory, or NULL for the library workspace. */
+size_t blasfeo_dsric_sv_worksize(int batch, int N, int nx);
+int blasfeo_dsric_sv_batch(int batch, int N, int nx, int nu, struct blasfeo_dmat_batch *sBAbt,
+	struct blasfeo_dmat_batch *sRSQ, const double *b, long long sb, const double *rq, long long srq, double *ux,
+	long long sux, double *pi, long long spi, int max_iter, double tol, int *iters, double *res, int *info,
+	void *work, size_t work_bytes, void *stream);
+
 /* Same as blasfeo_dsposv_l_vbatch, for callers whose matrices, vectors, sizes
  * and descriptors live in mapped (cudaHostAlloc / cudaHostRegister) host
  * memory: the kernels read the lower triangles straight over the host link

@@ -479,4 +479,71 @@ void OX(gemv_n)(int m, int n, REAL alpha, struct XMAT *sA, int ai, int aj, struc
 	}
 }
 
+/* z = beta*y + alpha*A^T*x, A m x n (blasfeo_dgemv_t,
+ * blasfeo_hp_pm/d_blas2_lib4.c:113): z_j = beta*y_j + alpha*sum_i A_ij x_i. */
+void OX(gemv_t)(int m, int n, REAL alpha, struct XMAT *sA, int ai, int aj, struct XVEC *sx, int xi,
+                REAL beta, struct XVEC *sy, int yi, struct XVEC *sz, int zi)
+{
+	REAL t[512];
+	for (int j = 0; j < n; j++) {
+		REAL c = 0;
+		for (int i = 0; i < m; i++) c += EL(sA, ai + i, aj + j) * sx->pa[xi + i];
+		t[j] = alpha * c + beta * sy->pa[yi + j];
+	}
+	for (int j = 0; j < n; j++) sz->pa[zi + j] = t[j];
+}
+
+/* z = A*x and z = A^T*x, A m x m lower non-unit (blasfeo_dtrmv_lnn,
+ * blasfeo_dtrmv_ltn; blasfeo_hp_pm/d_blas2_lib4.c:772, :1014); z may alias x. */
+void OX(trmv_lnn)(int m, struct XMAT *sA, int ai, int aj, struct XVEC *sx, int xi, struct XVEC *sz, int zi)
+{
+	REAL t[512];
+	for (int i = 0; i < m; i++) {
+		REAL c = 0;
+		for (int j = 0; j <= i; j++) c += EL(sA, ai + i, aj + j) * sx->pa[xi + j];
+		t[i] = c;
+	}
+	for (int i = 0; i < m; i++) sz->pa[zi + i] = t[i];
+}
+
+void OX(trmv_ltn)(int m, struct XMAT *sA, int ai, int aj, struct XVEC *sx, int xi, struct XVEC *sz, int zi)
+{
+	REAL t[512];
+	for (int j = 0; j < m; j++) {
+		REAL c = 0;
+		for (int i = j; i < m; i++) c += EL(sA, ai + i, aj + j) * sx->pa[xi + i];
+		t[j] = c;
+	}
+	for (int j = 0; j < m; j++) sz->pa[zi + j] = t[j];
+}
+
+/* A m x n lower trapezoid (blasfeo_dtrsv_lnn_mn, blasfeo_hp_pm/d_blas2_lib4.c:1275):
+ * z[0:n] = A[0:n,0:n]^{-1} x[0:n] (multiplying by the reciprocal pivots),
+ * z[n:m] = x[n:m] - A[n:m,0:n] z[0:n]; z may alias x. */
+void OX(trsv_lnn_mn)(int m, int n, struct XMAT *sA, int ai, int aj, struct XVEC *sx, int xi, struct XVEC *sz, int zi)
+{
+	REAL *x = sx->pa + xi, *z = sz->pa + zi;
+	if (m < n) m = n;
+	for (int i = 0; i < m; i++) {
+		REAL c = x[i];
+		const int lim = i < n ? i : n;
+		for (int l = 0; l < lim; l++) c -= EL(sA, ai + i, aj + l) * z[l];
+		z[i] = i < n ? c * ((REAL)1.0 / EL(sA, ai + i, aj + i)) : c;
+	}
+}
+
+/* A m x n lower trapezoid, transposed (blasfeo_dtrsv_ltn_mn, :1478):
+ * z[n:m] = x[n:m]; for i = n-1 .. 0: z[i] = (x[i] - sum_{l>i} A_li z_l) / A_ii. */
+void OX(trsv_ltn_mn)(int m, int n, struct XMAT *sA, int ai, int aj, struct XVEC *sx, int xi, struct XVEC *sz, int zi)
+{
+	REAL *x = sx->pa + xi, *z = sz->pa + zi;
+	if (n > m) n = m;
+	for (int i = n; i < m; i++) z[i] = x[i];
+	for (int i = n - 1; i >= 0; i--) {
+		REAL c = x[i];
+		for (int l = i + 1; l < m; l++) c -= EL(sA, ai + l, aj + i) * z[l];
+		z[i] = c * ((REAL)1.0 / EL(sA, ai + i, aj + i));
+	}
+}
+
 #undef EL

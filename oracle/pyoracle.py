@@ -206,7 +206,8 @@ class Api:
                      "trmm_rlnn": "trmm_rlnn", "trsv_lnn": "trsv_lnn", "trsv_ltn": "trsv_ltn",
                      "gemv_n": "gemv_n", "gecp": "gecp", "diare": "diare", "rowsw": "rowsw",
                      "syrk_ln_mn": "syrk_ln_mn", "trsm_rltu": "trsm_rltu", "potrf_l_mn": "potrf_l_mn",
-                     "getrf_np": "getrf_np"}[name]
+                     "getrf_np": "getrf_np", "gemv_t": "gemv_t", "trmv_lnn": "trmv_lnn", "trmv_ltn": "trmv_ltn",
+                     "trsv_lnn_mn": "trsv_lnn_mn", "trsv_ltn_mn": "trsv_ltn_mn"}[name]
             pre = "blasfeo_" if self.kind == "hp" else "blasfeo_ref_"
             sym = pre + prec + bname
         f = getattr(self.lib, sym)
@@ -274,6 +275,22 @@ class Api:
 
     def trsv_ltn(self, prec, m, A, ai, aj, x, xi, z, zi):
         self.fn(prec, "trsv_ltn")(m, A.ref, ai, aj, x.ref, xi, z.ref, zi)
+
+    def gemv_t(self, prec, m, n, alpha, A, ai, aj, x, xi, beta, y, yi, z, zi):
+        R = self._R(prec)
+        self.fn(prec, "gemv_t")(m, n, R(alpha), A.ref, ai, aj, x.ref, xi, R(beta), y.ref, yi, z.ref, zi)
+
+    def trmv_lnn(self, prec, m, A, ai, aj, x, xi, z, zi):
+        self.fn(prec, "trmv_lnn")(m, A.ref, ai, aj, x.ref, xi, z.ref, zi)
+
+    def trmv_ltn(self, prec, m, A, ai, aj, x, xi, z, zi):
+        self.fn(prec, "trmv_ltn")(m, A.ref, ai, aj, x.ref, xi, z.ref, zi)
+
+    def trsv_lnn_mn(self, prec, m, n, A, ai, aj, x, xi, z, zi):
+        self.fn(prec, "trsv_lnn_mn")(m, n, A.ref, ai, aj, x.ref, xi, z.ref, zi)
+
+    def trsv_ltn_mn(self, prec, m, n, A, ai, aj, x, xi, z, zi):
+        self.fn(prec, "trsv_ltn_mn")(m, n, A.ref, ai, aj, x.ref, xi, z.ref, zi)
 
     def gemv_n(self, prec, m, n, alpha, A, ai, aj, x, xi, beta, y, yi, z, zi):
         R = self._R(prec)

@@ -190,6 +190,35 @@ def cfg4(api, num=2):
     return out
 
 
+def cfg4_trs(api, num=2):
+    """The LQ solve of examples/example_d_riccati_recursion.c:203-270
+    (d_back_ric_trs_libstr) on the factors of :115-143, through the compiled
+    reference's level-2 routines (dtrmv_ltn/lnn, dgemv_n/t, dtrsv_lnn/ltn and
+    their _mn forms): config-4 dynamics (as cfg4), Q = R = I, S = 0, P_N = I,
+    linear terms rq_k ~ N(0,1) and b_k ~ N(0,1), N = 30, nx = 12, nu = 4."""
+    from tests.ric_oracle import ric_trf, ric_trs
+    rng = np.random.default_rng(44)
+    N, nx, nu = 30, 12, 4
+    m = nx + nu
+    out = {}
+    for p in range(num):
+        A, B = riccati_problem(rng)
+        BA = np.zeros((N, 16, nx))
+        BA[:, :m] = np.vstack([B.T, A.T])
+        RSQ = np.broadcast_to(np.eye(16), (N + 1, 16, 16)).copy()
+        b = np.zeros((N, 16))
+        b[:, :nx] = rng.standard_normal((N, nx))
+        rq = np.zeros((N + 1, 16))
+        rq[:N, :m] = rng.standard_normal((N, m))
+        rq[N, :nx] = rng.standard_normal(nx)
+        L = ric_trf(api, BA, RSQ, N, nx, nu)
+        ux, pi = ric_trs(api, L, BA, b, rq, N, nx, nu)
+        out["BA%d" % p], out["b%d" % p], out["rq%d" % p] = BA, b, rq
+        out["ux%d" % p] = np.stack([np.pad(u, (0, 16 - len(u))) for u in ux])
+        out["pi%d" % p] = np.stack(pi)
+    return out
+
+
 def cfg5(api):
     """A few ops of the mixed stream (log-uniform sizes 4..384): getrf_rp on
     N(0,1) square matrices (pivots), geqrf on tall m = 2n."""
@@ -245,7 +274,7 @@ def adjacent(api):
 def main(only=None):
     api = ref_api("generic")
     gens = {"cfg1.npz": cfg1, "cfg2.npz": cfg2, "cfg3.npz": cfg3, "cfg4.npz": cfg4, "cfg5.npz": cfg5,
-            "adjacent.npz": adjacent}
+            "adjacent.npz": adjacent, "cfg4_trs.npz": cfg4_trs}
     files = {}
     if only is None:
         for prec in ("d", "s"):

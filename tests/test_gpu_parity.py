@@ -182,10 +182,10 @@ def test_getrf_rp(bf, orc, prec, mn):
     dC, dD = dev(bf, m, n, prec, M), dev(bf, m, n, prec)
     piv = getattr(bf, "blasfeo_%sgetrf_rp" % prec)(m, n, dC, 0, 0, dD, 0, 0)
     assert np.array_equal(piv, piv_ref)
-    tol = tol(prec, 100)
-    assert relfro(dD.unpack(), hD.get()) <= tol
+    t = tol(prec, 100)
+    assert relfro(dD.unpack(), hD.get()) <= t
     k = min(m, n)
-    assert relfro(dD.diag_array(k), hD.diag(k)) <= tol
+    assert relfro(dD.diag_array(k), hD.diag(k)) <= t
 
 
 @pytest.mark.parametrize("prec", ["d", "s"])
@@ -213,10 +213,10 @@ def test_geqrf(bf, orc, prec, mn):
     orc.geqrf(prec, m, n, hC, 0, 0, hD, 0, 0)
     dC, dD = dev(bf, m, n, prec, M), dev(bf, m, n, prec)
     getattr(bf, "blasfeo_%sgeqrf" % prec)(m, n, dC, 0, 0, dD, 0, 0)
-    tol = tol(prec, 50)
-    assert relfro(dD.unpack(), hD.get()) <= tol
+    t = tol(prec, 50)
+    assert relfro(dD.unpack(), hD.get()) <= t
     k = min(m, n)
-    assert relfro(dD.diag_array(k), hD.diag(k)) <= tol
+    assert relfro(dD.diag_array(k), hD.diag(k)) <= t
 
 
 @pytest.mark.parametrize("prec", ["d", "s"])

@@ -435,3 +435,24 @@ def test_cm_reference_getrf_rp_pivots_match(mn):
     assert np.array_equal(piv[:min(m, n)], ppiv)
     assert relfro(cD.a, pD.get()) <= 1e-12
     assert _outside_same(cD.a, D0, 1, 3, m, n)
+
+
+def test_riccati_solve_oracle_vs_golden_and_kkt():
+    """The oracle's Riccati factorization + solve (tests/ric_oracle.py composing
+    the oracle routines) reproduces the compiled reference's outputs of
+    d_back_ric_trs_libstr (golden cfg4_trs.npz) and solves the LQ problem's KKT
+    system."""
+    from tests.ric_oracle import ric_trf, ric_trs, kkt_residual
+    g = np.load(os.path.join(GOLD, "cfg4_trs.npz"))
+    orc = oracle_api()
+    N, nx, nu = 30, 12, 4
+    RSQ = np.broadcast_to(np.eye(16), (N + 1, 16, 16)).copy()
+    for p in range(2):
+        BA, b, rq = g["BA%d" % p], g["b%d" % p], g["rq%d" % p]
+        L = ric_trf(orc, BA, RSQ, N, nx, nu)
+        ux, pi = ric_trs(orc, L, BA, b, rq, N, nx, nu)
+        for k in range(N + 1):
+            assert relfro(ux[k], g["ux%d" % p][k][:len(ux[k])]) <= 1e-14, (p, k)
+        assert relfro(np.stack(pi), g["pi%d" % p]) <= 1e-14
+        rs, rd = kkt_residual(BA, RSQ, b, rq, ux, pi, N, nx, nu)
+        assert max(np.abs(r).max() for r in rs + rd) <= 1e-12

@@ -119,6 +119,9 @@ def test_noalloc_largest_size_and_tensor_engine_allocate_nothing():
     for engine in (1, 2):
         st, inf, be, diff = out[engine]
         assert st == 0 and (inf == 0).all() and (be <= 1e-12).all(), engine
-        assert diff <= 1e-10, (engine, diff)  # both engines are backward stable to 1e-12 (cond <= 1e6)
+        # SIMT is the allocating call's engine: the same arithmetic, the same x.  The
+        # tensor-memory engine rounds differently; both solutions are backward stable
+        # to 1e-12, so they agree to about cond(A) * 1e-12 = 1e-6 (cond up to 1e6)
+        assert diff <= (1e-12 if engine == 1 else 1e-5), (engine, diff)
     free0, free1 = out["free"]
     assert free0 == free1, (free0, free1)
