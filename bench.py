@@ -304,6 +304,10 @@ class CpuRun:
         return max(self.sys.backward_error(i) for i in range(0, self.sys.num, max(1, self.sys.num // k)))
 
 
+DESC_DTYPE_CPU = np.dtype([("mem", "<u8"), ("pA", "<u8"), ("dA", "<u8"), ("m", "<i4"), ("n", "<i4"),
+                           ("pm", "<i4"), ("cn", "<i4"), ("use_dA", "<i4"), ("memsize", "<i4")])
+
+
 def cpu_driver():
     d = os.path.join(ROOT, "oracle")
     so = os.path.join(d, "libcpu_bench.so")
@@ -563,7 +567,7 @@ def main():
     dispatch = None
     if not args.no_fp64 and rank == 0:
         try:
-            dispatch = learned_dispatch()
+            dispatch = learned_dispatch(cpu=not args.no_cpu)
         except Exception as ex:  # reported, never silently replaced
             dispatch = {"error": repr(ex)}
     cpu = None
@@ -1024,37 +1028,142 @@ def cpu_riccati_leg(nbt, N, nx, nu, sBA, sRSQ, sL):
     return rep, Lref
 
 
-def learned_dispatch(nlaunch=64, ntrain=44, seed=5):
-    """Mixed-op stream (gemm_nt 40%, potrf_l 25%, getrf_rp 20%, geqrf 15%; sizes
-    log-uniform 4..384, geqrf m = 2n; batches log-uniform 256..8192; FP64): the
-    exhaustive autotuner times every kernel variant of `nlaunch` sampled
-    launches, the MLP cost model (CUDA training kernels) is trained on the
-    first `ntrain` launches and picks the variants of the held-out ones.  Reports
-    regret against the exhaustive best (mean per launch and on total time) for
-    the MLP, the built-in rule and a fixed variant, and the end-to-end GFLOP/s
-    of the held-out stream under each policy."""
+def learned_dispatch(n_ops=1_000_000, train_frac=0.3, seed=5, budget_s=150.0, cpu=True):
+    """Config 5, the mixed-op stream: ops drawn 40% gemm_nt, 25% potrf_l, 20%
+    getrf_rp, 15% geqrf (m = 2n), sizes log-uniform in 4..384 (geqrf n in
+    4..192), batched into launches of log-uniform 256..8192 instances, until
+    the launches hold n_ops instances.  The exhaustive autotuner times every
+    kernel variant of every launch; the MLP cost model is trained by the
+    library's CUDA kernels on the first train_frac of the launches and
+    installed in the library, which then dispatches the held-out launches
+    itself (variant -1; each new launch shape runs the model once on the
+    device).  Reported: regret of the library's picks, of the built-in rule and
+    of a fixed variant against the exhaustive best, on the held-out launches;
+    end-to-end GFLOP/s of the whole stream under each policy; the compiled
+    reference on the host cores for a sample of launches.  If the sweep
+    exceeds budget_s the stream is cut there and the ops actually covered are
+    reported."""
+    import torch
+    import blasfeo_b200 as bf
     from blasfeo_b200 import autotune as at
     from blasfeo_b200.costmodel import CostModel
-    recs = at.sweep(nlaunch, seed=seed, bmin=256, bmax=8192, nmax=384, reps=3)
-    X, y = at.training_set(recs[:ntrain])
+    lib = bf.lib
+    rng = np.random.default_rng(seed)
+    t0 = time.perf_counter()
+    recs, launches_kept, ops = [], [], 0
+    while ops < n_ops and time.perf_counter() - t0 < budget_s:
+        op, batch, m, n, k = at.sample_launch(rng)
+        batch = min(batch, n_ops - ops) if n_ops - ops >= 256 else batch
+        L = at.Launch(op, batch, m[:batch], n[:batch], k[:batch], seed=len(recs))
+        times = [min(L.time(v, 1), L.time(v, 1)) for v in range(at.NVAR[op])]
+        heur = min(L.time(-1, 1), L.time(-1, 1))
+        recs.append({"op": op, "batch": batch, "feat": L.feature_rows(), "times": np.array(times), "heur": heur,
+                     "flops": L.flops})
+        ops += batch
+        nbytes = 8.0 * float(np.sum(L.m * L.k + L.n * L.k + L.m * L.n))
+        if len(launches_kept) < 12 and len(recs) % 7 == 1 and nbytes < 3e8:
+            launches_kept.append(L)  # a sample for the CPU leg
+        else:
+            del L
+    sweep_s = time.perf_counter() - t0
+    ntr = max(4, int(len(recs) * train_frac))
+    X, y = at.training_set(recs[:ntr])
     cm = CostModel(at.NFEAT, seed=0)
-    cm.fit(X, y, epochs=300, lr=2e-3, batch=128)
-    test = recs[ntrain:]
+    cm.fit(X, y, epochs=200, lr=2e-3, batch=256)
+    test = recs[ntr:]
     picks = [cm.pick(r["feat"]) for r in test]
-    fl = sum(r["flops"] for r in test)
-    t_best = sum(float(r["times"].min()) for r in test)
-    t_mlp = sum(float(r["times"][p]) for r, p in zip(test, picks))
-    t_rule = sum(float(r["heur"]) for r in test)
-    t_v0 = sum(float(r["times"][0]) for r in test)
-    out = {"launches": nlaunch, "train": ntrain, "test": len(test),
-           "ops_in_test": {op: sum(1 for r in test if r["op"] == op) for op in at.OPS},
-           "instances_in_test": int(sum(r["batch"] for r in test))}
-    for name, picks_ in (("mlp", picks), ("rule", [-1] * len(test)), ("variant0", [0] * len(test))):
-        mean, tot = at.regret(test, picks_)
+    out = {"ops": ops, "launches": len(recs), "train_launches": ntr, "test_launches": len(test),
+           "complete": ops >= n_ops, "sweep_s": sweep_s,
+           "ops_by_kind": {op_: int(sum(r["batch"] for r in recs if r["op"] == op_)) for op_ in at.OPS}}
+    for name, pk in (("mlp", picks), ("rule", [-1] * len(test)), ("variant0", [0] * len(test))):
+        mean, tot = at.regret(test, pk)
         out["regret_" + name] = {"mean_per_launch": mean, "total_time": tot}
-    out["gflops"] = {"exhaustive": fl / t_best / 1e6, "mlp": fl / t_mlp / 1e6, "rule": fl / t_rule / 1e6,
-                     "variant0": fl / t_v0 / 1e6}
+    # the library dispatching the held-out launches itself with the installed model
+    rng2 = np.random.default_rng(seed)
+    lib_t, lib_match = 0.0, 0
+    try:
+        cm.install()
+        # rebuild the held-out launches (same draws) and time variant -1 through the library
+        idx = 0
+        ops2 = 0
+        while idx < len(recs):
+            op, batch, m, n, k = at.sample_launch(rng2)
+            batch = min(batch, n_ops - ops2) if n_ops - ops2 >= 256 else batch
+            ops2 += batch
+            if idx >= ntr:
+                L = at.Launch(op, batch, m[:batch], n[:batch], k[:batch], seed=idx)
+                P_ = lambda t_: C.c_void_p(t_.data_ptr())
+                pk = lib.blasfeo_b200_dispatch_pick(at.OPS.index(op), batch, P_(L.mv), P_(L.nv), P_(L.kv), L.maxm,
+                                                   L.maxn, L.maxk, None)
+                lib_match += int(pk == picks[idx - ntr])
+                lib_t += min(L.time(-1, 1), L.time(-1, 1))
+                del L
+            idx += 1
+    finally:
+        CostModel.uninstall()
+    best_test = sum(float(r["times"].min()) for r in test)
+    out["regret_library_dispatch"] = {"total_time": lib_t / best_test - 1.0 if best_test > 0 else None,
+                                      "picks_equal_to_model_argmin": lib_match, "of": len(test)}
+    fl = sum(r["flops"] for r in recs)
+    # whole stream: the training launches run with the exhaustive best (that is what was measured for them)
+    t_best = sum(float(r["times"].min()) for r in recs)
+    t_rule = sum(float(r["heur"]) for r in recs)
+    t_v0 = sum(float(r["times"][0]) for r in recs)
+    t_mlp = sum(float(r["times"].min()) for r in recs[:ntr]) + sum(float(r["times"][p]) for r, p in zip(test, picks))
+    out["stream_gflops"] = {"exhaustive": fl / t_best / 1e6, "mlp": fl / t_mlp / 1e6, "rule": fl / t_rule / 1e6,
+                            "variant0": fl / t_v0 / 1e6, "total_gflop": fl / 1e9}
+    if cpu:
+        try:
+            out["cpu_reference"] = cpu_ops_leg(launches_kept, {r_["op"]: 0 for r_ in recs})
+        except Exception as ex:  # reported, never silently replaced
+            out["cpu_reference"] = {"error": repr(ex)}
+    del launches_kept
+    torch.cuda.empty_cache()
     return out
+
+
+def cpu_ops_leg(launches, _ops):
+    """The compiled reference on host copies of a sample of the stream's
+    launches (blasfeo_dgemm_nt / dpotrf_l / dgetrf_rp per instance; dgeqrf from
+    the GENERIC build, whose HP Haswell version crashes on unaligned stack
+    buffers), one thread per physical core; GFLOP/s of the sample, and the same
+    sample's GPU time under the exhaustive best variants."""
+    from blasfeo_b200 import autotune as at
+    from oracle.pyoracle import DMat, ref_lib, ref_available
+    lib_, prefix, kind, name = cpu_library()
+    gen = ref_lib("generic") if ref_available("generic") else lib_
+    drv = cpu_driver()
+    drv.cpu_ops_batch.restype = C.c_double
+    f = lambda L_, s_: C.cast(getattr(L_, prefix + s_), C.c_void_p)
+    fl, tc, tg = 0.0, 0.0, 0.0
+    keep = []
+    for L in launches:
+        def host(slab, rows, cols):
+            h = np.ascontiguousarray(slab.buf.cpu().numpy())
+            d = slab.desc.cpu().numpy().view(DESC_DTYPE_CPU).copy()
+            shift = h.ctypes.data - slab.buf.data_ptr()
+            for fld in ("mem", "pA", "dA"):
+                d[fld] = (d[fld].astype(np.int64) + shift).astype(np.uint64)
+            arr = (DMat * len(d)).from_buffer_copy(d.tobytes())
+            keep.append((h, arr))
+            return arr
+        A = host(L.A, L.m, L.n)
+        B = host(L.B, L.n, L.k) if L.op == "gemm_nt" else A
+        D = host(L.D, L.m, L.n)
+        iv = lambda a: (C.c_int * len(a))(*[int(v) for v in a])
+        mm, nn, kk = iv(L.m), iv(L.n), iv(L.k)
+        opi = at.OPS.index(L.op)
+        geq = (C.cast(getattr(gen, "blasfeo_dgeqrf_worksize"), C.c_void_p), C.cast(getattr(gen, "blasfeo_dgeqrf"),
+                                                                                   C.c_void_p))
+        run = lambda P_: drv.cpu_ops_batch(P_, opi, L.batch, mm, nn, kk, A, B, D, f(lib_, "gemm_nt"),
+                                           f(lib_, "potrf_l"), f(lib_, "getrf_rp"), geq[0], geq[1], L.maxm, L.maxn)
+        P_, tp, _ = _cpu_times(run, passes=3, p1_passes=1)
+        tc += tp
+        fl += L.flops
+        tg += min(L.time(v, 1) for v in range(at.NVAR[L.op])) * 1e-3
+    return {"kind": kind, "library": name, "cores": P_, "launches": len(launches), "gflops": fl / tc / 1e9,
+            "gpu_gflops_same_sample": fl / tg / 1e9,
+            "sample": "%d launches of the stream (host copies of their slabs), %.2f GFLOP" % (len(launches), fl / 1e9)}
 
 
 def run_e2e(args, W, lib, torch, dev, stream, barrier, world):

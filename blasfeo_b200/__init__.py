@@ -197,6 +197,10 @@ _sig("blasfeo_b200_mlp_work_bytes", _sz, _i, _i)
 _sig("blasfeo_b200_mlp_forward", _i, _i, _i, _vp, _i, _vp, _vp, _vp, _vp)
 _sig("blasfeo_b200_mlp_grad", _i, _i, _i, _vp, _i, _vp, _vp, _vp, _vp, _vp, _vp)
 _sig("blasfeo_b200_mlp_adam", _i, _i, _vp, _vp, _vp, _vp, _i, _f, _vp)
+_sig("blasfeo_b200_cost_model_nfeat", _i)
+_sig("blasfeo_b200_set_cost_model", _i, _i, _i, _vp)
+_sig("blasfeo_b200_clear_cost_model", None)
+_sig("blasfeo_b200_dispatch_pick", _i, _i, _i, _vp, _vp, _vp, _i, _i, _i, _vp)
 _sig("blasfeo_dsposv_noalloc_scratch_bytes", _sz)
 _sig("blasfeo_dsposv_l_vbatch_noalloc", _i, _i, _vp, _i, _vp, _vp, _vp, _i, _d, _vp, _vp, _vp, _vp)
 

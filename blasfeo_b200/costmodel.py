@@ -92,3 +92,30 @@ class CostModel:
     def pick(self, feat_rows):
         """Variant with the smallest predicted time (feat_rows: one row per variant)."""
         return int(np.argmin(self.predict(feat_rows)))
+
+    def install(self):
+        """Make the library dispatch with this model: the *_vbatch routines called
+        with variant -1 take its picks (blasfeo_b200_set_cost_model)."""
+        p = np.ascontiguousarray(self.params.cpu().numpy(), dtype=np.float32)
+        check(lib.blasfeo_b200_set_cost_model(self.nin, self.H, C.c_void_p(p.ctypes.data)))
+
+    @staticmethod
+    def uninstall():
+        lib.blasfeo_b200_clear_cost_model()
+
+    def save(self, path, key):
+        """Persist the trained parameters, keyed like the autotune table (GPU,
+        CUDA version, library build): load() refuses a file of another key."""
+        np.savez(path, key=np.array(key), params=self.params.cpu().numpy(), nin=self.nin, hidden=self.H, mu=self.mu,
+                 sd=self.sd)
+
+    @classmethod
+    def load(cls, path, key, device="cuda"):
+        import torch
+        d = np.load(path)
+        if str(d["key"]) != key:
+            return None
+        cm = cls(int(d["nin"]), int(d["hidden"]), device=device)
+        cm.params = torch.from_numpy(d["params"].astype(np.float32)).to(device)
+        cm.mu, cm.sd = float(d["mu"]), float(d["sd"])
+        return cm

@@ -524,6 +524,7 @@ int blasfeo_dgemm_nt_vbatch_variant(int batch, const int *m, const int *n, const
                                     int variant, void *stream) {
 	if (batch < 0 || !m || !n || !k || !sA || !sB || !sC || !sD) return BLASFEO_B200_EINVAL;
 	if (variant > 5) return BLASFEO_B200_EINVAL;
+	if (variant < 0 && batch > 0) variant = bf::dispatch_pick(0, batch, m, n, k, max_m, max_n, max_k, (cudaStream_t)stream);
 	return bf::gemm_nt_launch<double, false>(batch, var_sizes(m, n, k), max_m, max_n, max_k, alpha,
 	                                         vbatch_arg<double>(sA), vbatch_arg<double>(sB), beta,
 	                                         vbatch_arg<double>(sC), vbatch_arg<double>(sD), (cudaStream_t)stream,

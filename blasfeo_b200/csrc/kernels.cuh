@@ -29,4 +29,10 @@ template <typename T>
 int potrf_launch(int batch, SizeArg sz, int max_m, MatArg<T> C, MatArg<T> D, int *info, cudaStream_t s,
                  int variant);
 
+// learned dispatch (dispatch.cu): the installed cost model's variant for a
+// launch of op (0 gemm_nt, 1 potrf_l, 2 getrf_rp, 3 geqrf) with device size
+// arrays m, n, k (k may be null: n), or -1 for the built-in rule
+int dispatch_pick(int op, int batch, const int *m, const int *n, const int *k, int max_m, int max_n, int max_k,
+                  cudaStream_t s);
+
 }  // namespace bf

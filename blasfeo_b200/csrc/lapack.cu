@@ -789,6 +789,7 @@ int blasfeo_dpotrf_l_vbatch_variant(int batch, const int *m, int max_m, const st
                                     const struct blasfeo_dmat *sD, int *info, int variant, void *stream) {
 	if (batch < 0 || !m || !sC || !sD || max_m < 0 || variant > 5) return BLASFEO_B200_EINVAL;
 	if (batch == 0 || max_m == 0) return BLASFEO_B200_OK;
+	if (variant < 0) variant = bf::dispatch_pick(1, batch, m, m, m, max_m, max_m, max_m, (cudaStream_t)stream);
 	return bf::potrf_launch<double>(batch, var_sizes(m, m, nullptr), max_m, vbatch_arg<double>(sC),
 	                                vbatch_arg<double>(sD), info, (cudaStream_t)stream, variant);
 }
@@ -801,6 +802,7 @@ int blasfeo_dgetrf_rp_vbatch_variant(int batch, const int *m, const int *n, int 
                                      int ipiv_stride, int *info, int variant, void *stream) {
 	if (batch < 0 || !m || !n || !sC || !sD || !ipiv || max_m < 0 || max_n < 0 || variant > 5) return BLASFEO_B200_EINVAL;
 	if (batch == 0 || max_m == 0 || max_n == 0) return BLASFEO_B200_OK;
+	if (variant < 0) variant = bf::dispatch_pick(2, batch, m, n, n, max_m, max_n, max_n, (cudaStream_t)stream);
 	return getrf_launch<double>(batch, var_sizes(m, n, nullptr), vbatch_arg<double>(sC), vbatch_arg<double>(sD), ipiv,
 	                            ipiv_stride, info, (cudaStream_t)stream, max_m, max_n, variant);
 }
@@ -814,6 +816,7 @@ int blasfeo_dgeqrf_vbatch_variant(int batch, const int *m, const int *n, int max
                                   void *stream) {
 	if (batch < 0 || !m || !n || !sC || !sD || max_m < 0 || max_n < 0 || variant > 5) return BLASFEO_B200_EINVAL;
 	if (batch == 0 || max_m == 0 || max_n == 0) return BLASFEO_B200_OK;
+	if (variant < 0) variant = bf::dispatch_pick(3, batch, m, n, n, max_m, max_n, max_n, (cudaStream_t)stream);
 	return geqrf_launch<double>(batch, var_sizes(m, n, nullptr), vbatch_arg<double>(sC), vbatch_arg<double>(sD),
 	                            (cudaStream_t)stream, max_m, max_n, variant);
 }

@@ -387,6 +387,29 @@ int blasfeo_dgetrf_rp_vbatch_variant(int batch, const int *m, const int *n, int 
 int blasfeo_dgeqrf_vbatch_variant(int batch, const int *m, const int *n, int max_m, int max_n,
 	const struct blasfeo_dmat *sC, const struct blasfeo_dmat *sD, int variant, void *stream);
 
+/* Learned dispatch (no reference counterpart).  With a cost model installed,
+ * the four *_vbatch_variant routines called with variant -1 (and the plain
+ * *_vbatch routines, which pass -1) take the variant the model predicts
+ * fastest instead of the built-in rule.  The model is the MLP of the
+ * blasfeo_b200_mlp_* kernels with nin = blasfeo_b200_cost_model_nfeat() inputs:
+ *   [op one-hot (gemm_nt, potrf_l, getrf_rp, geqrf), log2(batch)/13,
+ *    mean/9, max/9 and std/4 of log2 of the per-instance m, n and k,
+ *    variant one-hot (6)]
+ * (potrf_l: m = n = k = the sizes; getrf_rp, geqrf: k = n), trained to
+ * predict the log run time.  A pick runs the feature and MLP kernels on the
+ * launch's stream and synchronises it once to read the predictions; picks are
+ * cached per (device, op, batch, max_m, max_n, max_k), so a repeated launch
+ * shape dispatches without the model.  A stream under capture never runs the
+ * model (a cached pick, else the built-in rule).  set copies the parameters
+ * (blasfeo_b200_mlp_param_count(nin, hidden) floats, host memory) and clears
+ * the cache; EINVAL for a wrong nin.  dispatch_pick returns the variant a
+ * launch would take (-1: the built-in rule; -2: bad arguments). */
+int blasfeo_b200_cost_model_nfeat(void);
+int blasfeo_b200_set_cost_model(int nin, int hidden, const float *params);
+void blasfeo_b200_clear_cost_model(void);
+int blasfeo_b200_dispatch_pick(int op, int batch, const int *m, const int *n, const int *k, int max_m, int max_n,
+	int max_k, void *stream);
+
 /* ---- fused solvers (no reference counterpart; built from dpotrf_l + dtrsv_lnn + dtrsv_ltn) ----
  * Solve A x = b for a variable-size batch of SPD systems; A is read from the
  * lower triangle of each descriptor (full storage, upper part ignored).

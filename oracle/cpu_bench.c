@@ -219,3 +219,40 @@ double cpu_ric_trf_batch(int nthreads, int batch, int N, int nx, int nu, double 
 	                    (syrk_potrf_fn)syrk_potrf};
 	return run_threads(nthreads, batch, ric_one, &a, 16 * ((nx + 3) / 4 * 4) + 16);
 }
+
+/* ---- one batched launch of the mixed-op stream: gemm_nt (D = A B^T),
+ * potrf_l, getrf_rp, geqrf per instance (descriptor arrays in host memory,
+ * instance i of A / B / D at A[i], B[i], D[i]) ---- */
+typedef void (*getrf_fn)(int, int, struct dm *, int, int, struct dm *, int, int, int *);
+typedef int (*geqrf_ws_fn)(int, int);
+typedef void (*geqrf_fn)(int, int, struct dm *, int, int, struct dm *, int, int, void *);
+struct ops_arg {
+	int op;
+	const int *m, *n, *k;
+	struct dm *A, *B, *D;
+	gemm_fn gemm; potrf_fn potrf; getrf_fn getrf; geqrf_ws_fn geqrf_ws; geqrf_fn geqrf;
+};
+
+static void ops_one(void *p, int i, double *scr)
+{
+	struct ops_arg *a = (struct ops_arg *)p;
+	const int m = a->m[i], n = a->n[i];
+	switch (a->op) {
+	case 0: a->gemm(m, n, a->k[i], 1.0, &a->A[i], 0, 0, &a->B[i], 0, 0, 0.0, &a->D[i], 0, 0, &a->D[i], 0, 0); break;
+	case 1: a->potrf(n, &a->A[i], 0, 0, &a->D[i], 0, 0); break;
+	case 2: a->getrf(m, n, &a->A[i], 0, 0, &a->D[i], 0, 0, (int *)scr); break;
+	default: a->geqrf(m, n, &a->A[i], 0, 0, &a->D[i], 0, 0, scr + 512); break;
+	}
+}
+
+/* scratch per thread: pivots (512 ints) then the geqrf work buffer */
+double cpu_ops_batch(int nthreads, int op, int batch, const int *m, const int *n, const int *k, struct dm *A,
+                     struct dm *B, struct dm *D, void *gemm, void *potrf, void *getrf, void *geqrf_ws, void *geqrf,
+                     int max_m, int max_n)
+{
+	struct ops_arg a = {op, m, n, k, A, B, D, (gemm_fn)gemm, (potrf_fn)potrf, (getrf_fn)getrf,
+	                    (geqrf_ws_fn)geqrf_ws, (geqrf_fn)geqrf};
+	size_t ws = 1024;
+	if (op == 3 && geqrf_ws) ws += (size_t)((geqrf_ws_fn)geqrf_ws)(max_m, max_n) / sizeof(double) + 64;
+	return run_threads(nthreads, batch, ops_one, &a, ws);
+}

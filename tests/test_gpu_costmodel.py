@@ -100,5 +100,41 @@ def test_learned_dispatch_regret(bf):
     fixed_mean, fixed_tot = at.regret(test, [0] * len(test))
     print("regret mlp %.3f/%.3f  variant-0 %.3f/%.3f  rule %s" % (mlp_mean, mlp_tot, fixed_mean, fixed_tot,
                                                                   at.regret(test, [-1] * len(test))))
+    rule_mean, rule_tot = at.regret(test, [-1] * len(test))
     assert mlp_tot < 0.25
     assert mlp_tot < fixed_tot
+    # what the trained network gains over the method without it (the built-in
+    # rule the library uses when no model is installed), on the held-out launches
+    assert mlp_tot < rule_tot, (mlp_tot, rule_tot)
+
+
+def test_library_dispatch_uses_the_installed_model(bf):
+    """With the cost model installed, a *_vbatch call with variant -1 takes the
+    model's pick (the same variant the Python-side argmin chooses), computed on
+    the device from the launch's size arrays; without a model it takes the
+    built-in rule (-1).  Results equal those of the picked variant."""
+    import torch
+    from blasfeo_b200 import autotune as at
+    from blasfeo_b200.costmodel import CostModel
+    recs = at.sweep(16, seed=3, bmin=256, bmax=1024, nmax=160, reps=2)
+    X, y = at.training_set(recs)
+    cm = CostModel(at.NFEAT, seed=1)
+    cm.fit(X, y, epochs=120, lr=2e-3, batch=64)
+    assert bf.lib.blasfeo_b200_cost_model_nfeat() == at.NFEAT
+    rng = np.random.default_rng(9)
+    P = lambda t: C.c_void_p(t.data_ptr())
+    try:
+        cm.install()
+        for i in range(8):
+            op, batch, m, n, k = at.sample_launch(rng, at.OPS[i % 4], 256, 1024, 160)
+            L = at.Launch(op, batch, m, n, k, seed=i)
+            want = cm.pick(L.feature_rows())
+            got = bf.lib.blasfeo_b200_dispatch_pick(at.OPS.index(op), batch, P(L.mv), P(L.nv), P(L.kv), L.maxm, L.maxn,
+                                                    L.maxk, None)
+            assert got == want, (op, got, want)
+            assert L.run(-1) == 0  # the call itself dispatches through the model (cached pick)
+            torch.cuda.synchronize()
+    finally:
+        CostModel.uninstall()
+    assert bf.lib.blasfeo_b200_dispatch_pick(0, 4, P(L.mv), P(L.nv), P(L.kv), 4, 4, 4, None) == -1
+    assert bf.lib.blasfeo_b200_set_cost_model(at.NFEAT + 1, 128, None) == 1
