@@ -235,7 +235,9 @@ class HostSystems:
         for i, n in enumerate(self.ns):
             offs[i] = acc
             acc += size[int(n)]
-        self.slab = np.zeros(acc + 8)
+        # the reference's AVX kernels need 64-byte aligned panel-major storage
+        from oracle.pyoracle import _aligned_zeros
+        self.slab = _aligned_zeros(acc + 8, np.float64)
         for n, (idx, X) in mats.items():
             pm = (n + 3) // 4 * 4
             pad = torch.zeros((len(idx), pm, pm), dtype=torch.float64, device=X.device)
@@ -246,8 +248,8 @@ class HostSystems:
         self.mats_by_n = mats
         vlen = (self.ns + 3) // 4 * 4
         voff = np.concatenate([[0], np.cumsum(vlen)[:-1]]).astype(np.int64)
-        self.b = np.zeros(int(vlen.sum()) + 4)
-        self.x = np.zeros_like(self.b)
+        self.b = _aligned_zeros(int(vlen.sum()) + 4, np.float64)
+        self.x = _aligned_zeros(int(vlen.sum()) + 4, np.float64)
         for i, r in enumerate(rhs):
             self.b[voff[i]:voff[i] + len(r)] = r
         self.rhs, self.voff = rhs, voff
@@ -941,8 +943,12 @@ def riccati_errors(L, ref, nx, nu, N):
 
 
 def _host_slab(B):
-    """Host copy of a device uniform-batch slab (same layout): (array, pointer to instance 0, stride)."""
-    h = np.ascontiguousarray(B.buf.cpu().numpy()).view(np.float64)
+    """Host copy of a device uniform-batch slab (same layout, 64-byte aligned as
+    the reference's AVX kernels need): (array, pointer to instance 0, stride)."""
+    from oracle.pyoracle import _aligned_zeros
+    src = B.buf.cpu().numpy().view(np.float64)
+    h = _aligned_zeros(src.size, np.float64)
+    h[:] = src
     off = (B.s.pA - B.buf.data_ptr()) // 8
     return h, h.ctypes.data + 8 * off, B.s.stride
 
@@ -1139,7 +1145,10 @@ def cpu_ops_leg(launches, _ops):
     keep = []
     for L in launches:
         def host(slab, rows, cols):
-            h = np.ascontiguousarray(slab.buf.cpu().numpy())
+            from oracle.pyoracle import _aligned_zeros
+            src = slab.buf.cpu().numpy()
+            h = _aligned_zeros(src.size, np.float64)
+            h[:] = src
             d = slab.desc.cpu().numpy().view(DESC_DTYPE_CPU).copy()
             shift = h.ctypes.data - slab.buf.data_ptr()
             for fld in ("mem", "pA", "dA"):

@@ -146,36 +146,22 @@ __global__ void k_invdiag(SizeArg sz, MatArg<T> A) {
 	a.d[l] = T(1) / a.at(l, l);
 }
 
-// D = alpha * B * A^{-T}, A lower: one thread per row of D, columns left to
-// right; non-unit (trsm_rltn) multiplies each column by the cached inverse
-// diagonal (kernel/generic/kernel_dgemm_4x4_lib4.c:5970
-// kernel_dtrsm_nt_rl_inv), unit (trsm_rltu, blasfeo_ref/x_blas3_ref.c:1760)
-// takes the diagonal of A as 1 and never reads it.
-template <typename T, bool UNIT>
-__global__ void k_trsm_rltn(SizeArg sz, T alpha, MatArg<T> A, MatArg<T> B, MatArg<T> D) {
-	int b = blockIdx.x;
-	int m = sz.M(b), n = sz.N(b);
-	int i = blockIdx.y * blockDim.x + threadIdx.x;
-	if (i >= m) return;
-	PMat<T> a = A.get(b), bb = B.get(b), d = D.get(b);
-	const T *inv = a.d;
-	for (int j = 0; j < n; j++) {
-		T c = alpha * bb.at(i, j);
-		for (int l = 0; l < j; l++) c = fma(-d.at(i, l), a.at(j, l), c);
-		d.at(i, j) = UNIT ? c : c * inv[j];
-	}
-}
-
-// The same solve for n <= NMAX (16, 32, 64): the lower triangle of A and its
+// D = alpha * B * A^{-T}, A lower (trsm_rltn non-unit: each column is
+// multiplied by the cached inverse diagonal, kernel/generic/
+// kernel_dgemm_4x4_lib4.c:5970 kernel_dtrsm_nt_rl_inv; trsm_rltu unit: the
+// diagonal of A is taken as 1 and never read, blasfeo_ref/x_blas3_ref.c:1760).
+// Element (i,k) is d_ik = (alpha b_ik - sum_{l<k} d_il a_kl) * inv_k with the
+// sum accumulated in increasing l.
+//
+// For n <= NMAX (16, 32, 64): the lower triangle of A and its
 // inverse diagonal are staged in shared memory once per CTA, and each row of
 // the right-hand side lives in registers, updated right-looking (after d_ij:
 // c_ik -= d_ij a_kj for k > j, A's column j read by every thread at once).
 // TPR threads share a row (columns interleaved, k = TPR q + h), so a row of 64
 // doubles fits in registers; the thread that owns column j passes d_ij to its
-// partner by a shuffle within the pair.  Element (i,k) sees exactly the
-// operations of k_trsm_rltn, in the same order (alpha b_ik, then the FMAs over
-// l = 0..k-1), so the results are identical; nothing is re-read from global
-// memory inside the recurrence.  64 rows per CTA, blockDim.x = 64 TPR.
+// partner by a shuffle within the pair.  Element (i,k) sees alpha b_ik, then
+// the FMAs over l = 0..k-1 in order; nothing is re-read from global memory
+// inside the recurrence.  64 rows per CTA, blockDim.x = 64 TPR.
 template <typename T, bool UNIT, int NMAX, int TPR>
 __global__ void __launch_bounds__(64 * TPR) k_trsm_rltn_reg(SizeArg sz, T alpha, MatArg<T> A, MatArg<T> B,
                                                              MatArg<T> D) {
@@ -229,6 +215,87 @@ __global__ void __launch_bounds__(64 * TPR) k_trsm_rltn_reg(SizeArg sz, T alpha,
 	}
 }
 
+// n > 64: the same register solve by column blocks of 64.  Block J
+// (columns c0 = 64 J ..) first receives the contributions of the solved
+// columns l < c0, -sum_l d_il a_kl, from chunks of 64 columns of A staged in
+// shared memory (d_il re-read from D, where the row's threads wrote it), then
+// runs the in-block recurrence of k_trsm_rltn_reg.  Element (i,k) again sees
+// alpha b_ik followed by the FMAs over l = 0..k-1 in increasing l, as in
+// k_trsm_rltn_reg.  Dynamic shared memory: two 64 x 64 blocks of
+// A and 64 inverse-diagonal entries.
+template <typename T, bool UNIT, int TPR>
+__global__ void __launch_bounds__(64 * TPR) k_trsm_rltn_blk(SizeArg sz, T alpha, MatArg<T> A, MatArg<T> B,
+                                                             MatArg<T> D) {
+	constexpr int NB = 64, NQ = NB / TPR;
+	extern __shared__ __align__(16) unsigned char trsm_smem[];
+	T *sa = (T *)trsm_smem;      // sa[j * NB + k] = a(c0 + k, c0 + j), k > j
+	T *sg = sa + NB * NB;        // sg[l * NB + k] = a(c0 + k, l0 + l)
+	T *sinv = sg + NB * NB;
+	const int b = blockIdx.x;
+	const int m = sz.M(b), n = sz.N(b);
+	const PMat<T> a = A.get(b), bb = B.get(b), d = D.get(b);
+	const int tid = threadIdx.x, nt = blockDim.x;
+	const int h = tid % TPR;
+	const int i = blockIdx.y * 64 + tid / TPR;
+	const bool row = i < m;
+	const int lane = tid & 31;
+	const unsigned pair = (TPR == 1) ? (1u << lane) : (3u << (lane & ~1));
+	for (int c0 = 0; c0 < n; c0 += NB) {
+		const int nb = n - c0 < NB ? n - c0 : NB;
+		T c[NQ];
+#pragma unroll
+		for (int q = 0; q < NQ; q++) {
+			const int k = q * TPR + h;
+			c[q] = (row && k < nb) ? alpha * bb.at(i, c0 + k) : T(0);
+		}
+		for (int l0 = 0; l0 < c0; l0 += NB) {
+			__syncthreads();
+			for (int e = tid; e < NB * NB; e += nt) {
+				const int k = e & (NB - 1), l = e / NB;
+				sg[l * NB + k] = (k < nb) ? a.at(c0 + k, l0 + l) : T(0);
+			}
+			__syncthreads();
+			if (row) {
+#pragma unroll 4
+				for (int l = 0; l < NB; l++) {
+					const T dl = d.at(i, l0 + l);
+#pragma unroll
+					for (int q = 0; q < NQ; q++) c[q] = fma(-dl, sg[l * NB + q * TPR + h], c[q]);
+				}
+			}
+		}
+		__syncthreads();
+		for (int e = tid; e < NB * NB; e += nt) {
+			const int k = e & (NB - 1), j = e / NB;
+			if (j < nb && k < nb && k > j) sa[j * NB + k] = a.at(c0 + k, c0 + j);
+		}
+		if (!UNIT && tid < nb) sinv[tid] = a.d[c0 + tid];
+		__syncthreads();
+#pragma unroll
+		for (int j = 0; j < NB; j++) {
+			if (j >= nb) break;
+			const int qj = j / TPR, hj = j % TPR;
+			T dj = T(0);
+			if (h == hj) dj = UNIT ? c[qj] : c[qj] * sinv[j];
+			if (TPR > 1) dj = __shfl_sync(pair, dj, (lane & ~(TPR - 1)) | hj);
+			if (h == hj) c[qj] = dj;
+#pragma unroll
+			for (int q = 0; q < NQ; q++) {
+				const int k = q * TPR + h;
+				if (k > j && k < nb) c[q] = fma(-dj, sa[j * NB + k], c[q]);
+			}
+		}
+		if (row) {
+#pragma unroll
+			for (int q = 0; q < NQ; q++) {
+				const int k = q * TPR + h;
+				if (k < nb) d.at(i, c0 + k) = c[q];
+			}
+		}
+		__syncwarp();  // the row's other thread reads these columns in the next block
+	}
+}
+
 template <typename T, bool UNIT>
 void trsm_rltn_kernel(int batch, SizeArg sz, int m, int n, T alpha, MatArg<T> A, MatArg<T> B, MatArg<T> D,
                       cudaStream_t s) {
@@ -241,8 +308,12 @@ void trsm_rltn_kernel(int batch, SizeArg sz, int m, int n, T alpha, MatArg<T> A,
 		k_trsm_rltn_reg<T, UNIT, 32, 1><<<grid, 64, 0, s>>>(sz, alpha, A, B, D);
 	else if (n <= 64)
 		k_trsm_rltn_reg<T, UNIT, 64, TPR64><<<grid, 64 * TPR64, 0, s>>>(sz, alpha, A, B, D);
-	else
-		k_trsm_rltn<T, UNIT><<<grid, 64, 0, s>>>(sz, alpha, A, B, D);
+	else {
+		const size_t smem = (2 * 64 * 64 + 64) * sizeof(T);
+		auto kern = k_trsm_rltn_blk<T, UNIT, TPR64>;
+		if (smem > 48 * 1024) cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+		kern<<<grid, 64 * TPR64, smem, s>>>(sz, alpha, A, B, D);
+	}
 }
 
 // D = alpha * B * A, A lower non-unit (blasfeo_hp_pm/d_blas3_lib4.c:4893).

@@ -159,6 +159,56 @@ struct DiagCol<CHOL_NB, T, WIDTH> {
 	}
 };
 
+// FP32 data: the 16 x 16 lower block, staged row-major in blk (16 rows of 17),
+// is factored by every lane of the warp at once, each holding the whole lower
+// triangle in registers, so the pivot chain issues no shuffles: under the
+// trailing update of the other warps, which keeps the shared-memory / shuffle
+// unit busy, each of the 16 pivot steps of DiagCol waited for that unit
+// several times (clock64 probe of the n = 256 solver: 11.7k cycles per block).
+// Same operations in the same order as DiagCol (pivot rule of
+// kernel/generic/kernel_dgemm_4x4_lib4.c:5700-5710 with FP64 pivots and
+// reciprocals, column scaling, then the rank-1 update of the trailing columns
+// in column order), so the factor is bitwise the same.  Lane i < 16 receives
+// row i of L in r; lane i < nbk writes dinv[c0 + i]; the first non-positive
+// pivot (c0 + j + 1) goes to *bad.
+template <typename T>
+__device__ __forceinline__ void diag_factor_rep(const T *blk, int nbk, int c0, double *dinv, int *bad,
+                                                T (&r)[CHOL_NB], int lane) {
+	T a[CHOL_NB * (CHOL_NB + 1) / 2];  // packed lower triangle, (i, j) at i (i + 1) / 2 + j
+#pragma unroll
+	for (int i = 0; i < CHOL_NB; i++)
+#pragma unroll
+		for (int j = 0; j <= i; j++) a[i * (i + 1) / 2 + j] = blk[i * 17 + j];
+	double inv_all[CHOL_NB];
+	int first_bad = 0;
+#pragma unroll
+	for (int J = 0; J < CHOL_NB; J++) {
+		const double cj = (double)a[J * (J + 1) / 2 + J];
+		const bool ok = cj > 0.0;
+		const double inv = ok ? rsqrt(cj) : 0.0;
+		inv_all[J] = inv;
+		if (!ok && J < nbk && first_bad == 0) first_bad = J + 1;
+		a[J * (J + 1) / 2 + J] = (T)(ok ? cj * inv : 0.0);
+#pragma unroll
+		for (int i = J + 1; i < CHOL_NB; i++) a[i * (i + 1) / 2 + J] = a[i * (i + 1) / 2 + J] * (T)inv;
+#pragma unroll
+		for (int l = J + 1; l < CHOL_NB; l++)
+#pragma unroll
+			for (int i = l; i < CHOL_NB; i++)
+				a[i * (i + 1) / 2 + l] = fma(-a[i * (i + 1) / 2 + J], a[l * (l + 1) / 2 + J], a[i * (i + 1) / 2 + l]);
+	}
+#pragma unroll
+	for (int l = 0; l < CHOL_NB; l++) r[l] = T(0);
+#pragma unroll
+	for (int i = 0; i < CHOL_NB; i++)
+		if (lane == i) {
+#pragma unroll
+			for (int l = 0; l <= i; l++) r[l] = a[i * (i + 1) / 2 + l];
+			if (i < nbk) dinv[c0 + i] = inv_all[i];
+		}
+	if (lane == 0 && first_bad && *bad == 0) *bad = c0 + first_bad;
+}
+
 // Write the factored diagonal block (lane i: row i in r) back into S and into
 // the row-major Lt (reciprocal pivots, from the FP64 dinv, in column 16).
 template <typename T>
@@ -183,7 +233,7 @@ __device__ __forceinline__ void chol_diag_store(T *S, int c0, int nbk, const dou
 // into dinv[c0+j] (FP64), the first bad pivot (j+1) into *bad, and for the
 // panel solve a row-major 16x17 copy Lt of L_KK in the working precision with
 // the reciprocal pivots in column 16.
-template <typename T>
+template <typename T, bool REP = false>
 __device__ void chol_diag_factor(T *S, int c0, int nbk, double *dinv, T *Lt, int *bad) {
 	const int lane = threadIdx.x & 31;
 	T r[CHOL_NB];
@@ -198,7 +248,17 @@ __device__ void chol_diag_factor(T *S, int c0, int nbk, double *dinv, T *Lt, int
 		}
 		r[l] = x;
 	}
-	DiagCol<0, T>::run(r, lane, nbk, c0, dinv, bad);
+	if constexpr (REP && sizeof(T) == 4) {
+		if (lane < CHOL_NB) {
+#pragma unroll
+			for (int l = 0; l < CHOL_NB; l++) Lt[lane * 17 + l] = r[l];
+		}
+		__syncwarp();
+		diag_factor_rep<T>(Lt, nbk, c0, dinv, bad, r, lane);
+		__syncwarp();  // every lane has read the staged block before it is overwritten
+	} else {
+		DiagCol<0, T>::run(r, lane, nbk, c0, dinv, bad);
+	}
 	chol_diag_store<T>(S, c0, nbk, dinv, Lt, r, lane);
 }
 
@@ -210,7 +270,7 @@ __device__ void chol_diag_factor(T *S, int c0, int nbk, double *dinv, T *Lt, int
 // partial sums meet by one shuffle.  The update runs in the working precision
 // T, the factorization in FP64 registers (DiagCol).  Outputs as
 // chol_diag_factor.
-template <typename T>
+template <typename T, bool REP = false>
 __device__ void chol_diag_update_factor(T *S, int c0n, int nbk, int c0, double *dinv, T *Lt, int *bad) {
 	const int lane = threadIdx.x & 31;
 	const int i = lane & 15, h = lane >> 4;
@@ -243,7 +303,17 @@ __device__ void chol_diag_update_factor(T *S, int c0n, int nbk, int c0, double *
 		// real entries of the lower triangle; identity in the padding
 		r[l] = (l <= i && i < nbk && l < nbk) ? s : ((l == i && i >= nbk) ? T(1) : T(0));
 	}
-	DiagCol<0, T>::run(r, lane, nbk, c0n, dinv, bad);
+	if constexpr (REP && sizeof(T) == 4) {
+		if (lane < CHOL_NB) {
+#pragma unroll
+			for (int l = 0; l < CHOL_NB; l++) Lt[lane * 17 + l] = r[l];
+		}
+		__syncwarp();
+		diag_factor_rep<T>(Lt, nbk, c0n, dinv, bad, r, lane);
+		__syncwarp();  // every lane has read the staged block before it is overwritten
+	} else {
+		DiagCol<0, T>::run(r, lane, nbk, c0n, dinv, bad);
+	}
 	chol_diag_store<T>(S, c0n, nbk, dinv, Lt, r, lane);
 }
 
@@ -382,13 +452,15 @@ __device__ __forceinline__ void chol_tile_update(T *S, int ti, int tj, int c0) {
 // blocks of the factor are replaced at the end by their explicit inverses
 // (all blocks in parallel), for the blocked triangular solves; the blocks
 // below the diagonal keep L.
-template <typename T>
+// REP (FP32 only, kernels with registers to spare): the diagonal blocks are
+// factored by diag_factor_rep instead of DiagCol.
+template <typename T, bool REP = false>
 __device__ void chol_smem(T *S, int n, double *dinv, T *Lt, int *bad, bool inv_diag) {
 	const int P = (n + 3) >> 2;
 	const int NB = (n + 15) >> 4;
 	const int tid = threadIdx.x, nt = blockDim.x;
 	const int warp = tid >> 5, lane = tid & 31;
-	if (warp == 0) chol_diag_factor<T>(S, 0, min(CHOL_NB, n), dinv, Lt, bad);
+	if (warp == 0) chol_diag_factor<T, REP>(S, 0, min(CHOL_NB, n), dinv, Lt, bad);
 	__syncthreads();
 	for (int K = 0; K < NB; K++) {
 		const int c0 = 16 * K, k0 = 4 * K;
@@ -402,7 +474,7 @@ __device__ void chol_smem(T *S, int n, double *dinv, T *Lt, int *bad, bool inv_d
 		const int ntiles = R * (R + 1) / 2;
 		const int ndiag = ntiles < 10 ? ntiles : 10;
 		if (warp == 0) {
-			chol_diag_update_factor<T>(S, c0 + CHOL_NB, min(CHOL_NB, n - c0 - CHOL_NB), c0, dinv, Lt, bad);
+			chol_diag_update_factor<T, REP>(S, c0 + CHOL_NB, min(CHOL_NB, n - c0 - CHOL_NB), c0, dinv, Lt, bad);
 		} else if (warp & 3) {
 			// warps 4, 8, ... share warp 0's scheduler (warp w issues from
 			// sub-partition w % 4): they sit the update out so that the serial

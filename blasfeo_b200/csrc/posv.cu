@@ -153,11 +153,28 @@ __device__ void trsv_fwd(const T *S, int n, bool inv_diag, const double *dinv, T
 			if (lane < 16) ybuf[lane] = (lane < nbk) ? v : T(0);
 		}
 		__syncthreads();
-		for (int r = c0 + 16 + tid; r < n; r += nt) {
-			T s = w[r];
+		// rows below the block, one 4-row panel per thread: each column of a
+		// tile comes in one vector load (rows n.. of the last panel hold zeros
+		// below the diagonal and stay zero)
+		const int kb = c0 >> 2, P = (n + 3) >> 2;
+		for (int p = kb + 4 + tid; p < P; p += nt) {
+			T s0 = w[4 * p], s1 = w[4 * p + 1], s2 = w[4 * p + 2], s3 = w[4 * p + 3];
 #pragma unroll
-			for (int l = 0; l < 16; l++) s = fma(-lp_at(S, r, c0 + l), ybuf[l], s);
-			w[r] = s;
+			for (int q = 0; q < 4; q++)
+#pragma unroll
+				for (int c = 0; c < 4; c++) {
+					T a0, a1, a2, a3;
+					tile_col_ld<T>(S, p, kb + q, c, a0, a1, a2, a3);
+					const T y = ybuf[4 * q + c];
+					s0 = fma(-a0, y, s0);
+					s1 = fma(-a1, y, s1);
+					s2 = fma(-a2, y, s2);
+					s3 = fma(-a3, y, s3);
+				}
+			w[4 * p] = s0;
+			w[4 * p + 1] = s1;
+			w[4 * p + 2] = s2;
+			w[4 * p + 3] = s3;
 		}
 		if (tid < nbk) w[c0 + tid] = ybuf[tid];
 		__syncthreads();
@@ -193,11 +210,22 @@ __device__ void trsv_bwd(const T *S, int n, bool inv_diag, const double *dinv, T
 			if (lane < 16) ybuf[lane] = (lane < nbk) ? v : T(0);
 		}
 		__syncthreads();
+		// columns left of the block: for column j the 16 rows of block row K
+		// are column slices of four tiles (one vector load each); the panels
+		// of the block row past the matrix (q with kb + q >= P) are skipped,
+		// rows n.. of the last real panel hold zeros left of the diagonal
+		const int kb = c0 >> 2, P = (n + 3) >> 2;
 		for (int j = tid; j < c0; j += nt) {
 			T s = w[j];
-			for (int k = 0; k < nbk; k++) {
-				const int r = c0 + k;
-				s = fma(-lp_at(S, r, j), ybuf[k], s);
+#pragma unroll
+			for (int q = 0; q < 4; q++) {
+				if (kb + q >= P) break;
+				T a0, a1, a2, a3;
+				tile_col_ld<T>(S, kb + q, j >> 2, j & 3, a0, a1, a2, a3);
+				s = fma(-a0, ybuf[4 * q], s);
+				s = fma(-a1, ybuf[4 * q + 1], s);
+				s = fma(-a2, ybuf[4 * q + 2], s);
+				s = fma(-a3, ybuf[4 * q + 3], s);
 			}
 			w[j] = s;
 		}
@@ -399,7 +427,7 @@ __global__ void __launch_bounds__(NT, MINB) k_posv(int cls, int max_n, PosvWs ws
 		if (MIXED)
 			for (int i = tid; i < nv; i += nt) xs[i] = 0.0;
 		__syncthreads();
-		chol_smem<T>(S, n, dinv, (T *)scratch, s_bad, MIXED);
+		chol_smem<T, (MINB <= 2)>(S, n, dinv, (T *)scratch, s_bad, MIXED);
 
 		if (!MIXED) {
 			trsv_fwd<T>(S, n, false, dinv, w, ybuf);

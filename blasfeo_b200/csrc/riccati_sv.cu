@@ -410,11 +410,13 @@ int blasfeo_dric_gains_batch(int batch, int N, int nx, int nu, struct blasfeo_dm
 
 size_t blasfeo_dsric_sv_worksize(int batch, int N, int nx) {
 	if (batch <= 0 || N < 1 || nx < 1) return 0;
-	const size_t cnx = (size_t)(nx + 3) / 4 * 4;
-	const size_t ba = (RV * cnx + 16) * sizeof(float), rsq = (RV * RV + 16) * sizeof(float);
-	const size_t f32 = (size_t)batch * N * ba + 2 * (size_t)batch * (N + 1) * rsq;
+	// FP32 copies of BAbt and RSQ and the FP32 factors (each slab 256-byte
+	// aligned), then the residual and correction vectors
+	auto r256 = [](size_t x) { return (x + 255) / 256 * 256; };
+	const size_t f32 = r256(blasfeo_memsize_smat_batch(RV, nx, batch * N)) +
+	                   2 * r256(blasfeo_memsize_smat_batch(RV, RV, batch * (N + 1)));
 	const size_t vec = (size_t)batch * (2 * (N + 1) + 2 * N) * RV * sizeof(double);
-	return (f32 + 255) / 256 * 256 + vec + 256;
+	return f32 + vec;
 }
 
 int blasfeo_dsric_sv_batch(int batch, int N, int nx, int nu, struct blasfeo_dmat_batch *sBAbt,
