@@ -427,7 +427,7 @@ __global__ void __launch_bounds__(NT, MINB) k_posv(int cls, int max_n, PosvWs ws
 		if (MIXED)
 			for (int i = tid; i < nv; i += nt) xs[i] = 0.0;
 		__syncthreads();
-		chol_smem<T, (MINB <= 2)>(S, n, dinv, (T *)scratch, s_bad, MIXED);
+		chol_smem<T>(S, n, dinv, (T *)scratch, s_bad, MIXED);
 
 		if (!MIXED) {
 			trsv_fwd<T>(S, n, false, dinv, w, ybuf);
