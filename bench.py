@@ -1118,6 +1118,11 @@ def learned_dispatch(n_ops=1_000_000, train_frac=0.3, seed=5, budget_s=150.0, cp
     t_mlp = sum(float(r["times"].min()) for r in recs[:ntr]) + sum(float(r["times"][p]) for r, p in zip(test, picks))
     out["stream_gflops"] = {"exhaustive": fl / t_best / 1e6, "mlp": fl / t_mlp / 1e6, "rule": fl / t_rule / 1e6,
                             "variant0": fl / t_v0 / 1e6, "total_gflop": fl / 1e9}
+    out["by_op_exhaustive"] = {op_: {"ms": sum(float(r["times"].min()) for r in recs if r["op"] == op_),
+                                     "gflop": sum(r["flops"] for r in recs if r["op"] == op_) / 1e9}
+                               for op_ in at.OPS}
+    for v in out["by_op_exhaustive"].values():
+        v["gflops"] = v["gflop"] / (v["ms"] * 1e-3) if v["ms"] > 0 else None
     if cpu:
         try:
             out["cpu_reference"] = cpu_ops_leg(launches_kept, {r_["op"]: 0 for r_ in recs})

@@ -468,23 +468,37 @@ __device__ void chol_smem(T *S, int n, double *dinv, T *Lt, int *bad, bool inv_d
 		chol_panel_rows<T>(S, c0, c0 + CHOL_NB, 4 * P, tid, nt, Lt);
 		__syncthreads();
 		if (K + 1 >= NB) break;
-		// B. trailing tiles (ti,tj), k0+4 <= tj <= ti < P; the first 10 (the
-		// diagonal block K+1) belong to warp 0, which then factors that block
+		// B. trailing tiles (ti,tj), k0+4 <= tj <= ti < P; the 10 of the
+		// diagonal block K+1 belong to warp 0, which then factors that block
 		const int R = P - (k0 + 4);
-		const int ntiles = R * (R + 1) / 2;
-		const int ndiag = ntiles < 10 ? ntiles : 10;
 		if (warp == 0) {
 			chol_diag_update_factor<T, REP>(S, c0 + CHOL_NB, min(CHOL_NB, n - c0 - CHOL_NB), c0, dinv, Lt, bad);
 		} else if (warp & 3) {
 			// warps 4, 8, ... share warp 0's scheduler (warp w issues from
 			// sub-partition w % 4): they sit the update out so that the serial
 			// diagonal chain keeps its issue slots
-			const int nupd = ((nt >> 5) - ((nt >> 5) + 3) / 4) * 32;
-			const int urank = (warp - (warp >> 2) - 1) * 32 + lane;
-			for (int t = ndiag + urank; t < ntiles; t += nupd) {
-				int ti, tj;
-				tri_index(t, ti, tj);
-				chol_tile_update<T>(S, ti + k0 + 4, tj + k0 + 4, c0);
+			// A warp takes an 8 x 4 block of tiles (8 tile rows, 4 tile columns;
+			// lane l: row l / 4, column l % 4): each tile column slice of the
+			// panel is then read by 4 lanes and each tile row slice by 8 lanes
+			// at once (broadcast), 12 distinct 16-byte loads per 32 tile
+			// updates instead of 33 for 32 tiles of one tile row.  Shared-memory
+			// bandwidth bounds this update, and its traffic also delays the
+			// diagonal warp's loads and shuffles.  Tiles above the diagonal or
+			// past the matrix are skipped; the tiles of block K+1 (rows < 4)
+			// belong to warp 0.
+			const int nuw = (nt >> 5) - ((nt >> 5) + 3) / 4;
+			const int uw = warp - (warp >> 2) - 1;
+			const int scmax = (R + 3) >> 2, sr = (R + 7) >> 3;
+			int si = 0, base = 0, cnt = scmax < 2 ? scmax : 2;
+			for (int sidx = uw;; sidx += nuw) {
+				while (si < sr && sidx >= base + cnt) {
+					base += cnt;
+					si++;
+					cnt = (2 * si + 2 < scmax) ? 2 * si + 2 : scmax;
+				}
+				if (si >= sr) break;
+				const int ti = 8 * si + (lane >> 2), tj = 4 * (sidx - base) + (lane & 3);
+				if (ti < R && ti >= 4 && tj <= ti) chol_tile_update<T>(S, ti + k0 + 4, tj + k0 + 4, c0);
 			}
 		}
 		__syncthreads();

@@ -305,6 +305,177 @@ __global__ void __launch_bounds__(NT) k_getrf(SizeArg sz, MatArg<T> C, MatArg<T>
 	if (info && tid == 0) info[b] = s_bad;
 }
 
+// LU with row pivoting of one instance per CTA whose block stays in global
+// memory (L2), blocked by 16-column panels (the reference's HP driver is
+// blocked too: kernel_dgetrf_pivot panels and kernel_dgemm_nn corrections,
+// blasfeo_hp_pm/d_lapack_lib4.c:2396-3431).  Per panel c0:
+//   a. the panel (rows c0..m-1, 16 columns) is staged in shared memory;
+//   b. it is factored there column by column: pivot = first row of the largest
+//      |a| (kernel/generic/kernel_dgetrf_pivot_lib4.c:84-165), row swap inside
+//      the panel, scaling by the reciprocal pivot (0 for a zero pivot;
+//      getrf_np divides), rank-1 update of the panel's later columns;
+//   c. the panel goes back to global memory;
+//   d. its row swaps are applied, in order, to the columns outside the panel
+//      (one thread per column);
+//   e. U12 = L11^{-1} A12 for the columns right of the panel (one thread per
+//      column, unit lower L11 from shared memory), kept in shared memory;
+//   f. A22 -= L21 U12 as 4 x 4 register tiles (rank-16 update, 4-row tiles of
+//      the panel layout, consecutive threads on consecutive column tiles).
+// Shared memory: (m + 4) x 17 panel plus 16 x (n + 4) U12.
+template <typename T, int NT>
+__global__ void __launch_bounds__(NT) k_getrf_blk(SizeArg sz, MatArg<T> C, MatArg<T> D, int *ipiv,
+                                                   long long ipiv_stride, int *info, int smem_cap, int max_m,
+                                                   bool piv_on) {
+	extern __shared__ __align__(16) unsigned char smem_raw[];
+	__shared__ int s_idx[33];
+	__shared__ T s_val[32];
+	__shared__ int s_bad;
+	__shared__ int s_piv[16];
+	const int b = blockIdx.x;
+	const int m = sz.M(b), n = sz.N(b);
+	if (m <= 0 || n <= 0) return;
+	// instances whose whole block fits the shared-memory kernel are its work
+	const bool fits = (size_t)((m + 3) / 4 * 4) * ((n + 3) / 4 * 4) * sizeof(T) <= (size_t)(smem_cap < 0 ? 0 : smem_cap);
+	if (smem_cap >= 0 && fits) return;
+	const PMat<T> c = C.get(b), d = D.get(b);
+	const int tid = threadIdx.x;
+	int *piv = piv_on ? ipiv + ipiv_stride * b : nullptr;
+	T *P = (T *)smem_raw;                        // panel: row r at P + 17 r
+	T *Us = P + (size_t)(max_m + 4) * 17;        // U12: row k at Us + k * usld
+	const int usld = n + 4;
+	// D = C first (in place afterwards)
+	if (c.p != d.p || c.ri != d.ri || c.cj != d.cj) {
+		for (int e = tid; e < m * n; e += NT) {
+			const int i = e % m, j = e / m;
+			d.at(i, j) = c.at(i, j);
+		}
+	}
+	if (tid == 0) s_bad = 0;
+	__syncthreads();
+	const int mn = m < n ? m : n;
+	for (int c0 = 0; c0 < mn; c0 += 16) {
+		const int w = mn - c0 < 16 ? mn - c0 : 16;
+		const int pr = m - c0;
+		// a. stage the panel
+		for (int e = tid; e < pr * 16; e += NT) {
+			const int r = e >> 4, j = e & 15;
+			P[r * 17 + j] = (j < w) ? d.at(c0 + r, c0 + j) : T(0);
+		}
+		__syncthreads();
+		// b. factor it
+		for (int j = 0; j < w; j++) {
+			int ip = j;
+			if (piv_on) {
+				T best = T(-1);
+				int bi = INT_MAX;
+				for (int r = j + tid; r < pr; r += NT) {
+					const T a = dev_abs(P[r * 17 + j]);
+					if (a > best) {
+						best = a;
+						bi = r;
+					}
+				}
+				ip = block_argmax_first<T>(best, bi, s_idx, s_val);
+				if (ip != j && tid < 16) {
+					const T t = P[j * 17 + tid];
+					P[j * 17 + tid] = P[ip * 17 + tid];
+					P[ip * 17 + tid] = t;
+				}
+			}
+			if (tid == 0) s_piv[j] = c0 + ip;
+			__syncthreads();
+			const T pv = P[j * 17 + j];
+			const T inv = piv_on ? ((pv != T(0)) ? T(1) / pv : T(0)) : T(1) / pv;
+			if (tid == 0) {
+				if (piv_on) piv[c0 + j] = c0 + ip;
+				d.d[c0 + j] = inv;
+				if (pv == T(0) && s_bad == 0) s_bad = c0 + j + 1;
+			}
+			for (int r = j + 1 + tid; r < pr; r += NT) P[r * 17 + j] *= inv;
+			__syncthreads();
+			const int nc = w - j - 1;
+			if (nc > 0) {
+				for (int e = tid; e < (pr - j - 1) * nc; e += NT) {
+					const int r = j + 1 + e / nc, l = j + 1 + e % nc;
+					P[r * 17 + l] = fma(-P[r * 17 + j], P[j * 17 + l], P[r * 17 + l]);
+				}
+			}
+			__syncthreads();
+		}
+		// c. panel back to global memory
+		for (int e = tid; e < pr * w; e += NT) {
+			const int r = e / w, j = e % w;
+			d.at(c0 + r, c0 + j) = P[r * 17 + j];
+		}
+		// d. the panel's row swaps on the other columns, in order
+		if (piv_on) {
+			for (int l = tid; l < n; l += NT) {
+				if (l >= c0 && l < c0 + w) continue;
+				for (int j = 0; j < w; j++) {
+					const int ip = s_piv[j];
+					if (ip != c0 + j) {
+						const T t = d.at(c0 + j, l);
+						d.at(c0 + j, l) = d.at(ip, l);
+						d.at(ip, l) = t;
+					}
+				}
+			}
+		}
+		__syncthreads();
+		// e. U12 = L11^{-1} A12 (unit lower L11)
+		const int nr = n - c0 - w;
+		for (int l = tid; l < nr; l += NT) {
+			T u[16];
+#pragma unroll
+			for (int k = 0; k < 16; k++) u[k] = (k < w) ? d.at(c0 + k, c0 + w + l) : T(0);
+#pragma unroll
+			for (int k = 1; k < 16; k++)
+#pragma unroll
+				for (int kk = 0; kk < k; kk++) u[k] = fma(-P[k * 17 + kk], u[kk], u[k]);
+#pragma unroll
+			for (int k = 0; k < 16; k++) {
+				if (k < w) d.at(c0 + k, c0 + w + l) = u[k];
+				Us[k * usld + l] = (k < w) ? u[k] : T(0);
+			}
+		}
+		__syncthreads();
+		// f. A22 -= L21 U12 (rows c0 + w.., columns c0 + w..)
+		const int rows = pr - w;
+		if (rows > 0 && nr > 0) {
+			const int ntr = (rows + 3) >> 2, ntc = (nr + 3) >> 2;
+			for (int t = tid; t < ntr * ntc; t += NT) {
+				const int ti = t / ntc, tj = t % ntc;
+				const int r0 = w + 4 * ti, l0 = 4 * tj;
+				T acc[4][4];
+#pragma unroll
+				for (int a = 0; a < 4; a++)
+#pragma unroll
+					for (int q = 0; q < 4; q++)
+						acc[a][q] = (r0 + a < pr && l0 + q < nr) ? d.at(c0 + r0 + a, c0 + w + l0 + q) : T(0);
+#pragma unroll
+				for (int k = 0; k < 16; k++) {
+					T av[4], bv[4];
+#pragma unroll
+					for (int a = 0; a < 4; a++) av[a] = (r0 + a < pr) ? P[(r0 + a) * 17 + k] : T(0);
+#pragma unroll
+					for (int q = 0; q < 4; q++) bv[q] = Us[k * usld + l0 + q];
+#pragma unroll
+					for (int a = 0; a < 4; a++)
+#pragma unroll
+						for (int q = 0; q < 4; q++) acc[a][q] = fma(-av[a], bv[q], acc[a][q]);
+				}
+#pragma unroll
+				for (int a = 0; a < 4; a++)
+#pragma unroll
+					for (int q = 0; q < 4; q++)
+						if (r0 + a < pr && l0 + q < nr) d.at(c0 + r0 + a, c0 + w + l0 + q) = acc[a][q];
+			}
+		}
+		__syncthreads();
+	}
+	if (info && tid == 0) info[b] = s_bad;
+}
+
 template <typename T>
 __device__ T block_sum(T v, T *s_red) {
 	const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
@@ -522,6 +693,23 @@ void launch_getrf(int batch, SizeArg sz, int cap, size_t smem, MatArg<T> C, MatA
 	if (smem > 48 * 1024) cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
 	kern<<<batch, NT, smem, s>>>(sz, C, D, ipiv, ipiv_stride, info, cap, piv);
 }
+
+// blocked global-memory LU (k_getrf_blk) for the instances that do not fit
+// shared memory (cap >= 0) or for all of them (cap < 0)
+template <typename T, int NT>
+void launch_getrf_blk(int batch, SizeArg sz, int cap, int max_m, int max_n, MatArg<T> C, MatArg<T> D, int *ipiv,
+                      long long ipiv_stride, int *info, cudaStream_t s, bool piv = true) {
+	auto kern = k_getrf_blk<T, NT>;
+	const size_t smem = ((size_t)(max_m + 4) * 17 + (size_t)16 * (max_n + 4)) * sizeof(T);
+	if (smem > bf::max_smem_optin()) {
+		// panel and U12 beyond shared memory (blocks of more than ~1,500 rows):
+		// the unblocked global-memory kernel
+		launch_getrf<T, 512, false>(batch, sz, cap, 0, C, D, ipiv, ipiv_stride, info, s, piv);
+		return;
+	}
+	if (smem > 48 * 1024) cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+	kern<<<batch, NT, smem, s>>>(sz, C, D, ipiv, ipiv_stride, info, cap, max_m, piv);
+}
 template <typename T, int NT, bool SMEM>
 void launch_geqrf(int batch, SizeArg sz, int cap, size_t smem, MatArg<T> C, MatArg<T> D, cudaStream_t s) {
 	auto kern = k_geqrf<T, NT, SMEM>;
@@ -550,14 +738,15 @@ int getrf_launch(int batch, SizeArg sz, MatArg<T> C, MatArg<T> D, int *ipiv, lon
 	const int cap = (int)smem;
 	variant = pick_lu_variant(variant, max_m, max_n);
 	switch (variant) {
-	case 0: launch_getrf<T, 128, false>(batch, sz, -1, 0, C, D, ipiv, ipiv_stride, info, s, piv); break;
-	case 1: launch_getrf<T, 256, false>(batch, sz, -1, 0, C, D, ipiv, ipiv_stride, info, s, piv); break;
-	case 2: launch_getrf<T, 512, false>(batch, sz, -1, 0, C, D, ipiv, ipiv_stride, info, s, piv); break;
+	case 0: launch_getrf_blk<T, 128>(batch, sz, -1, max_m, max_n, C, D, ipiv, ipiv_stride, info, s, piv); break;
+	case 1: launch_getrf_blk<T, 256>(batch, sz, -1, max_m, max_n, C, D, ipiv, ipiv_stride, info, s, piv); break;
+	case 2: launch_getrf_blk<T, 512>(batch, sz, -1, max_m, max_n, C, D, ipiv, ipiv_stride, info, s, piv); break;
 	case 3: launch_getrf<T, 128, true>(batch, sz, cap, smem, C, D, ipiv, ipiv_stride, info, s, piv); break;
 	case 4: launch_getrf<T, 256, true>(batch, sz, cap, smem, C, D, ipiv, ipiv_stride, info, s, piv); break;
 	default: launch_getrf<T, 512, true>(batch, sz, cap, smem, C, D, ipiv, ipiv_stride, info, s, piv); break;
 	}
-	if (variant >= 3 && need > smem) launch_getrf<T, 512, false>(batch, sz, cap, 0, C, D, ipiv, ipiv_stride, info, s, piv);
+	if (variant >= 3 && need > smem)
+		launch_getrf_blk<T, 256>(batch, sz, cap, max_m, max_n, C, D, ipiv, ipiv_stride, info, s, piv);
 	return bf::check_launch();
 }
 
