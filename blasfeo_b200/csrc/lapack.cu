@@ -567,6 +567,178 @@ __global__ void __launch_bounds__(NT) k_geqrf(SizeArg sz, MatArg<T> C, MatArg<T>
 	}
 }
 
+// Householder QR of one instance per CTA whose block stays in global memory
+// (L2), blocked by 16-column panels with the compact WY form of the panel's
+// reflectors (the reference's HP driver applies 4-column blocks with
+// kernel_dlarf_t_4_lib4, blasfeo_hp_pm/d_lapack_lib4.c:3444 and
+// kernel/generic/kernel_dgeqrf_4_lib4.c:1030).  Per panel c0:
+//   a. the panel (rows c0..m-1, 16 columns) is staged in shared memory;
+//   b. it is factored there column by column with the reflector convention of
+//      dlarfg (kernel/generic/kernel_dgeqrf_4_lib4.c:80-96: beta = -sign(alpha)
+//      ||(alpha, x)||, tau = (beta - alpha) / beta, v = x / (alpha - beta);
+//      tau = 0 when x = 0), each reflector applied to the panel's later columns;
+//   c. panel and tau go back to global memory;
+//   d. T (upper triangular, H_0 H_1 .. H_15 = I - V T V^T) from V^T V:
+//      T_jj = tau_j, T_{0:j,j} = -tau_j T_{0:j,0:j} (V^T v_j)_{0:j};
+//   e. the trailing columns C = A(c0:m, c0+16:n) become Q^T C = C - V T^T (V^T C),
+//      one thread per column, four rows (one panel-layout sector) at a time.
+// Shared memory: (m + 4) x 17 panel, 16 x 17 T and V^T V.
+template <typename T, int NT>
+__global__ void __launch_bounds__(NT) k_geqrf_blk(SizeArg sz, MatArg<T> C, MatArg<T> D, int smem_cap, int max_m) {
+	extern __shared__ __align__(16) unsigned char smem_raw[];
+	__shared__ T s_red[33];
+	__shared__ T s_tau, s_sc, s_beta;
+	__shared__ T Tm[16 * 17];
+	__shared__ T G[16 * 17];
+	const int b = blockIdx.x;
+	const int m = sz.M(b), n = sz.N(b);
+	if (m <= 0 || n <= 0) return;
+	const bool fits = (size_t)((m + 3) / 4 * 4) * ((n + 3) / 4 * 4) * sizeof(T) <= (size_t)(smem_cap < 0 ? 0 : smem_cap);
+	if (smem_cap >= 0 && fits) return;
+	const PMat<T> c = C.get(b), d = D.get(b);
+	T *tau = d.d + d.ri;
+	const int tid = threadIdx.x;
+	const int warp = tid >> 5, lane = tid & 31, nw = NT >> 5;
+	T *P = (T *)smem_raw;  // panel: row r at P + 17 r
+	if (c.p != d.p || c.ri != d.ri || c.cj != d.cj) {
+		for (int e = tid; e < m * n; e += NT) {
+			const int i = e % m, j = e / m;
+			d.at(i, j) = c.at(i, j);
+		}
+	}
+	__syncthreads();
+	const int kmax = m < n ? m : n;
+	for (int c0 = 0; c0 < kmax; c0 += 16) {
+		const int w = kmax - c0 < 16 ? kmax - c0 : 16;
+		const int pr = m - c0;
+		// a. stage the panel
+		for (int e = tid; e < pr * 16; e += NT) {
+			const int r = e >> 4, j = e & 15;
+			P[r * 17 + j] = (j < w) ? d.at(c0 + r, c0 + j) : T(0);
+		}
+		__syncthreads();
+		// b. factor it
+		for (int j = 0; j < w; j++) {
+			T part = T(0);
+			for (int r = j + 1 + tid; r < pr; r += NT) {
+				const T x = P[r * 17 + j];
+				part = fma(x, x, part);
+			}
+			const T sq = block_sum<T>(part, s_red);
+			if (tid == 0) {
+				if (sq == T(0)) {
+					s_tau = T(0);
+					s_sc = T(1);
+					s_beta = P[j * 17 + j];
+				} else {
+					const T alpha = P[j * 17 + j];
+					T beta = sqrt(fma(alpha, alpha, sq));
+					if (alpha > T(0)) beta = -beta;
+					s_tau = (beta - alpha) / beta;
+					s_sc = T(1) / (alpha - beta);
+					s_beta = beta;
+				}
+				tau[c0 + j] = s_tau;
+			}
+			__syncthreads();
+			const T t = s_tau;
+			if (sq != T(0)) {
+				for (int r = j + 1 + tid; r < pr; r += NT) P[r * 17 + j] *= s_sc;
+				if (tid == 0) P[j * 17 + j] = s_beta;
+			}
+			__syncthreads();
+			for (int col = j + 1 + warp; col < w; col += nw) {
+				T wv = T(0);
+				for (int r = j + 1 + lane; r < pr; r += 32) wv = fma(P[r * 17 + j], P[r * 17 + col], wv);
+#pragma unroll
+				for (int off = 16; off > 0; off >>= 1) wv += __shfl_xor_sync(0xffffffffu, wv, off);
+				wv = -t * (wv + P[j * 17 + col]);
+				for (int r = j + 1 + lane; r < pr; r += 32) P[r * 17 + col] = fma(wv, P[r * 17 + j], P[r * 17 + col]);
+				__syncwarp();
+				if (lane == 0) P[j * 17 + col] += wv;
+			}
+			__syncthreads();
+		}
+		// c. panel back to global memory
+		for (int e = tid; e < pr * w; e += NT) {
+			const int r = e / w, j = e % w;
+			d.at(c0 + r, c0 + j) = P[r * 17 + j];
+		}
+		const int nr = n - c0 - w;
+		if (nr > 0) {
+			// d. G = V^T V (strictly upper part), V unit lower trapezoidal in P
+			for (int pq = warp; pq < 16 * 16; pq += nw) {
+				const int k = pq >> 4, j = pq & 15;
+				if (!(k < j && j < w)) continue;
+				T g = T(0);
+				for (int r = j + 1 + lane; r < pr; r += 32) g = fma(P[r * 17 + k], P[r * 17 + j], g);
+#pragma unroll
+				for (int off = 16; off > 0; off >>= 1) g += __shfl_xor_sync(0xffffffffu, g, off);
+				if (lane == 0) G[k * 17 + j] = g + P[j * 17 + k];
+			}
+			__syncthreads();
+			if (tid == 0) {
+				for (int j = 0; j < 16; j++) {
+					const T tj = (j < w) ? tau[c0 + j] : T(0);
+					for (int k = 0; k < j; k++) {
+						T z = T(0);
+						for (int q = k; q < j; q++) z = fma(Tm[k * 17 + q], G[q * 17 + j], z);
+						Tm[k * 17 + j] = -tj * z;
+					}
+					Tm[j * 17 + j] = tj;
+					for (int k = j + 1; k < 16; k++) Tm[k * 17 + j] = T(0);
+				}
+			}
+			__syncthreads();
+			// e. C = C - V T^T (V^T C), one thread per trailing column
+			for (int l = tid; l < nr; l += NT) {
+				const int col = c0 + w + l;
+				T wk[16];
+#pragma unroll
+				for (int k = 0; k < 16; k++) wk[k] = T(0);
+				for (int r0 = 0; r0 < pr; r0 += 4) {
+					T cv[4];
+#pragma unroll
+					for (int a = 0; a < 4; a++) cv[a] = (r0 + a < pr) ? d.at(c0 + r0 + a, col) : T(0);
+#pragma unroll
+					for (int a = 0; a < 4; a++) {
+						const int r = r0 + a;
+#pragma unroll
+						for (int k = 0; k < 16; k++) {
+							// V(r, k): 1 on the diagonal, the stored vector below, 0 above
+							const T v = (r > k) ? P[r * 17 + k] : ((r == k) ? T(1) : T(0));
+							wk[k] = fma(v, cv[a], wk[k]);
+						}
+					}
+				}
+				T wt[16];
+#pragma unroll
+				for (int k = 0; k < 16; k++) {
+					T z = T(0);
+#pragma unroll
+					for (int q = 0; q <= k; q++) z = fma(Tm[q * 17 + k], wk[q], z);
+					wt[k] = z;
+				}
+				for (int r0 = 0; r0 < pr; r0 += 4) {
+#pragma unroll
+					for (int a = 0; a < 4; a++) {
+						const int r = r0 + a;
+						if (r >= pr) break;
+						T cvl = d.at(c0 + r, col);
+#pragma unroll
+						for (int k = 0; k < 16; k++) {
+							const T v = (r > k) ? P[r * 17 + k] : ((r == k) ? T(1) : T(0));
+							cvl = fma(-v, wt[k], cvl);
+						}
+						d.at(c0 + r, col) = cvl;
+					}
+				}
+			}
+		}
+		__syncthreads();
+	}
+}
+
 }  // namespace
 
 namespace {
@@ -717,6 +889,21 @@ void launch_geqrf(int batch, SizeArg sz, int cap, size_t smem, MatArg<T> C, MatA
 	kern<<<batch, NT, smem, s>>>(sz, C, D, cap);
 }
 
+// blocked global-memory QR (k_geqrf_blk) for the instances that do not fit
+// shared memory (cap >= 0) or for all of them (cap < 0)
+template <typename T, int NT>
+void launch_geqrf_blk(int batch, SizeArg sz, int cap, int max_m, MatArg<T> C, MatArg<T> D, cudaStream_t s) {
+	auto kern = k_geqrf_blk<T, NT>;
+	const size_t smem = (size_t)(max_m + 4) * 17 * sizeof(T);
+	if (smem > bf::max_smem_optin()) {
+		// a panel beyond shared memory (more than ~1,500 rows): the unblocked kernel
+		launch_geqrf<T, 512, false>(batch, sz, cap, 0, C, D, s);
+		return;
+	}
+	if (smem > 48 * 1024) cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+	kern<<<batch, NT, smem, s>>>(sz, C, D, cap, max_m);
+}
+
 inline size_t lu_smem_bytes(int max_m, int max_n, size_t esz) {
 	return (size_t)((max_m + 3) / 4 * 4) * ((max_n + 3) / 4 * 4) * esz;
 }
@@ -759,14 +946,14 @@ int geqrf_launch(int batch, SizeArg sz, MatArg<T> C, MatArg<T> D, cudaStream_t s
 	const int cap = (int)smem;
 	variant = pick_lu_variant(variant, max_m, max_n);
 	switch (variant) {
-	case 0: launch_geqrf<T, 128, false>(batch, sz, -1, 0, C, D, s); break;
-	case 1: launch_geqrf<T, 256, false>(batch, sz, -1, 0, C, D, s); break;
-	case 2: launch_geqrf<T, 512, false>(batch, sz, -1, 0, C, D, s); break;
+	case 0: launch_geqrf_blk<T, 128>(batch, sz, -1, max_m, C, D, s); break;
+	case 1: launch_geqrf_blk<T, 256>(batch, sz, -1, max_m, C, D, s); break;
+	case 2: launch_geqrf_blk<T, 512>(batch, sz, -1, max_m, C, D, s); break;
 	case 3: launch_geqrf<T, 128, true>(batch, sz, cap, smem, C, D, s); break;
 	case 4: launch_geqrf<T, 256, true>(batch, sz, cap, smem, C, D, s); break;
 	default: launch_geqrf<T, 512, true>(batch, sz, cap, smem, C, D, s); break;
 	}
-	if (variant >= 3 && need > smem) launch_geqrf<T, 512, false>(batch, sz, cap, 0, C, D, s);
+	if (variant >= 3 && need > smem) launch_geqrf_blk<T, 256>(batch, sz, cap, max_m, C, D, s);
 	return bf::check_launch();
 }
 
