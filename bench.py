@@ -821,11 +821,44 @@ def other_configs(lib, torch, dev, stream, peak_bw, cpu=True):
             out["chain_n16"]["cpu_reference"] = {"error": repr(ex)}
     del slabs, L, X, D
     torch.cuda.empty_cache()
+    try:
+        out["potrf_n16_layouts"] = potrf_layouts(lib, torch, dev, stream, peak_bw, g, tm)
+    except Exception as ex:  # reported, never silently replaced
+        out["potrf_n16_layouts"] = {"error": repr(ex)}
 
     nbt, N, nx, nu = 4096, 30, 12, 4
     out.update(riccati_legs(lib, torch, dev, stream, peak_bw, g, tm, nbt, N, nx, nu, cpu))
     torch.cuda.empty_cache()
     return out
+
+
+def potrf_layouts(lib, torch, dev, stream, peak_bw, g, tm, nb=100000, n=16):
+    """potrf_l of 100,000 SPD 16 x 16 instances (the factor step of the n = 16
+    chain, S = A A^T + 16 I with A 16 x 32 ~ N(0,1)) on the back-to-back slab
+    (blasfeo_dpotrf_l_batch: one warp per instance, FP64 tensor cores) and on the
+    batch-interleaved slab (blasfeo_dpotrf_l_batch_il: a lane pair per instance);
+    algorithmic bytes = lower triangle in and out plus the inverse diagonal."""
+    from blasfeo_b200.api import DMatBatch, DMatBatchIL
+    from blasfeo_b200.workloads import fill_batch
+    A = torch.randn((nb, n, 2 * n), generator=g, dtype=torch.float64, device=dev)
+    S = A @ A.transpose(1, 2) + n * torch.eye(n, dtype=torch.float64, device=dev)
+    C0, D0 = DMatBatch(n, n, nb), DMatBatch(n, n, nb)
+    fill_batch(C0, S)
+    Ci, Di = DMatBatchIL(n, n, nb).from_batch(C0), DMatBatchIL(n, n, nb)
+    sh = C.c_void_p(stream.cuda_stream)
+    ms_b = tm(lambda: lib.blasfeo_dpotrf_l_batch(nb, n, C0.ref, 0, 0, D0.ref, 0, 0, None, sh))
+    ms_i = tm(lambda: lib.blasfeo_dpotrf_l_batch_il(nb, n, Ci.ref, Di.ref, None, sh))
+    out = DMatBatch(n, n, nb)
+    Di.to_batch(out)
+    torch.cuda.synchronize()
+    a_, b_ = np.tril(out.unpack_all()), np.tril(D0.unpack_all())
+    by = (2 * n * (n + 1) / 2 + n) * 8 * nb
+    res = {"instances": nb}
+    for name, ms in (("back_to_back", ms_b), ("interleaved", ms_i)):
+        res[name] = {"ms": ms, "instances_per_s": nb / ms * 1e3, "gbs": by / ms / 1e6, "frac_of_hbm": by / ms / 1e6 / peak_bw}
+    res["winner"] = "interleaved" if ms_i < ms_b else "back_to_back"
+    res["relfro_between_layouts"] = float(np.linalg.norm(a_ - b_) / np.linalg.norm(b_))
+    return res
 
 
 def riccati_legs(lib, torch, dev, stream, peak_bw, g, tm, nbt, N, nx, nu, cpu):

@@ -63,6 +63,12 @@ class smat_batch(dmat_batch):
     pass
 
 
+class dmat_batch_il(C.Structure):
+    """struct blasfeo_dmat_batch_il (batch-interleaved slab)."""
+    _fields_ = [("mem", C.c_void_p), ("m", C.c_int), ("n", C.c_int), ("pm", C.c_int), ("cn", C.c_int),
+                ("batch", C.c_int), ("il", C.c_int), ("gstride", C.c_longlong), ("memsize", C.c_size_t)]
+
+
 class cm_dmat(C.Structure):
     """struct blasfeo_cm_dmat (include/blasfeo_common.h:220-229 layout): pA is
     column-major with leading dimension m."""
@@ -198,6 +204,12 @@ _sig("blasfeo_b200_mlp_forward", _i, _i, _i, _vp, _i, _vp, _vp, _vp, _vp)
 _sig("blasfeo_b200_mlp_grad", _i, _i, _i, _vp, _i, _vp, _vp, _vp, _vp, _vp, _vp)
 _sig("blasfeo_b200_mlp_adam", _i, _i, _vp, _vp, _vp, _vp, _i, _f, _vp)
 _sig("blasfeo_b200_cost_model_nfeat", _i)
+_IL = P(dmat_batch_il)
+_sig("blasfeo_memsize_dmat_batch_il", _sz, _i, _i, _i)
+_sig("blasfeo_create_dmat_batch_il", None, _i, _i, _i, _IL, _vp)
+_sig("blasfeo_dmat_batch_to_il", _i, _DB, _IL, _vp)
+_sig("blasfeo_dmat_batch_from_il", _i, _IL, _DB, _vp)
+_sig("blasfeo_dpotrf_l_batch_il", _i, _i, _i, _IL, _IL, _vp, _vp)
 _sig("blasfeo_b200_set_cost_model", _i, _i, _i, _vp)
 _sig("blasfeo_b200_clear_cost_model", None)
 _sig("blasfeo_b200_dispatch_pick", _i, _i, _i, _vp, _vp, _vp, _i, _i, _i, _vp)

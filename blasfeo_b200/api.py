@@ -15,10 +15,10 @@ import ctypes as C
 
 import numpy as np
 
-from . import lib, dmat, smat, dvec, svec, dmat_batch, smat_batch, cm_dmat, cm_smat, check
+from . import lib, dmat, smat, dvec, svec, dmat_batch, smat_batch, dmat_batch_il, cm_dmat, cm_smat, check
 
 __all__ = [
-    "DMat", "SMat", "DVec", "SVec", "DMatBatch", "SMatBatch", "device_buffer", "set_stream", "set_sync",
+    "DMat", "SMat", "DVec", "SVec", "DMatBatch", "SMatBatch", "DMatBatchIL", "device_buffer", "set_stream", "set_sync",
     "set_posv_engine", "POSV_DEFAULT", "POSV_SIMT", "POSV_TENSOR",
     "blasfeo_dgemm_nt", "blasfeo_dsyrk_ln", "blasfeo_dtrsm_rltn", "blasfeo_dtrmm_rlnn", "blasfeo_dpotrf_l",
     "blasfeo_dsyrk_dpotrf_ln", "blasfeo_dgetrf_rp", "blasfeo_dgeqrf", "blasfeo_dgeqrf_worksize",
@@ -225,6 +225,30 @@ class SMatBatch(_MatBatch):
     _np = np.float32
     _desc = smat_batch
     _inst = SMat
+
+
+class DMatBatchIL:
+    """A batch-interleaved slab (struct blasfeo_dmat_batch_il): element slot e
+    of instance b at mem[(b // 16) * gstride + 16 e + b % 16]."""
+
+    def __init__(self, m, n, batch):
+        self.m, self.n, self.batch = m, n, batch
+        nbytes = lib.blasfeo_memsize_dmat_batch_il(m, n, batch)
+        self.buf = device_buffer(nbytes)
+        self.s = dmat_batch_il()
+        lib.blasfeo_create_dmat_batch_il(m, n, batch, C.byref(self.s), C.c_void_p(self.buf.data_ptr()))
+
+    @property
+    def ref(self):
+        return C.byref(self.s)
+
+    def from_batch(self, B, stream=None):
+        check(lib.blasfeo_dmat_batch_to_il(B.ref, self.ref, stream))
+        return self
+
+    def to_batch(self, B, stream=None):
+        check(lib.blasfeo_dmat_batch_from_il(self.ref, B.ref, stream))
+        return B
 
 
 def descriptor_array(mats):

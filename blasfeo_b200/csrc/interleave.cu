@@ -1,0 +1,232 @@
+// Batch-interleaved panel layout for uniform batches of small matrices.
+//
+// The instances of a batch are taken in groups of IL = 16.  Inside a group
+// every element slot of the lib4 panel layout (include/blasfeo_common.h:112:
+// element (i,j) at e = (i - i%4)*cn + 4j + i%4, then the inverse diagonal at
+// e = pm*cn + k) holds the IL instances' values side by side:
+//   value of instance b at mem[(b / IL) * gstride + e * IL + b % IL],
+// gstride = IL * (pm*cn + dA slots), the slab rounded to 64 bytes per group.
+// Kernels that give instance b to lanes of one warp then read one element of
+// 16 instances as one contiguous 128-byte (FP64) run, whatever the element:
+// every load is coalesced and vectorisable, with no staging in shared memory.
+// The back-to-back slab (struct blasfeo_dmat_batch) keeps each instance
+// contiguous instead, which suits kernels that give an instance to a warp and
+// move it with one bulk copy.
+//
+// Here: layout, conversions from and to the back-to-back slab, and the
+// Cholesky factorization (potrf_l, the reference's blasfeo_dpotrf_l,
+// blasfeo_hp_pm/d_lapack_lib4.c:918) with a lane pair per instance for
+// n <= 16: the pair holds the lower triangle in FP64 registers, even rows on
+// one lane and odd rows on the other (at most 72 doubles each), pivots by the
+// reference's rule (kernel/generic/kernel_dgemm_4x4_lib4.c:5700-5710: c > 0 ->
+// sqrt(c) and its reciprocal, else 0 and 0), the column of each pivot passed
+// to the partner by shuffles.  16 instances per warp.
+#include "common.cuh"
+
+namespace {
+
+constexpr int IL = 16;
+
+struct IlGeom {
+	int pm, cn, dl;
+	long long slots, gstride;
+};
+
+__host__ __device__ inline IlGeom il_geom(int m, int n) {
+	IlGeom g;
+	g.pm = (m + 3) / 4 * 4;
+	g.cn = (n + 3) / 4 * 4;
+	const int mn = m < n ? m : n;
+	g.dl = (mn + 15) / 16 * 16;
+	g.slots = (long long)g.pm * g.cn + g.dl;
+	g.gstride = (g.slots * IL + 7) / 8 * 8;  // 64-byte aligned groups (FP64)
+	return g;
+}
+
+__device__ __forceinline__ long long pm_el(int i, int j, int cn) { return (long long)(i & ~3) * cn + 4 * j + (i & 3); }
+
+// back-to-back slab <-> interleaved: one thread per (instance, slot), the
+// interleaved side written / read in runs of IL consecutive instances
+__global__ void k_to_il(long long total, int slots, const double *__restrict__ src, long long sstride,
+                        double *__restrict__ dst, long long gstride) {
+	for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < total;
+	     t += (long long)gridDim.x * blockDim.x) {
+		const long long g = t / ((long long)slots * IL);
+		const long long r = t % ((long long)slots * IL);
+		const int e = (int)(r / IL), l = (int)(r % IL);
+		const long long b = g * IL + l;
+		dst[g * gstride + r] = src[b * sstride + e];
+	}
+}
+__global__ void k_from_il(long long total, int slots, const double *__restrict__ src, long long gstride,
+                          double *__restrict__ dst, long long dstride) {
+	for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < total;
+	     t += (long long)gridDim.x * blockDim.x) {
+		const long long g = t / ((long long)slots * IL);
+		const long long r = t % ((long long)slots * IL);
+		const int e = (int)(r / IL), l = (int)(r % IL);
+		const long long b = g * IL + l;
+		dst[b * dstride + e] = src[g * gstride + r];
+	}
+}
+
+// One pivot column J of the pair Cholesky (recursive template: every index
+// into a[][] is a compile-time constant, so a[][] stays in registers).
+// Lane parity h owns rows i = 2r + h; a[r][j] = L(2r + h, j) for j <= 2r + 1.
+template <int J>
+struct IlCol {
+	static __device__ __forceinline__ void run(double (&a)[8][16], int h, int n, bool act, double *dinv, int &bad) {
+		constexpr int PR = J >> 1;
+		const double mine = (h == (J & 1)) ? a[PR][J] : 0.0;
+		const double other = __shfl_xor_sync(0xffffffffu, mine, 1);
+		const double c = (h == (J & 1)) ? mine : other;
+		const bool ok = c > 0.0;
+		const double inv = ok ? rsqrt(c) : 0.0;
+		if (!ok && J < n && bad == 0) bad = J + 1;
+		if (h == (J & 1)) {
+			a[PR][J] = ok ? c * inv : 0.0;
+			if (act && J < n) dinv[J * IL] = inv;
+		}
+#pragma unroll
+		for (int r = 0; r < 8; r++)
+			if (J <= 2 * r + 1 && 2 * r + h > J) a[r][J] *= inv;
+#pragma unroll
+		for (int l = J + 1; l < 16; l++) {
+			const double own = (h == (l & 1)) ? a[l >> 1][J] : 0.0;
+			const double oth = __shfl_xor_sync(0xffffffffu, own, 1);
+			const double llj = (h == (l & 1)) ? own : oth;
+#pragma unroll
+			for (int r = 0; r < 8; r++)
+				if (l <= 2 * r + 1 && 2 * r + h >= l) a[r][l] = fma(-a[r][J], llj, a[r][l]);
+		}
+		IlCol<J + 1>::run(a, h, n, act, dinv, bad);
+	}
+};
+template <>
+struct IlCol<16> {
+	static __device__ __forceinline__ void run(double (&)[8][16], int, int, bool, double *, int &) {}
+};
+
+// Cholesky of n <= 16 per lane pair: lane 2t + h of a warp takes rows 2r + h
+// of instance 16 * (global warp) + t.
+__global__ void __launch_bounds__(256) k_dpotrf_il(int batch, int n, const double *__restrict__ C, double *D,
+                                                   long long gstride, int cn, int pmcn, int *info) {
+	const int lane = threadIdx.x & 31;
+	const int t = lane >> 1, h = lane & 1;
+	const long long gw = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+	const long long b = gw * IL + t;
+	const bool act = b < batch;
+	const double *cg = C + gw * gstride + t;
+	double *dg = D + gw * gstride + t;
+	double a[8][16];
+#pragma unroll
+	for (int r = 0; r < 8; r++)
+#pragma unroll
+		for (int j = 0; j < 16; j++) {
+			const int i = 2 * r + h;
+			double v = 0.0;
+			if (j <= 2 * r + 1) {
+				if (act && i < n && j < n && j <= i)
+					v = cg[pm_el(i, j, cn) * IL];
+				else if (i == j)
+					v = 1.0;  // padding rows and columns factor to the identity
+			}
+			a[r][j] = v;
+		}
+	int bad = 0;
+	IlCol<0>::run(a, h, n, act, dg + (long long)pmcn * IL, bad);
+	if (act) {
+#pragma unroll
+		for (int r = 0; r < 8; r++)
+#pragma unroll
+			for (int j = 0; j < 16; j++) {
+				const int i = 2 * r + h;
+				if (j <= 2 * r + 1 && i < n && j <= i) dg[pm_el(i, j, cn) * IL] = a[r][j];
+			}
+		if (h == 0 && info) info[b] = bad;
+	}
+}
+
+inline int grid_for(long long total, int threads) {
+	long long g = (total + threads - 1) / threads;
+	const long long cap = (long long)bf::num_sms() * 16;
+	return (int)(g < 1 ? 1 : (g > cap ? cap : g));
+}
+
+}  // namespace
+
+extern "C" {
+
+size_t blasfeo_memsize_dmat_batch_il(int m, int n, int batch) {
+	if (m <= 0 || n <= 0 || batch <= 0) return 0;
+	const IlGeom g = il_geom(m, n);
+	return (size_t)((batch + IL - 1) / IL) * (size_t)g.gstride * sizeof(double);
+}
+
+void blasfeo_create_dmat_batch_il(int m, int n, int batch, struct blasfeo_dmat_batch_il *sA, void *memory) {
+	const IlGeom g = il_geom(m, n);
+	sA->mem = (double *)memory;
+	sA->m = m;
+	sA->n = n;
+	sA->pm = g.pm;
+	sA->cn = g.cn;
+	sA->batch = batch;
+	sA->il = IL;
+	sA->gstride = g.gstride;
+	sA->memsize = blasfeo_memsize_dmat_batch_il(m, n, batch);
+}
+
+int blasfeo_dmat_batch_to_il(const struct blasfeo_dmat_batch *src, struct blasfeo_dmat_batch_il *dst, void *stream) {
+	if (!src || !dst || !src->mem || !dst->mem || src->m != dst->m || src->n != dst->n || src->batch < dst->batch)
+		return BLASFEO_B200_EINVAL;
+	if (dst->batch == 0) return BLASFEO_B200_OK;
+	const IlGeom g = il_geom(dst->m, dst->n);
+	// whole groups by the kernel, a partial last group instance by instance
+	// (the slots of its missing instances are left as they are)
+	const long long total = (long long)((dst->batch + IL - 1) / IL) * g.slots * IL;
+	const long long full = (long long)(dst->batch / IL) * g.slots * IL;
+	if (full > 0)
+		k_to_il<<<grid_for(full, 256), 256, 0, (cudaStream_t)stream>>>(full, (int)g.slots, src->pA, src->stride,
+		                                                               dst->mem, dst->gstride);
+	if (total > full) {
+		for (int b = (int)(dst->batch / IL) * IL; b < dst->batch; b++)
+			cudaMemcpy2DAsync(dst->mem + (long long)(b / IL) * dst->gstride + b % IL, IL * sizeof(double),
+			                  src->pA + (long long)b * src->stride, sizeof(double), sizeof(double), g.slots,
+			                  cudaMemcpyDeviceToDevice, (cudaStream_t)stream);
+	}
+	return bf::check_launch();
+}
+
+int blasfeo_dmat_batch_from_il(const struct blasfeo_dmat_batch_il *src, struct blasfeo_dmat_batch *dst, void *stream) {
+	if (!src || !dst || !src->mem || !dst->mem || src->m != dst->m || src->n != dst->n || dst->batch < src->batch)
+		return BLASFEO_B200_EINVAL;
+	if (src->batch == 0) return BLASFEO_B200_OK;
+	const IlGeom g = il_geom(src->m, src->n);
+	const long long full = (long long)(src->batch / IL) * g.slots * IL;
+	if (full > 0)
+		k_from_il<<<grid_for(full, 256), 256, 0, (cudaStream_t)stream>>>(full, (int)g.slots, src->mem, src->gstride,
+		                                                                 dst->pA, dst->stride);
+	for (int b = (int)(src->batch / IL) * IL; b < src->batch; b++)
+		cudaMemcpy2DAsync(dst->pA + (long long)b * dst->stride, sizeof(double),
+		                  src->mem + (long long)(b / IL) * src->gstride + b % IL, IL * sizeof(double),
+		                  sizeof(double), g.slots, cudaMemcpyDeviceToDevice, (cudaStream_t)stream);
+	return bf::check_launch();
+}
+
+int blasfeo_dpotrf_l_batch_il(int batch, int m, struct blasfeo_dmat_batch_il *sC, struct blasfeo_dmat_batch_il *sD,
+                              int *info, void *stream) {
+	if (batch < 0 || m < 0 || !sC || !sD || !sC->mem || !sD->mem) return BLASFEO_B200_EINVAL;
+	if (batch == 0 || m == 0) return BLASFEO_B200_OK;
+	if (m > 16) return BLASFEO_B200_ENOTSUP;
+	if (sC->m < m || sC->n < m || sD->m < m || sD->n < m || sC->batch < batch || sD->batch < batch ||
+	    sC->pm != sD->pm || sC->cn != sD->cn || sC->gstride != sD->gstride)
+		return BLASFEO_B200_EINVAL;
+	const long long warps = (batch + IL - 1) / IL;
+	const int threads = 256;
+	const long long blocks = (warps * 32 + threads - 1) / threads;
+	k_dpotrf_il<<<(unsigned)blocks, threads, 0, (cudaStream_t)stream>>>(batch, m, sC->mem, sD->mem, sC->gstride,
+	                                                                     sC->cn, sC->pm * sC->cn, info);
+	return bf::check_launch();
+}
+
+}  // extern "C"

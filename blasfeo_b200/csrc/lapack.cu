@@ -908,10 +908,19 @@ inline size_t lu_smem_bytes(int max_m, int max_n, size_t esz) {
 	return (size_t)((max_m + 3) / 4 * 4) * ((max_n + 3) / 4 * 4) * esz;
 }
 
-inline int pick_lu_variant(int variant, int max_m, int max_n) {
+// built-in rule for getrf (qr = false) and geqrf (qr = true), from uniform
+// batches timed on the B200 at n = 32..384: the shared-memory kernel with 128
+// threads for small blocks, the blocked global-memory kernels above (128,
+// 256 or 512 threads by size)
+inline int pick_lu_variant(int variant, int max_m, int max_n, bool qr = false) {
 	if (variant < 0) {
 		const int mx = max_m > max_n ? max_m : max_n;
-		variant = mx <= 64 ? 3 : (mx <= 160 ? 4 : 5);
+		if (mx <= 48)
+			variant = 3;
+		else if (!qr)
+			variant = mx <= 192 ? 0 : 1;
+		else
+			variant = mx <= 128 ? 0 : (mx <= 256 ? 1 : 2);
 	}
 	return variant;
 }
@@ -944,7 +953,7 @@ int geqrf_launch(int batch, SizeArg sz, MatArg<T> C, MatArg<T> D, cudaStream_t s
 	const size_t need = lu_smem_bytes(max_m, max_n, sizeof(T));
 	const size_t smem = need < cap_full ? need : cap_full;
 	const int cap = (int)smem;
-	variant = pick_lu_variant(variant, max_m, max_n);
+	variant = pick_lu_variant(variant, max_m, max_n, true);
 	switch (variant) {
 	case 0: launch_geqrf_blk<T, 128>(batch, sz, -1, max_m, C, D, s); break;
 	case 1: launch_geqrf_blk<T, 256>(batch, sz, -1, max_m, C, D, s); break;

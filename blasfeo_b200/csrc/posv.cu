@@ -422,7 +422,11 @@ __global__ void __launch_bounds__(NT, MINB) k_posv(int cls, int max_n, PosvWs ws
 
 		// lower triangle -> lower panels (converted to T), identity padding; the
 		// mixed path with refinement slots also keeps an FP64 copy there
-		load_lp_vec<T, double, 2>(S, n, a.p, a.cn, MIXED ? slot : nullptr);
+		// one CTA per SM (the largest classes) keeps more loads in flight per thread
+		if (MINB <= 2)
+			load_lp_vec<T, double, 4>(S, n, a.p, a.cn, MIXED ? slot : nullptr);
+		else
+			load_lp_vec<T, double, 2>(S, n, a.p, a.cn, MIXED ? slot : nullptr);
 		for (int i = tid; i < nv; i += nt) w[i] = (i < n) ? (T)bg[i] : T(0);
 		if (MIXED)
 			for (int i = tid; i < nv; i += nt) xs[i] = 0.0;

@@ -85,6 +85,20 @@ struct blasfeo_smat_batch {
 	size_t memsize;
 };
 
+/* batch-interleaved uniform batch (no reference counterpart): instances in
+ * groups of il (16); element slot e of the panel layout (element (i,j) at
+ * e = (i - i%4)*cn + 4*j + i%4, then the inverse diagonal at e = pm*cn + k)
+ * of instance b at mem[(b / il) * gstride + e * il + b % il], so one element of
+ * 16 consecutive instances is one contiguous 128-byte run. */
+struct blasfeo_dmat_batch_il {
+	double *mem;
+	int m, n, pm, cn;
+	int batch;
+	int il;
+	long long gstride;  /* elements per group of il instances */
+	size_t memsize;     /* bytes of the whole slab */
+};
+
 /* column-major descriptors, include/blasfeo_common.h:220-229 (same fields and
  * order): pA is a column-major array in DEVICE memory whose leading dimension
  * is m, element (i,j) at pA[i + j*m] (the reference's BLAS API sets m = lda). */
@@ -274,6 +288,20 @@ void blasfeo_dtrsv_ltn(int m, struct blasfeo_dmat *sA, int ai, int aj, struct bl
 size_t blasfeo_memsize_dmat_batch(int m, int n, int batch);
 void blasfeo_create_dmat_batch(int m, int n, int batch, struct blasfeo_dmat_batch *sA, void *memory);
 void blasfeo_dmat_batch_instance(struct blasfeo_dmat_batch *sA, int b, struct blasfeo_dmat *out);
+/* batch-interleaved slabs (no reference counterpart): size, creation, and
+ * conversion from / to the back-to-back slab of the same m x n (on `stream`;
+ * EINVAL for mismatched sizes or a source with fewer instances). */
+size_t blasfeo_memsize_dmat_batch_il(int m, int n, int batch);
+void blasfeo_create_dmat_batch_il(int m, int n, int batch, struct blasfeo_dmat_batch_il *sA, void *memory);
+int blasfeo_dmat_batch_to_il(const struct blasfeo_dmat_batch *src, struct blasfeo_dmat_batch_il *dst, void *stream);
+int blasfeo_dmat_batch_from_il(const struct blasfeo_dmat_batch_il *src, struct blasfeo_dmat_batch *dst, void *stream);
+/* potrf_l (include/blasfeo_d_blasfeo_api.h:280, one instance per lane pair)
+ * on interleaved slabs of equal geometry, m <= 16 (else ENOTSUP): the m x m
+ * lower factor of each instance of sC into sD with the inverse diagonal in its
+ * dA slots; info[b] as for blasfeo_dpotrf_l_batch. */
+int blasfeo_dpotrf_l_batch_il(int batch, int m, struct blasfeo_dmat_batch_il *sC, struct blasfeo_dmat_batch_il *sD,
+	int *info, void *stream);
+
 /* Host column-major batch <-> uniform-batch slab (no reference counterpart;
  * the batched form of blasfeo_pack_dmat / blasfeo_unpack_dmat): instance b of
  * the host array starts at A + b*strideA (ld lda) and maps to the m x n block
