@@ -296,12 +296,62 @@ __global__ void __launch_bounds__(64 * TPR) k_trsm_rltn_blk(SizeArg sz, T alpha,
 	}
 }
 
+// Few rows (a single instance of config-1 size): one warp per row of D, 8
+// rows per CTA, so the rows' serial chains run on several SMs at once.  A's
+// lower triangle and inverse diagonal are staged in shared memory per CTA;
+// lane l holds the columns k = 2l, 2l + 1 of its row in registers; step j:
+// the owner lane finishes d_ij, a shuffle hands it to the warp, every lane
+// updates its columns k > j (same operations in the same order as
+// k_trsm_rltn_reg).  n <= 64.
+template <typename T, bool UNIT>
+__global__ void __launch_bounds__(256) k_trsm_rltn_row(SizeArg sz, T alpha, MatArg<T> A, MatArg<T> B, MatArg<T> D) {
+	__shared__ T sa[64 * 64];  // sa[j * 64 + k] = a(k, j), k > j
+	__shared__ T sinv[64];
+	const int b = blockIdx.x;
+	const int m = sz.M(b), n = sz.N(b);
+	const PMat<T> a = A.get(b), bb = B.get(b), d = D.get(b);
+	for (int e = threadIdx.x; e < 64 * 64; e += blockDim.x) {
+		const int k = e & 63, j = e >> 6;
+		if (j < n && k < n && k > j) sa[j * 64 + k] = a.at(k, j);
+	}
+	if (!UNIT && threadIdx.x < n) sinv[threadIdx.x] = a.d[threadIdx.x];
+	__syncthreads();
+	const int lane = threadIdx.x & 31;
+	const int i = blockIdx.y * 8 + (threadIdx.x >> 5);
+	if (i >= m) return;  // whole warps leave
+	T c0 = (2 * lane < n) ? alpha * bb.at(i, 2 * lane) : T(0);
+	T c1 = (2 * lane + 1 < n) ? alpha * bb.at(i, 2 * lane + 1) : T(0);
+	for (int j = 0; j < n; j++) {
+		const int owner = j >> 1;
+		T dj = T(0);
+		if (lane == owner) {
+			const T cj = (j & 1) ? c1 : c0;
+			dj = UNIT ? cj : cj * sinv[j];
+			if (j & 1)
+				c1 = dj;
+			else
+				c0 = dj;
+		}
+		dj = __shfl_sync(0xffffffffu, dj, owner);
+		const int k0 = 2 * lane, k1 = 2 * lane + 1;
+		if (k0 > j && k0 < n) c0 = fma(-dj, sa[j * 64 + k0], c0);
+		if (k1 > j && k1 < n) c1 = fma(-dj, sa[j * 64 + k1], c1);
+	}
+	if (2 * lane < n) d.at(i, 2 * lane) = c0;
+	if (2 * lane + 1 < n) d.at(i, 2 * lane + 1) = c1;
+}
+
 template <typename T, bool UNIT>
 void trsm_rltn_kernel(int batch, SizeArg sz, int m, int n, T alpha, MatArg<T> A, MatArg<T> B, MatArg<T> D,
                       cudaStream_t s) {
 	const dim3 grid(batch, cdiv(m, 64));
 	// a row of 64 doubles takes two threads (registers); everything else one
 	constexpr int TPR64 = sizeof(T) == 8 ? 2 : 1;
+	if (n <= 64 && (long long)batch * cdiv(m, 64) * 4 <= bf::num_sms()) {
+		// too few CTAs to fill the GPU with the 64-row kernel: a warp per row
+		k_trsm_rltn_row<T, UNIT><<<dim3(batch, cdiv(m, 8)), 256, 0, s>>>(sz, alpha, A, B, D);
+		return;
+	}
 	if (n <= 16)
 		k_trsm_rltn_reg<T, UNIT, 16, 1><<<grid, 64, 0, s>>>(sz, alpha, A, B, D);
 	else if (n <= 32)
