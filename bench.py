@@ -137,6 +137,53 @@ def run_case(argv):
             bf.check(lib.blasfeo_dric_trf_batch(batch, N, nx, nu, sBA.ref, sRSQ.ref, sL.ref, P(info), None))
         torch.cuda.synchronize()
         assert bool((info == 0).all().item())
+    elif op == "cfg3":
+        # the headline call on `batch` systems of the benchmark's distribution
+        from blasfeo_b200.workloads import SpdBatch
+        W = SpdBatch(*gen_config3(batch, 1000, "cuda"))
+        info = torch.zeros(batch, dtype=torch.int32, device=dev)
+        for _ in range(reps):
+            bf.check(lib.blasfeo_dsposv_l_vbatch(batch, P(W.nvec), W.max_n, P(W.desc), P(W.bdesc), P(W.xdesc), 30,
+                                                 1e-12, None, None, P(info), None, 0, None))
+        torch.cuda.synchronize()
+        assert bool((info == 0).all().item())
+    elif op in ("getrf", "geqrf"):
+        A, D = bf.DMatBatch(n, n, batch), bf.DMatBatch(n, n, batch)
+        fill_batch(A, torch.rand((batch, n, n), dtype=torch.float64, device=dev) * 2 - 1)
+        ipiv = torch.zeros(batch * n, dtype=torch.int32, device=dev)
+        for _ in range(reps):
+            if op == "getrf":
+                bf.check(lib.blasfeo_dgetrf_rp_batch(batch, n, n, A.ref, 0, 0, D.ref, 0, 0, P(ipiv), None, None))
+            else:
+                bf.check(lib.blasfeo_dgeqrf_batch(batch, n, n, A.ref, 0, 0, D.ref, 0, 0, None))
+    elif op in ("chain", "chain_il"):
+        from blasfeo_b200.api import DMatBatchIL
+        g = torch.Generator(device=dev)
+        g.manual_seed(2)
+        sl = {}
+        for name, (r, c) in (("A", (16, 32)), ("R", (16, 16)), ("C", (16, 16)), ("G", (16, 16))):
+            sl[name] = bf.DMatBatch(r, c, batch)
+            fill_batch(sl[name], torch.randn((batch, r, c), generator=g, dtype=torch.float64, device=dev))
+        outs = [bf.DMatBatch(16, 16, batch) for _ in range(3)]
+        info = torch.zeros(batch, dtype=torch.int32, device=dev)
+        if op == "chain_il":
+            sl = {k: DMatBatchIL(v.m, v.n, batch).from_batch(v) for k, v in sl.items()}
+            outs = [DMatBatchIL(16, 16, batch) for _ in range(3)]
+            f = lib.blasfeo_dsyrk_dpotrf_dtrsm_dgemm_batch_il
+        else:
+            f = lib.blasfeo_dsyrk_dpotrf_dtrsm_dgemm_batch
+        for _ in range(reps):
+            bf.check(f(batch, 16, 32, 16.0, *(sl[k].ref for k in "ARCG"), *(o.ref for o in outs), P(info), None))
+        torch.cuda.synchronize()
+        assert bool((info == 0).all().item())
+    elif op == "potrf_il":
+        from blasfeo_b200.api import DMatBatchIL
+        A = torch.randn((batch, n, 2 * n), dtype=torch.float64, device=dev)
+        Cm = bf.DMatBatch(n, n, batch)
+        fill_batch(Cm, A @ A.transpose(1, 2) + n * torch.eye(n, dtype=torch.float64, device=dev))
+        Ci, Di = DMatBatchIL(n, n, batch).from_batch(Cm), DMatBatchIL(n, n, batch)
+        for _ in range(reps):
+            bf.check(lib.blasfeo_dpotrf_l_batch_il(batch, n, Ci.ref, Di.ref, None, None))
     else:
         raise SystemExit("unknown case %r" % op)
     torch.cuda.synchronize()
@@ -819,6 +866,10 @@ def other_configs(lib, torch, dev, stream, peak_bw, cpu=True):
             out["chain_n16"]["cpu_reference"] = cpu_chain_leg(nb, slabs, L, X, D)
         except Exception as ex:  # reported, never silently replaced
             out["chain_n16"]["cpu_reference"] = {"error": repr(ex)}
+    try:
+        out["chain_n16"]["interleaved"] = chain_interleaved(lib, torch, stream, peak_bw, tm, nb, slabs, L, X, D, ms)
+    except Exception as ex:  # reported, never silently replaced
+        out["chain_n16"]["interleaved"] = {"error": repr(ex)}
     del slabs, L, X, D
     torch.cuda.empty_cache()
     try:
@@ -830,6 +881,35 @@ def other_configs(lib, torch, dev, stream, peak_bw, cpu=True):
     out.update(riccati_legs(lib, torch, dev, stream, peak_bw, g, tm, nbt, N, nx, nu, cpu))
     torch.cuda.empty_cache()
     return out
+
+
+def chain_interleaved(lib, torch, stream, peak_bw, tm, nb, slabs, L, X, D, ms_b2b):
+    """The same 100,000 chain instances on batch-interleaved slabs
+    (blasfeo_dsyrk_dpotrf_dtrsm_dgemm_batch_il, a quad of lanes per instance);
+    the conversions happen outside the timed region.  Same algorithmic bytes
+    as the back-to-back leg; outputs compared with the back-to-back call's."""
+    import numpy as np
+    from blasfeo_b200.api import DMatBatch, DMatBatchIL
+    sh = C.c_void_p(stream.cuda_stream)
+    ins = [DMatBatchIL(slabs[n].m, slabs[n].n, nb).from_batch(slabs[n], sh) for n in "ARCG"]
+    outs = [DMatBatchIL(16, 16, nb) for _ in range(3)]
+    info = torch.zeros(nb, dtype=torch.int32, device=ins[0].buf.device)
+    ms = tm(lambda: lib.blasfeo_dsyrk_dpotrf_dtrsm_dgemm_batch_il(nb, 16, 32, 16.0, *(x.ref for x in ins),
+                                                                *(x.ref for x in outs), C.c_void_p(info.data_ptr()),
+                                                                sh))
+    if not bool((info == 0).all().item()):
+        raise RuntimeError("interleaved chain reported a non-positive pivot")
+    diff = {}
+    for name, il, ref in (("L", outs[0], L), ("X", outs[1], X), ("D", outs[2], D)):
+        back = il.to_batch(DMatBatch(16, 16, nb), sh)
+        torch.cuda.synchronize()
+        a_, b_ = back.unpack_all()[:2000], ref.unpack_all()[:2000]
+        if name == "L":
+            a_, b_ = np.tril(a_), np.tril(b_)
+        diff[name] = float(np.linalg.norm(a_ - b_) / np.linalg.norm(b_))
+    by = 15424.0 * nb
+    return {"ms": ms, "instances_per_s": nb / ms * 1e3, "gbs": by / ms / 1e6, "frac_of_hbm": by / ms / 1e6 / peak_bw,
+            "speedup_vs_back_to_back": ms_b2b / ms, "relfro_vs_back_to_back_first_2000": diff}
 
 
 def potrf_layouts(lib, torch, dev, stream, peak_bw, g, tm, nb=100000, n=16):
@@ -859,6 +939,42 @@ def potrf_layouts(lib, torch, dev, stream, peak_bw, g, tm, nb=100000, n=16):
     res["winner"] = "interleaved" if ms_i < ms_b else "back_to_back"
     res["relfro_between_layouts"] = float(np.linalg.norm(a_ - b_) / np.linalg.norm(b_))
     return res
+
+
+def riccati_interleaved(lib, torch, sh, peak_bw, tm, nbt, N, nx, nu, BAs, RSQ, L_b2b, ms_b2b):
+    """The FP64 factorization of the same problems on stage-major
+    batch-interleaved slabs (blasfeo_dric_trf_batch_il, a quad of lanes per
+    problem; stage k of problem b at instance k * bs + b); conversions outside
+    the timed region; factors compared with the back-to-back call's."""
+    import numpy as np
+    from blasfeo_b200.api import DMatBatch, DMatBatchIL
+    from blasfeo_b200.workloads import fill_batch
+    dev = BAs.device
+    bs = (nbt + 15) // 16 * 16
+    ba = torch.zeros((N * bs, 16, nx), dtype=torch.float64, device=dev)
+    ba.view(N, bs, 16, nx)[:, :nbt] = BAs.reshape(nbt, N, 16, nx).transpose(0, 1)
+    rsq = torch.zeros(((N + 1) * bs, 16, 16), dtype=torch.float64, device=dev)
+    rsq.view(N + 1, bs, 16, 16)[:, :nbt] = RSQ.reshape(nbt, N + 1, 16, 16).transpose(0, 1)
+    tBA, tRSQ = DMatBatch(16, nx, N * bs), DMatBatch(16, 16, (N + 1) * bs)
+    fill_batch(tBA, ba.contiguous())
+    fill_batch(tRSQ, rsq.contiguous())
+    iBA, iRSQ = DMatBatchIL(16, nx, N * bs).from_batch(tBA, sh), DMatBatchIL(16, 16, (N + 1) * bs).from_batch(tRSQ, sh)
+    iL = DMatBatchIL(16, 16, (N + 1) * bs)
+    info = torch.zeros(nbt, dtype=torch.int32, device=dev)
+    ms = tm(lambda: lib.blasfeo_dric_trf_batch_il(nbt, N, nx, nu, iBA.ref, iRSQ.ref, iL.ref, C.c_void_p(info.data_ptr()),
+                                                  sh))
+    if not bool((info == 0).all().item()):
+        raise RuntimeError("interleaved Riccati factorization reported a non-positive pivot")
+    back = iL.to_batch(DMatBatch(16, 16, (N + 1) * bs), sh)
+    torch.cuda.synchronize()
+    Lil = back.unpack_all().reshape(N + 1, bs, 16, 16)[:, :nbt].transpose(1, 0, 2, 3)
+    m = nu + nx  # the written blocks: m x m at stages < N, nx x nx at stage N
+    a_ = np.concatenate([np.tril(Lil[:, :N, :m, :m]).ravel(), np.tril(Lil[:, N, :nx, :nx]).ravel()])
+    b_ = np.concatenate([np.tril(L_b2b[:, :N, :m, :m]).ravel(), np.tril(L_b2b[:, N, :nx, :nx]).ravel()])
+    by = (16 * nx + 16 * 16 + 136) * 8 * N * nbt
+    return {"ms": ms, "problems_per_s": nbt / ms * 1e3, "gbs": by / ms / 1e6, "frac_of_hbm": by / ms / 1e6 / peak_bw,
+            "speedup_vs_back_to_back": ms_b2b / ms,
+            "relfro_vs_back_to_back": float(np.linalg.norm(a_ - b_) / np.linalg.norm(b_))}
 
 
 def riccati_legs(lib, torch, dev, stream, peak_bw, g, tm, nbt, N, nx, nu, cpu):
@@ -912,6 +1028,11 @@ def riccati_legs(lib, torch, dev, stream, peak_bw, g, tm, nbt, N, nx, nu, cpu):
         Ls[prec] = sL.unpack_all().reshape(nbt, N + 1, 16, 16)
         slabs[prec] = (sBA, sRSQ, sL)
     sBA, sRSQ, sL = slabs["d"]
+    try:
+        out["riccati_d_N30"]["interleaved"] = riccati_interleaved(lib, torch, sh, peak_bw, tm, nbt, N, nx, nu, BAs,
+                                                                  RSQ, Ls["d"], out["riccati_d_N30"]["ms"])
+    except Exception as ex:  # reported, never silently replaced
+        out["riccati_d_N30"]["interleaved"] = {"error": repr(ex)}
     if cpu:
         try:
             out["riccati_d_N30"]["cpu_reference"], Ls["ref"] = cpu_riccati_leg(nbt, N, nx, nu, sBA, sRSQ, sL)

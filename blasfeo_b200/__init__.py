@@ -210,6 +210,8 @@ _sig("blasfeo_create_dmat_batch_il", None, _i, _i, _i, _IL, _vp)
 _sig("blasfeo_dmat_batch_to_il", _i, _DB, _IL, _vp)
 _sig("blasfeo_dmat_batch_from_il", _i, _IL, _DB, _vp)
 _sig("blasfeo_dpotrf_l_batch_il", _i, _i, _i, _IL, _IL, _vp, _vp)
+_sig("blasfeo_dsyrk_dpotrf_dtrsm_dgemm_batch_il", _i, _i, _i, _i, _d, _IL, _IL, _IL, _IL, _IL, _IL, _IL, _vp, _vp)
+_sig("blasfeo_dric_trf_batch_il", _i, _i, _i, _i, _i, _IL, _IL, _IL, _vp, _vp)
 _sig("blasfeo_b200_set_cost_model", _i, _i, _i, _vp)
 _sig("blasfeo_b200_clear_cost_model", None)
 _sig("blasfeo_b200_dispatch_pick", _i, _i, _i, _vp, _vp, _vp, _i, _i, _i, _vp)

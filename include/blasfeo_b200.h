@@ -301,6 +301,23 @@ int blasfeo_dmat_batch_from_il(const struct blasfeo_dmat_batch_il *src, struct b
  * dA slots; info[b] as for blasfeo_dpotrf_l_batch. */
 int blasfeo_dpotrf_l_batch_il(int batch, int m, struct blasfeo_dmat_batch_il *sC, struct blasfeo_dmat_batch_il *sD,
 	int *info, void *stream);
+/* The fused chain blasfeo_dsyrk_dpotrf_dtrsm_dgemm_batch on interleaved slabs
+ * (one instance per quad of lanes): m = 16 only (else ENOTSUP), sA 16 x k with
+ * k >= 1, sR, sC, sG, sL, sX, sD 16 x 16 of one group stride; results equal to
+ * the back-to-back call's, info[b] as there (never -3: no bulk copies). */
+int blasfeo_dsyrk_dpotrf_dtrsm_dgemm_batch_il(int batch, int m, int k, double shift,
+	struct blasfeo_dmat_batch_il *sA, struct blasfeo_dmat_batch_il *sR, struct blasfeo_dmat_batch_il *sC,
+	struct blasfeo_dmat_batch_il *sG, struct blasfeo_dmat_batch_il *sL, struct blasfeo_dmat_batch_il *sX,
+	struct blasfeo_dmat_batch_il *sD, int *info, void *stream);
+/* The Riccati factorization blasfeo_dric_trf_batch on interleaved slabs (one
+ * problem per quad of lanes), nu + nx <= 16 (else ENOTSUP).  Stage-major
+ * slabs: stage k of problem b is instance k * bs + b, bs = batch rounded up
+ * to a multiple of 16 (so the problems of a group sit side by side at every
+ * stage); sBAbt 16 x nx with >= N * bs instances, sRSQ and sL 16 x 16 with
+ * >= (N+1) * bs instances, all on 16-byte boundaries (else EINVAL).  Outputs
+ * and info[b] as blasfeo_dric_trf_batch (never -3: no bulk-copy waits). */
+int blasfeo_dric_trf_batch_il(int batch, int N, int nx, int nu, struct blasfeo_dmat_batch_il *sBAbt,
+	struct blasfeo_dmat_batch_il *sRSQ, struct blasfeo_dmat_batch_il *sL, int *info, void *stream);
 
 /* Host column-major batch <-> uniform-batch slab (no reference counterpart;
  * the batched form of blasfeo_pack_dmat / blasfeo_unpack_dmat): instance b of

@@ -80,3 +80,93 @@ def test_potrf_il_rejects(bf):
     assert bf.lib.blasfeo_dpotrf_l_batch_il(4, 20, a.ref, a.ref, None, None) == 4   # n > 16
     b = DMatBatchIL(16, 16, 4)
     assert bf.lib.blasfeo_dpotrf_l_batch_il(5, 16, b.ref, b.ref, None, None) == 1   # batch beyond the slab
+
+
+def _il_chain(bf, A, R, Cm, G, shift):
+    import torch
+    from blasfeo_b200.api import DMatBatchIL
+    nb, m, k = A.shape
+    ins = []
+    for X in (A, R, Cm, G):
+        ins.append(DMatBatchIL(X.shape[1], X.shape[2], nb).from_batch(bf.DMatBatch(X.shape[1], X.shape[2],
+                                                                                   nb).pack_all(X)))
+    outs = [DMatBatchIL(m, m, nb) for _ in range(3)]
+    info = torch.full((nb,), -9, dtype=torch.int32, device="cuda")
+    st = bf.lib.blasfeo_dsyrk_dpotrf_dtrsm_dgemm_batch_il(nb, m, k, shift, *(x.ref for x in ins),
+                                                          *(x.ref for x in outs), C.c_void_p(info.data_ptr()), None)
+    assert st == 0
+    res = [o.to_batch(bf.DMatBatch(m, m, nb)) for o in outs]
+    torch.cuda.synchronize()
+    return res, info.cpu().numpy()
+
+
+def test_chain_il_vs_golden_reference_outputs(bf):
+    import os
+    g = np.load(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "cfg2.npz"))
+    (dL, dX, dD), info = _il_chain(bf, g["A"], g["R"], g["C"], g["G"], 16.0)
+    assert (info == 0).all()
+    L, X, D = dL.unpack_all(), dX.unpack_all(), dD.unpack_all()
+    for b in range(g["A"].shape[0]):
+        assert relfro(np.tril(L[b]), g["L"][b]) <= 1e-13
+        assert relfro(X[b], g["X"][b]) <= 1e-13
+        assert relfro(D[b], g["D"][b]) <= 1e-13
+
+
+@pytest.mark.parametrize("nb,k", [(1037, 32), (45, 7), (8, 1)])
+def test_chain_il_vs_back_to_back_and_oracle(bf, nb, k):
+    """Partial last group, partial last warp, k not a multiple of 4, and one
+    instance with a zero row of A under shift 0 (zero pivot, info = row + 1)."""
+    import torch
+    rng = np.random.default_rng(nb + k)
+    m = 16
+    A = rng.standard_normal((nb, m, k))
+    R, Cm, G = (rng.standard_normal((nb, m, m)) for _ in range(3))
+    shift = 0.0 if k >= m else 16.0
+    bad = min(5, nb - 1)
+    if shift == 0.0:
+        A[bad, 5, :] = 0.0
+    (dL, dX, dD), info = _il_chain(bf, A, R, Cm, G, shift)
+    # the back-to-back kernel on the same instances
+    bb = [bf.DMatBatch(X.shape[1], X.shape[2], nb).pack_all(X) for X in (A, R, Cm, G)]
+    oL, oX, oD = (bf.DMatBatch(m, m, nb) for _ in range(3))
+    info2 = torch.full((nb,), -9, dtype=torch.int32, device="cuda")
+    assert bf.lib.blasfeo_dsyrk_dpotrf_dtrsm_dgemm_batch(nb, m, k, shift, *(x.ref for x in bb), oL.ref, oX.ref,
+                                                         oD.ref, C.c_void_p(info2.data_ptr()), None) == 0
+    torch.cuda.synchronize()
+    assert np.array_equal(info, info2.cpu().numpy())
+    if shift == 0.0:
+        assert info[bad] == 6 and (np.delete(info, bad) == 0).all()
+    else:
+        assert (info == 0).all()
+    L, X, D, dg = dL.unpack_all(), dX.unpack_all(), dD.unpack_all(), dL.diag_all(m)
+    ok = info == 0
+    assert relfro(np.tril(L[ok]), np.tril(oL.unpack_all()[ok])) <= 1e-13
+    assert relfro(X[ok], oX.unpack_all()[ok]) <= 1e-13
+    assert relfro(D[ok], oD.unpack_all()[ok]) <= 1e-13
+    assert relfro(dg[ok], oL.diag_all(m)[ok]) <= 1e-13
+    orc = oracle_api()
+    from oracle.pyoracle import HostMat
+    for b in sorted({0, nb // 2, nb - 1}):
+        if not ok[b]:
+            continue
+        hS = HostMat(m, m).set(A[b] @ A[b].T + shift * np.eye(m))
+        hL = HostMat(m, m)
+        orc.potrf_l("d", m, hS, 0, 0, hL, 0, 0)
+        Lr = np.tril(hL.get())
+        Xr = np.linalg.solve(Lr, R[b].T).T
+        assert relfro(np.tril(L[b]), Lr) <= 1e-13
+        assert relfro(X[b], Xr) <= 1e-12
+        assert relfro(D[b], Cm[b] - Xr @ G[b].T) <= 1e-12
+
+
+def test_chain_il_rejects(bf):
+    from blasfeo_b200.api import DMatBatchIL
+    A, Q = DMatBatchIL(16, 32, 4), [DMatBatchIL(16, 16, 4) for _ in range(6)]
+    f = bf.lib.blasfeo_dsyrk_dpotrf_dtrsm_dgemm_batch_il
+    assert f(4, 12, 32, 1.0, A.ref, *(x.ref for x in Q), None, None) == 4      # m != 16
+    assert f(4, 16, 32, 1.0, A.ref, *(x.ref for x in Q), None, None) == 0
+    assert f(5, 16, 32, 1.0, A.ref, *(x.ref for x in Q), None, None) == 1      # batch beyond the slabs
+    assert f(4, 16, 31, 1.0, A.ref, *(x.ref for x in Q), None, None) == 1      # k disagrees with sA
+    B = DMatBatchIL(16, 12, 4)
+    assert f(4, 16, 32, 1.0, A.ref, B.ref, *(x.ref for x in Q[1:]), None, None) == 1  # R not 16 x 16
+    assert f(0, 16, 32, 1.0, A.ref, *(x.ref for x in Q), None, None) == 0

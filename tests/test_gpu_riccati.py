@@ -121,3 +121,92 @@ def test_riccati_reports_bad_pivot(bf):
     L, info = run(bf, "d", BAs, RSQs, nx, nu)
     assert info[0] == 0 and info[2] == 0
     assert info[1] == 16 * (N - 1) + 3
+
+
+def run_il(bf, BAs, RSQs, nx, nu):
+    """The interleaved-slab factorization: stage-major slabs (stage k of
+    problem b at instance k * bs + b, bs = batch rounded up to 16)."""
+    import ctypes as C
+    import torch
+    from blasfeo_b200.api import DMatBatchIL
+    nbt, N = BAs.shape[:2]
+    bs = (nbt + 15) // 16 * 16
+    ba = np.zeros((max(N, 1) * bs, 16, nx))
+    rsq = np.zeros(((N + 1) * bs, 16, 16))
+    for k in range(N):
+        ba[k * bs: k * bs + nbt] = BAs[:, k]
+    for k in range(N + 1):
+        rsq[k * bs: k * bs + nbt] = RSQs[:, k]
+    iBA = DMatBatchIL(16, nx, len(ba)).from_batch(bf.DMatBatch(16, nx, len(ba)).pack_all(ba))
+    iRSQ = DMatBatchIL(16, 16, len(rsq)).from_batch(bf.DMatBatch(16, 16, len(rsq)).pack_all(rsq))
+    iL = DMatBatchIL(16, 16, len(rsq))
+    info = torch.full((nbt,), -9, dtype=torch.int32, device="cuda")
+    st = bf.lib.blasfeo_dric_trf_batch_il(nbt, N, nx, nu, iBA.ref, iRSQ.ref, iL.ref, C.c_void_p(info.data_ptr()),
+                                          None)
+    assert st == 0
+    out = iL.to_batch(bf.DMatBatch(16, 16, len(rsq)))
+    torch.cuda.synchronize()
+    Lall, dall = out.unpack_all(), out.diag_all(16)
+    L = np.stack([Lall[k * bs: k * bs + nbt] for k in range(N + 1)], axis=1)
+    dA = np.stack([dall[k * bs: k * bs + nbt] for k in range(N + 1)], axis=1)
+    return L, dA, info.cpu().numpy()
+
+
+def test_riccati_il_vs_golden_reference(bf):
+    g = np.load(os.path.join(GOLD, "cfg4.npz"))
+    N, nx, nu = 30, 12, 4
+    BAs, RSQs = zip(*[problem_mats(g["A%d" % p], g["B%d" % p], N, nx, nu) for p in range(2)])
+    L, _, info = run_il(bf, np.stack(BAs), np.stack(RSQs), nx, nu)
+    assert (info == 0).all()
+    for p in range(2):
+        for k in range(N + 1):
+            m = nx if k == N else nx + nu
+            assert relfro(np.tril(L[p, k, :m, :m]), g["L%d" % p][k][:m, :m]) <= 1e-13, (p, k)
+
+
+@pytest.mark.parametrize("dims", [(12, 4, 30, 53), (8, 3, 7, 16), (5, 0, 4, 9), (13, 3, 1, 40), (4, 4, 0, 21)])
+def test_riccati_il_vs_back_to_back_and_oracle(bf, dims):
+    """Batches with partial groups and partial warps, nu = 0, N = 0 and N = 1,
+    and one problem with an indefinite stage (same info as the back-to-back
+    kernel)."""
+    nx, nu, N, nbt = dims
+    rng = np.random.default_rng(nx * 1000 + nu * 100 + N + nbt)
+    m = nx + nu
+    BAs = np.zeros((nbt, N, 16, nx))
+    RSQs = np.zeros((nbt, N + 1, 16, 16))
+    for b in range(nbt):
+        for k in range(N + 1):
+            G = rng.standard_normal((m, m))
+            RSQs[b, k, :m, :m] = G @ G.T / m + np.eye(m)
+            if k < N:
+                BAs[b, k, :m] = rng.standard_normal((m, nx)) / np.sqrt(nx)
+    bad_b = nbt // 3
+    RSQs[bad_b, N // 2, 1, 1] = -50.0
+    L, dA, info = run_il(bf, BAs, RSQs, nx, nu)
+    L2, info2 = run(bf, "d", BAs, RSQs, nx, nu)
+    assert np.array_equal(info, info2)
+    assert info[bad_b] > 0 and (np.delete(info, bad_b) == 0).all()
+    for k in range(N + 1):
+        mm = nx if k == N else m
+        ok = info == 0
+        assert relfro(np.tril(L[ok, k, :mm, :mm]), np.tril(L2[ok, k, :mm, :mm])) <= 1e-13, k
+        assert relfro(dA[ok, k, :mm], 1.0 / np.diagonal(L2[ok, k, :mm, :mm], axis1=1, axis2=2)) <= 1e-13, k
+    orc = oracle_api()
+    for b in (0, nbt - 1):
+        if info[b]:
+            continue
+        Ls = oracle_riccati(orc, BAs[b], RSQs[b], N, nx, nu)
+        for k in range(N + 1):
+            mm = nx if k == N else m
+            assert relfro(np.tril(L[b, k, :mm, :mm]), Ls[k]) <= 1e-13, (b, k)
+
+
+def test_riccati_il_rejects(bf):
+    from blasfeo_b200.api import DMatBatchIL
+    f = bf.lib.blasfeo_dric_trf_batch_il
+    BA, R = DMatBatchIL(16, 12, 2 * 16), DMatBatchIL(16, 16, 3 * 16)
+    assert f(10, 2, 12, 4, BA.ref, R.ref, R.ref, None, None) == 0
+    assert f(10, 2, 13, 4, BA.ref, R.ref, R.ref, None, None) == 4     # nu + nx > 16
+    assert f(10, 2, 11, 4, BA.ref, R.ref, R.ref, None, None) == 1     # BAbt not 16 x nx
+    assert f(17, 2, 12, 4, BA.ref, R.ref, R.ref, None, None) == 1     # slabs shorter than (N+1) * 32
+    assert f(0, 2, 12, 4, BA.ref, R.ref, R.ref, None, None) == 0
