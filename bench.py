@@ -117,7 +117,7 @@ def run_case(argv):
             bf.check(st)
         torch.cuda.synchronize()
         assert bool((info == 0).all().item())
-    elif op == "ric":
+    elif op in ("ric", "ric_il"):
         N, nx, nu = n, 12, 4
         g = torch.Generator(device=dev)
         g.manual_seed(4)
@@ -133,8 +133,22 @@ def run_case(argv):
         fill_batch(sBA, BA[:, None].expand(batch, N, 16, nx).reshape(batch * N, 16, nx).contiguous())
         fill_batch(sRSQ, torch.eye(16, dtype=torch.float64, device=dev).expand(batch * (N + 1), 16, 16).contiguous())
         info = torch.zeros(batch, dtype=torch.int32, device=dev)
+        if op == "ric_il":
+            # stage-major interleaved slabs: stage k of problem b at instance k * bs + b
+            from blasfeo_b200.api import DMatBatchIL
+            bs = (batch + 15) // 16 * 16
+            ba = torch.zeros((N * bs, 16, nx), dtype=torch.float64, device=dev)
+            ba.view(N, bs, 16, nx)[:, :batch] = BA[None]
+            tBA, tRSQ = bf.DMatBatch(16, nx, N * bs), bf.DMatBatch(16, 16, (N + 1) * bs)
+            fill_batch(tBA, ba)
+            fill_batch(tRSQ, torch.eye(16, dtype=torch.float64, device=dev).expand((N + 1) * bs, 16, 16).contiguous())
+            sBA, sRSQ = DMatBatchIL(16, nx, N * bs).from_batch(tBA), DMatBatchIL(16, 16, (N + 1) * bs).from_batch(tRSQ)
+            sL = DMatBatchIL(16, 16, (N + 1) * bs)
+            f = lib.blasfeo_dric_trf_batch_il
+        else:
+            f = lib.blasfeo_dric_trf_batch
         for _ in range(reps):
-            bf.check(lib.blasfeo_dric_trf_batch(batch, N, nx, nu, sBA.ref, sRSQ.ref, sL.ref, P(info), None))
+            bf.check(f(batch, N, nx, nu, sBA.ref, sRSQ.ref, sL.ref, P(info), None))
         torch.cuda.synchronize()
         assert bool((info == 0).all().item())
     elif op == "cfg3":

@@ -9,9 +9,9 @@
 // (d_lapack_lib4.c:918) + blasfeo_dtrsm_rltn (d_blas3_lib4.c:4123) +
 // blasfeo_dgemm_nt (d_blas3_lib4.c:727)):
 //   S = A A^T + shift I   in registers, rank-1 updates of the lane's rows by
-//                         column l of A, read from a shared-memory stage that
-//                         cp.async fills 16 columns at a time (the copies
-//                         hold no registers, so a lane has 32 in flight);
+//                         column l of A, read from shared memory that
+//                         cp.async fills 8 columns at a time, double-buffered
+//                         (the copies hold no registers);
 //   L = chol(S)           column by column in registers, pivot rule of
 //                         kernel/generic/kernel_dgemm_4x4_lib4.c:5700-5710
 //                         (c > 0 -> sqrt(c) and 1/sqrt(c), else 0 and 0), the
@@ -22,11 +22,13 @@
 //                         column, d_ij = (r_ij - sum_{l<j} d_il L_jl) *
 //                         (1/L_jj) as the reference's trsm, each L_jl read
 //                         once from shared memory for the 4 rows;
-//   D = C - X G^T         G staged the same way, its copies issued before
-//                         the factorization so that they land under it.
-// Each load or copy moves one element of 8 consecutive instances (64 bytes):
-// loads that a warp waits on one at a time would leave it latency-bound with
-// the 8 warps per SM that its registers allow.
+//   D = C - X G^T         G staged the same way, rows 0..7 issued before the
+//                         factorization so that they land under it, rows
+//                         8..15 under the first half of D.
+// Each load or copy moves one element of 8 consecutive instances (64 bytes).
+// Loads that a warp waits on one at a time leave it latency-bound, so the
+// kernel keeps copies in flight and 12 warps per SM (168 registers, 16.5 KB
+// of shared memory per warp).
 // L's lower triangle and inverse diagonal, X and D are written once.
 #include "quad.cuh"
 
@@ -46,29 +48,37 @@ struct ChainIlArgs {
 
 constexpr int WPB = 4;                // warps per block
 constexpr int LSLOTS = 120 + 16;      // strictly lower L, then the inverse diagonal
-constexpr int BSLOTS = 256;           // staging buffer: 16 x 16 elements of 8 instances
+constexpr int BSLOTS = 128;           // staging buffer: 128 elements of 8 instances
 
-// 16 rows x 16 columns (columns c0 .. c0+15 of a panel-major 16 x * slab with
-// panel stride cn, columns >= ncol skipped) of the warp's 8 instances into
-// stage[(16 i + c) * 8 + t]: each element of 8 instances is one 64-byte run in
-// HBM, copied as four 16-byte pieces; 32 pieces per lane, none held in
-// registers.
-__device__ __forceinline__ void stage_16x16(double (*stage)[QPW], const double *grp, int cn, int c0, int ncol,
-                                            int lane) {
-#pragma unroll 8
-	for (int r = 0; r < 32; r++) {
+// 128 elements (i, c) of the warp's 8 instances, i in [r0, r0 + nr), c in
+// [c0, c0 + nc) (nr * nc = 128) of a panel-major slab with panel stride cn,
+// columns >= ncol skipped, into stage[nc (i - r0) + (c - c0)][t]: each element
+// of 8 instances is one 64-byte run in HBM, copied as four 16-byte pieces; 16
+// pieces per lane, none held in registers.
+__device__ __forceinline__ void stage_128(double (*stage)[QPW], const double *grp, int cn, int r0, int c0, int nc,
+                                          int ncol, int lane) {
+#pragma unroll 4
+	for (int r = 0; r < 16; r++) {
 		const int p = lane + 32 * r;
 		const int el = p >> 2, part = p & 3;
-		const int i = el >> 4, c = el & 15;
-		if (c0 + c < ncol) cpa16(&stage[el][2 * part], grp + pme(i, c0 + c, cn) * IL + 2 * part);
+		const int i = r0 + el / nc, c = c0 + el % nc;
+		if (c < ncol) cpa16(&stage[el][2 * part], grp + pme(i, c, cn) * IL + 2 * part);
 	}
 }
 
-__global__ void __launch_bounds__(WPB * 32) k_chain16_il(ChainIlArgs a) {
-	// per warp: L_jl (l < j) of its 8 instances at lsm[w][tri(j) + l][t], the
-	// inverse pivots at lsm[w][120 + j][t]; a staging buffer for 16 columns of
-	// A, then for G -- the 8 quads of a warp read 8 consecutive doubles, no
-	// bank conflict
+template <int N>
+__device__ __forceinline__ void cpa_wait() {
+	asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+
+__global__ void __launch_bounds__(WPB * 32, 3) k_chain16_il(ChainIlArgs a) {
+	// per warp: L_jl (l < j) of its 8 instances at lw[tri(j) + l][t], the
+	// inverse pivots at lw[120 + j][t]; a 128-element staging buffer st.  A is
+	// staged 8 columns at a time, alternately into st and into lw (free until
+	// the factorization), so the next chunk's copies run under the current
+	// chunk's products; G rows 0..7 go to st before the factorization, rows
+	// 8..15 to lw after the solve.  The 8 quads of a warp read 8 consecutive
+	// doubles, no bank conflict.
 	extern __shared__ __align__(16) double dsm[];
 	const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
 	double(*lw)[QPW] = (double(*)[QPW])(dsm + (size_t)w * (LSLOTS + BSLOTS) * QPW);
@@ -90,22 +100,45 @@ __global__ void __launch_bounds__(WPB * 32) k_chain16_il(ChainIlArgs a) {
 	double *Xg = a.X + g * a.g16 + sl0 + t;
 	double *Dg = a.D + g * a.g16 + sl0 + t;
 
-	// 1. S = A A^T + shift I (rows q + 4s), A staged 16 columns at a time
+	// 1. S = A A^T + shift I (rows q + 4s), A staged 8 columns at a time,
+	// double-buffered
 	double S[4][16];
 #pragma unroll
 	for (int s = 0; s < 4; s++)
 #pragma unroll
 		for (int j = 0; j < 16; j++) S[s][j] = 0.0;
-	for (int c0 = 0; c0 < a.k; c0 += 16) {
-		stage_16x16(st, Ag, a.cna, c0, a.k, lane);
-		cpa_commit();
-		cpa_wait_all();
+	const int nch = (a.k + 7) / 8;
+	stage_128(st, Ag, a.cna, 0, 0, 8, a.k, lane);
+	cpa_commit();
+	for (int ch = 0; ch < nch; ch++) {
+		double(*cur)[QPW] = (ch & 1) ? lw : st;
+		if (ch + 1 < nch) {
+			stage_128((ch & 1) ? st : lw, Ag, a.cna, 0, 8 * (ch + 1), 8, a.k, lane);
+			cpa_commit();
+			cpa_wait<1>();
+		} else {
+			cpa_wait<0>();
+		}
 		__syncwarp();
-		syrk_rows(S, st, min(16, a.k - c0), 16, q, t);
+		const int nc = min(8, a.k - 8 * ch);
+#pragma unroll 2
+		for (int c = 0; c < nc; c++) {
+			double col[16];
+#pragma unroll
+			for (int i = 0; i < 16; i++) col[i] = cur[8 * i + c][t];
+#pragma unroll
+			for (int s = 0; s < 4; s++) {
+				const double ai =
+				    (q == 0) ? col[4 * s] : (q == 1) ? col[4 * s + 1] : (q == 2) ? col[4 * s + 2] : col[4 * s + 3];
+#pragma unroll
+				for (int j = 0; j < 16; j++)
+					if (j <= 4 * s + 3) S[s][j] = fma(ai, col[j], S[s][j]);
+			}
+		}
 		__syncwarp();
 	}
-	// G's copies run under the factorization and the solve
-	stage_16x16(st, Gg, 16, 0, 16, lane);
+	// G rows 0..7: copies run under the factorization and the solve
+	stage_128(st, Gg, 16, 0, 0, 16, 16, lane);
 	cpa_commit();
 	// shift on the diagonal; entries right of it (computed with the others,
 	// never used) cleared
@@ -154,23 +187,36 @@ __global__ void __launch_bounds__(WPB * 32) k_chain16_il(ChainIlArgs a) {
 			for (int j = 0; j < 16; j++) Xg[pme(q + 4 * s, j, 16) * IL] = x[s][j];
 	}
 
-	// 4. D = C - X G^T, G from the staging buffer
-	cpa_wait_all();
+	// 4. D = C - X G^T: G rows 8..15 staged into lw (the solve is done with
+	// it), columns 0..7 of D from st meanwhile
 	__syncwarp();
-#pragma unroll 2
-	for (int j = 0; j < 16; j++) {
-		double cv[4];
-#pragma unroll
-		for (int s = 0; s < 4; s++) cv[s] = Cm[pme(q + 4 * s, j, 16) * IL];
-#pragma unroll
-		for (int l = 0; l < 16; l++) {
-			const double gv = st[16 * j + l][t];
-#pragma unroll
-			for (int s = 0; s < 4; s++) cv[s] = fma(-x[s][l], gv, cv[s]);
+	stage_128(lw, Gg, 16, 8, 0, 16, 16, lane);
+	cpa_commit();
+	cpa_wait<1>();
+	__syncwarp();
+#pragma unroll 1
+	for (int h = 0; h < 2; h++) {
+		if (h == 1) {
+			cpa_wait<0>();
+			__syncwarp();
 		}
-		if (act) {
+		double(*gs)[QPW] = h ? lw : st;
+#pragma unroll 2
+		for (int jj = 0; jj < 8; jj++) {
+			const int j = 8 * h + jj;
+			double cv[4];
 #pragma unroll
-			for (int s = 0; s < 4; s++) Dg[pme(q + 4 * s, j, 16) * IL] = cv[s];
+			for (int s = 0; s < 4; s++) cv[s] = Cm[pme(q + 4 * s, j, 16) * IL];
+#pragma unroll
+			for (int l = 0; l < 16; l++) {
+				const double gv = gs[16 * jj + l][t];
+#pragma unroll
+				for (int s = 0; s < 4; s++) cv[s] = fma(-x[s][l], gv, cv[s]);
+			}
+			if (act) {
+#pragma unroll
+				for (int s = 0; s < 4; s++) Dg[pme(q + 4 * s, j, 16) * IL] = cv[s];
+			}
 		}
 	}
 }

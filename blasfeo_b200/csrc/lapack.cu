@@ -341,8 +341,11 @@ __global__ void __launch_bounds__(NT) k_getrf_blk(SizeArg sz, MatArg<T> C, MatAr
 	const int tid = threadIdx.x;
 	int *piv = piv_on ? ipiv + ipiv_stride * b : nullptr;
 	T *P = (T *)smem_raw;                        // panel: row r at P + 17 r
-	T *Us = P + (size_t)(max_m + 4) * 17;        // U12: row k at Us + k * usld
-	const int usld = n + 4;
+	// U12: row k at Us + k * usld, its column l at slot (l % 4) * q4 + l / 4, so
+	// that the update's threads (consecutive 4-column tiles) read consecutive
+	// slots for each of a tile's 4 columns (no bank conflict)
+	T *Us = P + (size_t)(max_m + 4) * 17;
+	const int usld = n + 4, q4 = usld / 4;
 	// D = C first (in place afterwards)
 	if (c.p != d.p || c.ri != d.ri || c.cj != d.cj) {
 		for (int e = tid; e < m * n; e += NT) {
@@ -435,7 +438,7 @@ __global__ void __launch_bounds__(NT) k_getrf_blk(SizeArg sz, MatArg<T> C, MatAr
 #pragma unroll
 			for (int k = 0; k < 16; k++) {
 				if (k < w) d.at(c0 + k, c0 + w + l) = u[k];
-				Us[k * usld + l] = (k < w) ? u[k] : T(0);
+				Us[k * usld + (l & 3) * q4 + (l >> 2)] = (k < w) ? u[k] : T(0);
 			}
 		}
 		__syncthreads();
@@ -458,7 +461,7 @@ __global__ void __launch_bounds__(NT) k_getrf_blk(SizeArg sz, MatArg<T> C, MatAr
 #pragma unroll
 					for (int a = 0; a < 4; a++) av[a] = (r0 + a < pr) ? P[(r0 + a) * 17 + k] : T(0);
 #pragma unroll
-					for (int q = 0; q < 4; q++) bv[q] = Us[k * usld + l0 + q];
+					for (int q = 0; q < 4; q++) bv[q] = Us[k * usld + q * q4 + tj];
 #pragma unroll
 					for (int a = 0; a < 4; a++)
 #pragma unroll

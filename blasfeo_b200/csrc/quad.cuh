@@ -1,10 +1,11 @@
 // Building blocks of the kernels that give one instance of a batch-interleaved
-// slab (interleave.cu) to a quad of lanes: lane q of the quad owns the rows
-// i = q + 4s (s = 0..3) of a 16 x 16 operand, 8 instances per warp.
+// slab (interleave.cu) to a group of G lanes (G = 4: a quad): lane o of the
+// group owns the rows i = o + G s of a 16 x 16 operand, 32 / G instances per
+// warp.
 //
 // Layout: element slot e of instance b at mem[(b / IL) * gstride + e * IL + b % IL];
-// the warp's 8 instances are half of one group, so one element of all of them
-// is a contiguous 64-byte run.
+// the warp's 32 / G instances are consecutive inside one group, so one element
+// of all of them is one contiguous run of 256 / G bytes.
 #pragma once
 
 #include "common.cuh"
@@ -33,47 +34,96 @@ __device__ __forceinline__ void cpa16(void *dst, const void *src) {
 __device__ __forceinline__ void cpa_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
 __device__ __forceinline__ void cpa_wait_all() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
 
-// Cholesky column J of the quad's 16 x 16 operand, J = 0..15 by recursion
-// (compile-time indices only, so S stays in registers).  S[s][j] = entry
-// (q + 4s, j), j <= 4s + 3.  Pivot rule of the reference
+// Cholesky column J of a 16 x 16 operand spread over a group of G lanes (G =
+// 4, 8 or 16; lane o of the group owns the rows i = o + G s, s < 16 / G), J =
+// 0..15 by recursion (compile-time indices only, so S stays in registers).
+// S[s][j] = entry (o + G s, j), j <= G s + G - 1.  Pivot rule of the reference
 // (kernel/generic/kernel_dgemm_4x4_lib4.c:5700-5710): c > 0 -> L_jj = sqrt(c)
 // (formed as c * rsqrt(c)) and 1/L_jj = rsqrt(c), else 0 and 0.  The inverse
 // pivot of column J < m goes to dA[J * IL] (HBM, when act) and, when PARK, to
-// ism[QPW * J] (shared memory); bad = first J < m with a non-positive pivot,
-// plus one.  Columns >= m must hold an identity block (they factor to it).
-template <int J, bool PARK>
-struct QCol {
-	static __device__ __forceinline__ void run(double (&S)[4][16], int q, int lane, int m, double *ism, double *dA,
+// ism[(32 / G) * J] (shared memory); bad = first J < m with a non-positive
+// pivot, plus one.  Columns >= m must hold an identity block (they factor to
+// it).
+template <int G>
+__device__ __forceinline__ int gowner(int lane, int i) { return (lane & ~(G - 1)) | (i & (G - 1)); }
+
+template <int G, int J, bool PARK>
+struct GCol {
+	static __device__ __forceinline__ void run(double (&S)[16 / G][16], int o, int lane, int m, double *ism, double *dA,
 	                                           bool act, int &bad) {
-		constexpr int SJ = J >> 2;
-		const double mine = (q == (J & 3)) ? S[SJ][J] : 0.0;
-		const double c = __shfl_sync(0xffffffffu, mine, owner(lane, J));
+		constexpr int R = 16 / G;
+		constexpr int SJ = J / G;
+		const double mine = (o == J % G) ? S[SJ][J] : 0.0;
+		const double c = __shfl_sync(0xffffffffu, mine, gowner<G>(lane, J));
 		const bool ok = c > 0.0;
 		const double iv = ok ? rsqrt(c) : 0.0;
 		if (!ok && J < m && bad == 0) bad = J + 1;
-		if (q == (J & 3)) {
+		if (o == J % G) {
 			S[SJ][J] = ok ? c * iv : 0.0;
-			if (PARK) ism[QPW * J] = iv;
+			if (PARK) ism[(32 / G) * J] = iv;
 			if (act && J < m) dA[J * IL] = iv;
 		}
 #pragma unroll
-		for (int s = 0; s < 4; s++)
-			if (J <= 4 * s + 3 && q + 4 * s > J) S[s][J] *= iv;
+		for (int s = 0; s < R; s++)
+			if (J <= G * s + G - 1 && o + G * s > J) S[s][J] *= iv;
 #pragma unroll
 		for (int l = J + 1; l < 16; l++) {
-			const double own = (q == (l & 3)) ? S[l >> 2][J] : 0.0;
-			const double llj = __shfl_sync(0xffffffffu, own, owner(lane, l));
+			const double own = (o == l % G) ? S[l / G][J] : 0.0;
+			const double llj = __shfl_sync(0xffffffffu, own, gowner<G>(lane, l));
 #pragma unroll
-			for (int s = 0; s < 4; s++)
-				if (l <= 4 * s + 3 && q + 4 * s >= l) S[s][l] = fma(-S[s][J], llj, S[s][l]);
+			for (int s = 0; s < R; s++)
+				if (l <= G * s + G - 1 && o + G * s >= l) S[s][l] = fma(-S[s][J], llj, S[s][l]);
 		}
-		QCol<J + 1, PARK>::run(S, q, lane, m, ism, dA, act, bad);
+		GCol<G, J + 1, PARK>::run(S, o, lane, m, ism, dA, act, bad);
 	}
 };
-template <bool PARK>
-struct QCol<16, PARK> {
-	static __device__ __forceinline__ void run(double (&)[4][16], int, int, int, double *, double *, bool, int &) {}
+template <int G, bool PARK>
+struct GCol<G, 16, PARK> {
+	static __device__ __forceinline__ void run(double (&)[16 / G][16], int, int, int, double *, double *, bool, int &) {}
 };
+
+// the quad form (G = 4) used by the n = 16 chain
+template <int J, bool PARK>
+using QCol = GCol<4, J, PARK>;
+
+// S[s][j] += sum over c < nc of W(o + G s, c) W(j, c) for a group of G lanes,
+// W column-major in shared memory: W(i, c) at w[16 c + i][t] (rows >= mrow
+// read as zero).  Column c is read by broadcast; the lane's own entries are
+// 16 consecutive slots over the group (no bank conflict).  Entries
+// j > o + G s are computed and left for the caller to clear.
+template <int G, int P>
+__device__ __forceinline__ void syrk_rows_cm(double (&S)[16 / G][16], const double (*w)[P], int nc, int mrow, int o,
+                                             int t) {
+	constexpr int R = 16 / G;
+#pragma unroll 2
+	for (int c = 0; c < nc; c++) {
+		double col[16], ai[R];
+#pragma unroll
+		for (int i = 0; i < 16; i++) col[i] = (i < mrow) ? w[16 * c + i][t] : 0.0;
+#pragma unroll
+		for (int s = 0; s < R; s++) ai[s] = (o + G * s < mrow) ? w[16 * c + o + G * s][t] : 0.0;
+#pragma unroll
+		for (int s = 0; s < R; s++)
+#pragma unroll
+			for (int j = 0; j < 16; j++)
+				if (j <= G * s + G - 1) S[s][j] = fma(ai[s], col[j], S[s][j]);
+	}
+}
+
+// clear the entries right of the diagonal of the group's rows, optionally
+// adding `shift` on the diagonal.  Selects, not conditional stores: a store
+// under (j == o + G s) is turned into S[s][o + G s] and S into a local-memory
+// array.
+template <int G>
+__device__ __forceinline__ void clear_upper_g(double (&S)[16 / G][16], int o, double shift) {
+#pragma unroll
+	for (int s = 0; s < 16 / G; s++)
+#pragma unroll
+		for (int j = G * s; j < G * s + G; j++) {
+			const double v = S[s][j] + ((j == o + G * s) ? shift : 0.0);
+			S[s][j] = (j > o + G * s) ? 0.0 : v;
+		}
+}
 
 // S[s][j] += sum over the columns c < nc of W(q + 4s, c) W(j, c), W read from
 // shared memory at w[16 i + c][t] (rows >= mrow read as zero): the syrk of the
@@ -96,18 +146,7 @@ __device__ __forceinline__ void syrk_rows(double (&S)[4][16], const double (*w)[
 	}
 }
 
-// clear the entries right of the diagonal of the quad's rows, optionally
-// adding `shift` on the diagonal.  Selects, not conditional stores: a store
-// under (j == q + 4s) is turned into S[s][q + 4s] and S into a local-memory
-// array.
-__device__ __forceinline__ void clear_upper(double (&S)[4][16], int q, double shift) {
-#pragma unroll
-	for (int s = 0; s < 4; s++)
-#pragma unroll
-		for (int j = 4 * s; j < 4 * s + 4; j++) {
-			const double v = S[s][j] + ((j == q + 4 * s) ? shift : 0.0);
-			S[s][j] = (j > q + 4 * s) ? 0.0 : v;
-		}
-}
+// the quad form of clear_upper_g
+__device__ __forceinline__ void clear_upper(double (&S)[4][16], int q, double shift) { clear_upper_g<4>(S, q, shift); }
 
 }  // namespace quad
