@@ -22,6 +22,7 @@
 // sqrt(c) and its reciprocal, else 0 and 0), the column of each pivot passed
 // to the partner by shuffles.  16 instances per warp.
 #include "common.cuh"
+#include "quad.cuh"
 
 namespace {
 
@@ -70,80 +71,53 @@ __global__ void k_from_il(long long total, int slots, const double *__restrict__
 	}
 }
 
-// One pivot column J of the pair Cholesky (recursive template: every index
-// into a[][] is a compile-time constant, so a[][] stays in registers).
-// Lane parity h owns rows i = 2r + h; a[r][j] = L(2r + h, j) for j <= 2r + 1.
-template <int J>
-struct IlCol {
-	static __device__ __forceinline__ void run(double (&a)[8][16], int h, int n, bool act, double *dinv, int &bad) {
-		constexpr int PR = J >> 1;
-		const double mine = (h == (J & 1)) ? a[PR][J] : 0.0;
-		const double other = __shfl_xor_sync(0xffffffffu, mine, 1);
-		const double c = (h == (J & 1)) ? mine : other;
-		const bool ok = c > 0.0;
-		const double inv = ok ? rsqrt(c) : 0.0;
-		if (!ok && J < n && bad == 0) bad = J + 1;
-		if (h == (J & 1)) {
-			a[PR][J] = ok ? c * inv : 0.0;
-			if (act && J < n) dinv[J * IL] = inv;
-		}
-#pragma unroll
-		for (int r = 0; r < 8; r++)
-			if (J <= 2 * r + 1 && 2 * r + h > J) a[r][J] *= inv;
-#pragma unroll
-		for (int l = J + 1; l < 16; l++) {
-			const double own = (h == (l & 1)) ? a[l >> 1][J] : 0.0;
-			const double oth = __shfl_xor_sync(0xffffffffu, own, 1);
-			const double llj = (h == (l & 1)) ? own : oth;
-#pragma unroll
-			for (int r = 0; r < 8; r++)
-				if (l <= 2 * r + 1 && 2 * r + h >= l) a[r][l] = fma(-a[r][J], llj, a[r][l]);
-		}
-		IlCol<J + 1>::run(a, h, n, act, dinv, bad);
-	}
-};
-template <>
-struct IlCol<16> {
-	static __device__ __forceinline__ void run(double (&)[8][16], int, int, bool, double *, int &) {}
-};
-
-// Cholesky of n <= 16 per lane pair: lane 2t + h of a warp takes rows 2r + h
-// of instance 16 * (global warp) + t.
-__global__ void __launch_bounds__(256) k_dpotrf_il(int batch, int n, const double *__restrict__ C, double *D,
+// Cholesky of n <= 16 per group of G lanes (quad::GCol): lane o of a group
+// takes rows o + G s of instance (32 / G) * (global warp) + (lane / G); G = 2
+// is a lane pair (8 rows per lane, 72 doubles of the lower triangle), G = 4 a
+// quad (4 rows, 40 doubles).  Rows and columns >= n factor as an identity
+// block.
+#ifndef POTRF_IL_G
+#define POTRF_IL_G 2
+#endif
+template <int G>
+__global__ void __launch_bounds__(256, (G >= 4) ? 2 : 1) k_dpotrf_il(int batch, int n, const double *__restrict__ C, double *D,
                                                    long long gstride, int cn, int pmcn, int *info) {
+	constexpr int P = 32 / G, R = 16 / G;
 	const int lane = threadIdx.x & 31;
-	const int t = lane >> 1, h = lane & 1;
+	const int o = lane % G, t = lane / G;
 	const long long gw = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-	const long long b = gw * IL + t;
+	const long long b0 = gw * P;
+	if (b0 >= batch) return;  // a whole warp past the batch (no block barrier follows)
+	const long long b = b0 + t;
 	const bool act = b < batch;
-	const double *cg = C + gw * gstride + t;
-	double *dg = D + gw * gstride + t;
-	double a[8][16];
+	const double *cg = C + (b0 / IL) * gstride + (b0 % IL) + t;
+	double *dg = D + (b0 / IL) * gstride + (b0 % IL) + t;
+	double a[R][16];
 #pragma unroll
-	for (int r = 0; r < 8; r++)
+	for (int s = 0; s < R; s++)
 #pragma unroll
 		for (int j = 0; j < 16; j++) {
-			const int i = 2 * r + h;
+			const int i = o + G * s;
 			double v = 0.0;
-			if (j <= 2 * r + 1) {
+			if (j <= G * s + G - 1) {
 				if (act && i < n && j < n && j <= i)
 					v = cg[pm_el(i, j, cn) * IL];
 				else if (i == j)
 					v = 1.0;  // padding rows and columns factor to the identity
 			}
-			a[r][j] = v;
+			a[s][j] = v;
 		}
 	int bad = 0;
-	IlCol<0>::run(a, h, n, act, dg + (long long)pmcn * IL, bad);
+	quad::GCol<G, 0, false>::run(a, o, lane, n, nullptr, dg + (long long)pmcn * IL, act, bad);
 	if (act) {
 #pragma unroll
-		for (int r = 0; r < 8; r++)
+		for (int s = 0; s < R; s++)
 #pragma unroll
 			for (int j = 0; j < 16; j++) {
-				const int i = 2 * r + h;
-				if (j <= 2 * r + 1 && i < n && j <= i) dg[pm_el(i, j, cn) * IL] = a[r][j];
+				const int i = o + G * s;
+				if (j <= G * s + G - 1 && i < n && j <= i) dg[pm_el(i, j, cn) * IL] = a[s][j];
 			}
-		if (h == 0 && info) info[b] = bad;
+		if (o == 0 && info) info[b] = bad;
 	}
 }
 
@@ -221,11 +195,12 @@ int blasfeo_dpotrf_l_batch_il(int batch, int m, struct blasfeo_dmat_batch_il *sC
 	if (sC->m < m || sC->n < m || sD->m < m || sD->n < m || sC->batch < batch || sD->batch < batch ||
 	    sC->pm != sD->pm || sC->cn != sD->cn || sC->gstride != sD->gstride)
 		return BLASFEO_B200_EINVAL;
-	const long long warps = (batch + IL - 1) / IL;
+	constexpr int G = POTRF_IL_G, P = 32 / G;
+	const long long warps = (batch + P - 1) / P;
 	const int threads = 256;
 	const long long blocks = (warps * 32 + threads - 1) / threads;
-	k_dpotrf_il<<<(unsigned)blocks, threads, 0, (cudaStream_t)stream>>>(batch, m, sC->mem, sD->mem, sC->gstride,
-	                                                                     sC->cn, sC->pm * sC->cn, info);
+	k_dpotrf_il<G><<<(unsigned)blocks, threads, 0, (cudaStream_t)stream>>>(batch, m, sC->mem, sD->mem, sC->gstride,
+	                                                                        sC->cn, sC->pm * sC->cn, info);
 	return bf::check_launch();
 }
 

@@ -227,6 +227,36 @@ __device__ int block_argmax_first(T v, int idx, int *s_idx, T *s_val) {
 	return r;
 }
 
+// block_argmax_first with one barrier: every thread reduces the per-warp
+// results itself.  Two calls must be separated by a __syncthreads (the
+// per-warp slots are reused).
+template <typename T>
+__device__ int block_argmax_first1(T v, int idx, int *s_idx, T *s_val) {
+	const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+#pragma unroll
+	for (int off = 16; off > 0; off >>= 1) {
+		T ov = __shfl_down_sync(0xffffffffu, v, off);
+		int oi = __shfl_down_sync(0xffffffffu, idx, off);
+		if (ov > v || (ov == v && oi < idx)) {
+			v = ov;
+			idx = oi;
+		}
+	}
+	if (lane == 0) {
+		s_val[warp] = v;
+		s_idx[warp] = idx;
+	}
+	__syncthreads();
+	T bv = s_val[0];
+	int bi = s_idx[0];
+	for (int w = 1; w < nw; w++)
+		if (s_val[w] > bv || (s_val[w] == bv && s_idx[w] < bi)) {
+			bv = s_val[w];
+			bi = s_idx[w];
+		}
+	return bi;
+}
+
 // LU with row pivoting of one instance per CTA.  SMEM: the instance's m x n
 // block is copied into shared memory (panel-major), factored there and
 // copied back; only instances whose block fits in smem_cap bytes are taken.
@@ -273,6 +303,7 @@ __global__ void __launch_bounds__(NT) k_getrf(SizeArg sz, MatArg<T> C, MatArg<T>
 				}
 			}
 			ip = block_argmax_first<T>(best, bi, s_idx, s_val);
+			if (ip >= m) ip = j;  // no candidate compared above -1: a column of NaNs
 			if (ip != j)
 				for (int l = tid; l < n; l += NT) {
 					T t = d.at(j, l);
@@ -313,17 +344,22 @@ __global__ void __launch_bounds__(NT) k_getrf(SizeArg sz, MatArg<T> C, MatArg<T>
 //   b. it is factored there column by column: pivot = first row of the largest
 //      |a| (kernel/generic/kernel_dgetrf_pivot_lib4.c:84-165), row swap inside
 //      the panel, scaling by the reciprocal pivot (0 for a zero pivot;
-//      getrf_np divides), rank-1 update of the panel's later columns;
+//      getrf_np divides), rank-1 update of the panel's later columns -- two
+//      barriers per column, each thread scaling and updating its own rows and
+//      finding their candidate for the next pivot;
 //   c. the panel goes back to global memory;
-//   d. its row swaps are applied, in order, to the columns outside the panel
-//      (one thread per column);
+//   d. its row swaps, in order, are one permutation of at most 32 rows,
+//      applied to the columns outside the panel (one thread per column, all
+//      loads before the stores);
 //   e. U12 = L11^{-1} A12 for the columns right of the panel (one thread per
 //      column, unit lower L11 from shared memory), kept in shared memory;
 //   f. A22 -= L21 U12 as 4 x 4 register tiles (rank-16 update, 4-row tiles of
-//      the panel layout, consecutive threads on consecutive column tiles).
-// Shared memory: (m + 4) x 17 panel plus 16 x (n + 4) U12.
-template <typename T, int NT>
-__global__ void __launch_bounds__(NT) k_getrf_blk(SizeArg sz, MatArg<T> C, MatArg<T> D, int *ipiv,
+//      the panel layout, consecutive threads on consecutive column tiles, the
+//      next tile's loads in flight under the current tile's products).
+// Shared memory: (m + 4) x 17 panel, 16 x (n + 4) U12, m + 4 ints.  MINB
+// blocks per SM cap the registers (the variants differ in it).
+template <typename T, int NT, int MINB>
+__global__ void __launch_bounds__(NT, MINB) k_getrf_blk(SizeArg sz, MatArg<T> C, MatArg<T> D, int *ipiv,
                                                    long long ipiv_stride, int *info, int smem_cap, int max_m,
                                                    bool piv_on) {
 	extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -331,6 +367,7 @@ __global__ void __launch_bounds__(NT) k_getrf_blk(SizeArg sz, MatArg<T> C, MatAr
 	__shared__ T s_val[32];
 	__shared__ int s_bad;
 	__shared__ int s_piv[16];
+	__shared__ int s_rows[32], s_from[32], s_nmv;
 	const int b = blockIdx.x;
 	const int m = sz.M(b), n = sz.N(b);
 	if (m <= 0 || n <= 0) return;
@@ -346,6 +383,7 @@ __global__ void __launch_bounds__(NT) k_getrf_blk(SizeArg sz, MatArg<T> C, MatAr
 	// slots for each of a tile's 4 columns (no bank conflict)
 	T *Us = P + (size_t)(max_m + 4) * 17;
 	const int usld = n + 4, q4 = usld / 4;
+	int *cont = (int *)(Us + (size_t)16 * usld);  // row permutation of a panel (max_m + 4 ints)
 	// D = C first (in place afterwards)
 	if (c.p != d.p || c.ri != d.ri || c.cj != d.cj) {
 		for (int e = tid; e < m * n; e += NT) {
@@ -365,20 +403,25 @@ __global__ void __launch_bounds__(NT) k_getrf_blk(SizeArg sz, MatArg<T> C, MatAr
 			P[r * 17 + j] = (j < w) ? d.at(c0 + r, c0 + j) : T(0);
 		}
 		__syncthreads();
-		// b. factor it
+		// b. factor it: per column one barrier for the pivot search and one
+		// after the row swap; each thread scales and updates its own rows
+		// (r = j+1+tid, +NT, ...) against the pivot row and tracks their
+		// largest |entry| of the next column for the next pivot search
+		T best = T(-1);
+		int bi = INT_MAX;
+		if (piv_on)
+			for (int r = tid; r < pr; r += NT) {
+				const T a = dev_abs(P[r * 17]);
+				if (a > best) {
+					best = a;
+					bi = r;
+				}
+			}
 		for (int j = 0; j < w; j++) {
 			int ip = j;
 			if (piv_on) {
-				T best = T(-1);
-				int bi = INT_MAX;
-				for (int r = j + tid; r < pr; r += NT) {
-					const T a = dev_abs(P[r * 17 + j]);
-					if (a > best) {
-						best = a;
-						bi = r;
-					}
-				}
-				ip = block_argmax_first<T>(best, bi, s_idx, s_val);
+				ip = block_argmax_first1<T>(best, bi, s_idx, s_val);
+				if (ip >= pr) ip = j;  // no candidate compared above -1: a column of NaNs
 				if (ip != j && tid < 16) {
 					const T t = P[j * 17 + tid];
 					P[j * 17 + tid] = P[ip * 17 + tid];
@@ -394,34 +437,83 @@ __global__ void __launch_bounds__(NT) k_getrf_blk(SizeArg sz, MatArg<T> C, MatAr
 				d.d[c0 + j] = inv;
 				if (pv == T(0) && s_bad == 0) s_bad = c0 + j + 1;
 			}
-			for (int r = j + 1 + tid; r < pr; r += NT) P[r * 17 + j] *= inv;
-			__syncthreads();
-			const int nc = w - j - 1;
-			if (nc > 0) {
-				for (int e = tid; e < (pr - j - 1) * nc; e += NT) {
-					const int r = j + 1 + e / nc, l = j + 1 + e % nc;
-					P[r * 17 + l] = fma(-P[r * 17 + j], P[j * 17 + l], P[r * 17 + l]);
+			T urow[16];
+#pragma unroll
+			for (int l = 0; l < 16; l++) urow[l] = (l > j && l < w) ? P[j * 17 + l] : T(0);
+			best = T(-1);
+			bi = INT_MAX;
+			for (int r = j + 1 + tid; r < pr; r += NT) {
+				T *row = P + r * 17;
+				const T lj = row[j] * inv;
+				row[j] = lj;
+#pragma unroll
+				for (int l = 0; l < 16; l++)
+					if (l > j && l < w) row[l] = fma(-lj, urow[l], row[l]);
+				if (j + 1 < w) {
+					const T a = dev_abs(row[j + 1]);
+					if (a > best) {
+						best = a;
+						bi = r;
+					}
 				}
 			}
-			__syncthreads();
 		}
+		__syncthreads();
 		// c. panel back to global memory
 		for (int e = tid; e < pr * w; e += NT) {
 			const int r = e / w, j = e % w;
 			d.at(c0 + r, c0 + j) = P[r * 17 + j];
 		}
-		// d. the panel's row swaps on the other columns, in order
+		// d. the panel's row swaps on the other columns: the 16 swaps in order
+		// make one permutation of at most 32 rows.  cont[r] (shared, one int
+		// per panel row) starts as r; thread 0 runs the swaps on it; the rows
+		// that received another row's content (s_rows[k] gets the old row
+		// s_from[k]) are collected in parallel; each column thread then
+		// loads all of them before it stores any.
 		if (piv_on) {
+			for (int r = tid; r < pr; r += NT) cont[r] = r;
+			if (tid == 0) s_nmv = 0;
+			__syncthreads();
+			if (tid == 0) {
+				for (int j = 0; j < w; j++) {
+					const int r2 = s_piv[j] - c0;
+					if (r2 == j) continue;
+					const int t = cont[j];
+					cont[j] = cont[r2];
+					cont[r2] = t;
+				}
+			}
+			__syncthreads();
+			if (tid < 2 * w) {
+				// candidates: the panel rows, and the pivot rows below them
+				// (each once: the first j that names it)
+				int r = -1;
+				if (tid < w) {
+					r = tid;
+				} else {
+					const int r2 = s_piv[tid - w] - c0;
+					bool first = r2 >= w;
+					for (int j = 0; j < tid - w && first; j++)
+						if (s_piv[j] - c0 == r2) first = false;
+					if (first) r = r2;
+				}
+				if (r >= 0 && cont[r] != r) {
+					const int k = atomicAdd(&s_nmv, 1);
+					s_rows[k] = c0 + r;
+					s_from[k] = c0 + cont[r];
+				}
+			}
+			__syncthreads();
+			const int nmv = s_nmv;
 			for (int l = tid; l < n; l += NT) {
 				if (l >= c0 && l < c0 + w) continue;
-				for (int j = 0; j < w; j++) {
-					const int ip = s_piv[j];
-					if (ip != c0 + j) {
-						const T t = d.at(c0 + j, l);
-						d.at(c0 + j, l) = d.at(ip, l);
-						d.at(ip, l) = t;
-					}
-				}
+				T v[32];
+#pragma unroll
+				for (int k = 0; k < 32; k++)
+					if (k < nmv) v[k] = d.at(s_from[k], l);
+#pragma unroll
+				for (int k = 0; k < 32; k++)
+					if (k < nmv) d.at(s_rows[k], l) = v[k];
 			}
 		}
 		__syncthreads();
@@ -442,19 +534,32 @@ __global__ void __launch_bounds__(NT) k_getrf_blk(SizeArg sz, MatArg<T> C, MatAr
 			}
 		}
 		__syncthreads();
-		// f. A22 -= L21 U12 (rows c0 + w.., columns c0 + w..)
+		// f. A22 -= L21 U12 (rows c0 + w.., columns c0 + w..), a 4 x 4 tile per
+		// thread and step; the next tile's loads are issued before this one's
+		// products, so a thread always has one tile's L2 round trip in flight
 		const int rows = pr - w;
 		if (rows > 0 && nr > 0) {
-			const int ntr = (rows + 3) >> 2, ntc = (nr + 3) >> 2;
-			for (int t = tid; t < ntr * ntc; t += NT) {
+			const int ntr = (rows + 3) >> 2, ntc = (nr + 3) >> 2, ntt = ntr * ntc;
+			auto load_tile = [&](int t, T (&v)[4][4]) {
+				const int ti = t / ntc, tj = t % ntc;
+				const int r0 = w + 4 * ti, l0 = 4 * tj;
+#pragma unroll
+				for (int a = 0; a < 4; a++)
+#pragma unroll
+					for (int q = 0; q < 4; q++)
+						v[a][q] = (r0 + a < pr && l0 + q < nr) ? d.at(c0 + r0 + a, c0 + w + l0 + q) : T(0);
+			};
+			T nxt[4][4];
+			if (tid < ntt) load_tile(tid, nxt);
+			for (int t = tid; t < ntt; t += NT) {
 				const int ti = t / ntc, tj = t % ntc;
 				const int r0 = w + 4 * ti, l0 = 4 * tj;
 				T acc[4][4];
 #pragma unroll
 				for (int a = 0; a < 4; a++)
 #pragma unroll
-					for (int q = 0; q < 4; q++)
-						acc[a][q] = (r0 + a < pr && l0 + q < nr) ? d.at(c0 + r0 + a, c0 + w + l0 + q) : T(0);
+					for (int q = 0; q < 4; q++) acc[a][q] = nxt[a][q];
+				if (t + NT < ntt) load_tile(t + NT, nxt);
 #pragma unroll
 				for (int k = 0; k < 16; k++) {
 					T av[4], bv[4];
@@ -858,9 +963,11 @@ int syrk_potrf_batch(int batch, int m, int k, BT *sA, int ai, int aj, BT *sB, in
 	return bf::potrf_launch<T>(batch, uniform_sizes(m, m, 0), m, D, D, info, s, -1);
 }
 
-// variant: -1 auto; 0..2: global memory only, 128/256/512 threads; 3..5: the
-// instances whose block fits in shared memory there (128/256/512 threads),
-// the others in global memory (a second launch, 512 threads).
+// variant: -1 auto; 0..2: the blocked global-memory kernels (getrf: 128
+// threads with 4 or 2 blocks per SM, 256 threads; geqrf: 128/256/512
+// threads); 3..5: the instances whose block fits in shared memory there
+// (128/256/512 threads), the others in the blocked global-memory kernel (a
+// second launch, 256 threads).
 template <typename T, int NT, bool SMEM>
 void launch_getrf(int batch, SizeArg sz, int cap, size_t smem, MatArg<T> C, MatArg<T> D, int *ipiv,
                   long long ipiv_stride, int *info, cudaStream_t s, bool piv = true) {
@@ -871,11 +978,11 @@ void launch_getrf(int batch, SizeArg sz, int cap, size_t smem, MatArg<T> C, MatA
 
 // blocked global-memory LU (k_getrf_blk) for the instances that do not fit
 // shared memory (cap >= 0) or for all of them (cap < 0)
-template <typename T, int NT>
+template <typename T, int NT, int MINB>
 void launch_getrf_blk(int batch, SizeArg sz, int cap, int max_m, int max_n, MatArg<T> C, MatArg<T> D, int *ipiv,
                       long long ipiv_stride, int *info, cudaStream_t s, bool piv = true) {
-	auto kern = k_getrf_blk<T, NT>;
-	const size_t smem = ((size_t)(max_m + 4) * 17 + (size_t)16 * (max_n + 4)) * sizeof(T);
+	auto kern = k_getrf_blk<T, NT, MINB>;
+	const size_t smem = ((size_t)(max_m + 4) * 17 + (size_t)16 * (max_n + 4)) * sizeof(T) + (size_t)(max_m + 4) * sizeof(int);
 	if (smem > bf::max_smem_optin()) {
 		// panel and U12 beyond shared memory (blocks of more than ~1,500 rows):
 		// the unblocked global-memory kernel
@@ -913,15 +1020,16 @@ inline size_t lu_smem_bytes(int max_m, int max_n, size_t esz) {
 
 // built-in rule for getrf (qr = false) and geqrf (qr = true), from uniform
 // batches timed on the B200 at n = 32..384: the shared-memory kernel with 128
-// threads for small blocks, the blocked global-memory kernels above (128,
-// 256 or 512 threads by size)
+// threads for small blocks, the blocked global-memory kernels above (getrf:
+// 128 threads with 4 blocks per SM up to n = 160, with 2 up to 224, then 256
+// threads; geqrf: 128, 256 or 512 threads by size)
 inline int pick_lu_variant(int variant, int max_m, int max_n, bool qr = false) {
 	if (variant < 0) {
 		const int mx = max_m > max_n ? max_m : max_n;
 		if (mx <= 48)
 			variant = 3;
 		else if (!qr)
-			variant = mx <= 192 ? 0 : 1;
+			variant = mx <= 160 ? 0 : (mx <= 224 ? 1 : 2);
 		else
 			variant = mx <= 128 ? 0 : (mx <= 256 ? 1 : 2);
 	}
@@ -937,15 +1045,16 @@ int getrf_launch(int batch, SizeArg sz, MatArg<T> C, MatArg<T> D, int *ipiv, lon
 	const int cap = (int)smem;
 	variant = pick_lu_variant(variant, max_m, max_n);
 	switch (variant) {
-	case 0: launch_getrf_blk<T, 128>(batch, sz, -1, max_m, max_n, C, D, ipiv, ipiv_stride, info, s, piv); break;
-	case 1: launch_getrf_blk<T, 256>(batch, sz, -1, max_m, max_n, C, D, ipiv, ipiv_stride, info, s, piv); break;
-	case 2: launch_getrf_blk<T, 512>(batch, sz, -1, max_m, max_n, C, D, ipiv, ipiv_stride, info, s, piv); break;
+	// blocked: 128 threads with 4 or 2 blocks per SM (register cap), 256 threads
+	case 0: launch_getrf_blk<T, 128, 4>(batch, sz, -1, max_m, max_n, C, D, ipiv, ipiv_stride, info, s, piv); break;
+	case 1: launch_getrf_blk<T, 128, 2>(batch, sz, -1, max_m, max_n, C, D, ipiv, ipiv_stride, info, s, piv); break;
+	case 2: launch_getrf_blk<T, 256, 1>(batch, sz, -1, max_m, max_n, C, D, ipiv, ipiv_stride, info, s, piv); break;
 	case 3: launch_getrf<T, 128, true>(batch, sz, cap, smem, C, D, ipiv, ipiv_stride, info, s, piv); break;
 	case 4: launch_getrf<T, 256, true>(batch, sz, cap, smem, C, D, ipiv, ipiv_stride, info, s, piv); break;
 	default: launch_getrf<T, 512, true>(batch, sz, cap, smem, C, D, ipiv, ipiv_stride, info, s, piv); break;
 	}
 	if (variant >= 3 && need > smem)
-		launch_getrf_blk<T, 256>(batch, sz, cap, max_m, max_n, C, D, ipiv, ipiv_stride, info, s, piv);
+		launch_getrf_blk<T, 256, 1>(batch, sz, cap, max_m, max_n, C, D, ipiv, ipiv_stride, info, s, piv);
 	return bf::check_launch();
 }
 

@@ -416,7 +416,10 @@ int blasfeo_dgeqrf_vbatch(int batch, const int *m, const int *n, int max_m, int 
  * op 1 potrf_l: 0..3 shared memory with 64/128/256/512 threads, 4 global
  *   memory, 5 one warp per instance on the FP64 tensor cores (max_m <= 64;
  *   larger batches take the heuristic);
- * op 2 getrf_rp and 3 geqrf: global or shared memory, 128/256/512 threads.
+ * op 2 getrf_rp: 0..2 blocked in global memory (128 threads with 4 or 2
+ *   blocks per SM, 256 threads), 3..5 shared memory with 128/256/512 threads;
+ * op 3 geqrf: 0..2 blocked in global memory with 128/256/512 threads, 3..5
+ *   shared memory with 128/256/512 threads.
  * Variants change the schedule and, through the summation order of the dot
  * products, the rounding of an element; every variant meets the routine's
  * tolerance against the reference (pivot choices of getrf are identical). */
