@@ -688,8 +688,11 @@ __global__ void __launch_bounds__(NT) k_geqrf(SizeArg sz, MatArg<T> C, MatArg<T>
 //   c. panel and tau go back to global memory;
 //   d. T (upper triangular, H_0 H_1 .. H_15 = I - V T V^T) from V^T V:
 //      T_jj = tau_j, T_{0:j,j} = -tau_j T_{0:j,0:j} (V^T v_j)_{0:j};
+//      (lane k of warp 0 computes row k of T: the rows are independent);
 //   e. the trailing columns C = A(c0:m, c0+16:n) become Q^T C = C - V T^T (V^T C),
-//      one thread per column, four rows (one panel-layout sector) at a time.
+//      a warp per pair of columns with its lanes over the rows (V^T C by
+//      butterfly sums; the update's next rows loaded before the current ones
+//      are stored).
 // Shared memory: (m + 4) x 17 panel, 16 x 17 T and V^T V.
 template <typename T, int NT>
 __global__ void __launch_bounds__(NT) k_geqrf_blk(SizeArg sz, MatArg<T> C, MatArg<T> D, int smem_cap, int max_m) {
@@ -774,72 +777,113 @@ __global__ void __launch_bounds__(NT) k_geqrf_blk(SizeArg sz, MatArg<T> C, MatAr
 		}
 		const int nr = n - c0 - w;
 		if (nr > 0) {
-			// d. G = V^T V (strictly upper part), V unit lower trapezoidal in P
-			for (int pq = warp; pq < 16 * 16; pq += nw) {
-				const int k = pq >> 4, j = pq & 15;
-				if (!(k < j && j < w)) continue;
-				T g = T(0);
-				for (int r = j + 1 + lane; r < pr; r += 32) g = fma(P[r * 17 + k], P[r * 17 + j], g);
+			// d. G = V^T V (strictly upper part), V unit lower trapezoidal in P:
+			// a warp per column j, its lanes over the rows r >= j, all k < j at
+			// once, butterfly sums
+			for (int j = 1 + warp; j < w; j += nw) {
+				T g[16];
 #pragma unroll
-				for (int off = 16; off > 0; off >>= 1) g += __shfl_xor_sync(0xffffffffu, g, off);
-				if (lane == 0) G[k * 17 + j] = g + P[j * 17 + k];
+				for (int k = 0; k < 16; k++) g[k] = T(0);
+				for (int r = j + lane; r < pr; r += 32) {
+					const T vj = (r == j) ? T(1) : P[r * 17 + j];
+#pragma unroll
+					for (int k = 0; k < 16; k++)
+						if (k < j) g[k] = fma(P[r * 17 + k], vj, g[k]);
+				}
+#pragma unroll
+				for (int k = 0; k < 16; k++)
+#pragma unroll
+					for (int off = 16; off > 0; off >>= 1) g[k] += __shfl_xor_sync(0xffffffffu, g[k], off);
+				if (lane == 0) {
+#pragma unroll
+					for (int k = 0; k < 16; k++)
+						if (k < j) G[k * 17 + j] = g[k];
+				}
 			}
 			__syncthreads();
-			if (tid == 0) {
+			// T row by row: lane k of warp 0 owns row k (T_kj for j >= k
+			// depends only on row k and on G), so the 16 rows are independent
+			if (tid < 16) {
+				const int k = tid;
+				T t[16];
+#pragma unroll
 				for (int j = 0; j < 16; j++) {
 					const T tj = (j < w) ? tau[c0 + j] : T(0);
-					for (int k = 0; k < j; k++) {
-						T z = T(0);
-						for (int q = k; q < j; q++) z = fma(Tm[k * 17 + q], G[q * 17 + j], z);
-						Tm[k * 17 + j] = -tj * z;
-					}
-					Tm[j * 17 + j] = tj;
-					for (int k = j + 1; k < 16; k++) Tm[k * 17 + j] = T(0);
-				}
-			}
-			__syncthreads();
-			// e. C = C - V T^T (V^T C), one thread per trailing column
-			for (int l = tid; l < nr; l += NT) {
-				const int col = c0 + w + l;
-				T wk[16];
-#pragma unroll
-				for (int k = 0; k < 16; k++) wk[k] = T(0);
-				for (int r0 = 0; r0 < pr; r0 += 4) {
-					T cv[4];
-#pragma unroll
-					for (int a = 0; a < 4; a++) cv[a] = (r0 + a < pr) ? d.at(c0 + r0 + a, col) : T(0);
-#pragma unroll
-					for (int a = 0; a < 4; a++) {
-						const int r = r0 + a;
-#pragma unroll
-						for (int k = 0; k < 16; k++) {
-							// V(r, k): 1 on the diagonal, the stored vector below, 0 above
-							const T v = (r > k) ? P[r * 17 + k] : ((r == k) ? T(1) : T(0));
-							wk[k] = fma(v, cv[a], wk[k]);
-						}
-					}
-				}
-				T wt[16];
-#pragma unroll
-				for (int k = 0; k < 16; k++) {
 					T z = T(0);
 #pragma unroll
-					for (int q = 0; q <= k; q++) z = fma(Tm[q * 17 + k], wk[q], z);
-					wt[k] = z;
+					for (int q = 0; q < j; q++)
+						if (q >= k) z = fma(t[q], G[q * 17 + j], z);
+					// columns j >= w hold no reflector: exact zeros (G there is stale)
+					t[j] = (j >= w || j < k) ? T(0) : ((j == k) ? tj : -tj * z);
 				}
-				for (int r0 = 0; r0 < pr; r0 += 4) {
 #pragma unroll
-					for (int a = 0; a < 4; a++) {
-						const int r = r0 + a;
-						if (r >= pr) break;
-						T cvl = d.at(c0 + r, col);
+				for (int j = 0; j < 16; j++) Tm[k * 17 + j] = t[j];
+			}
+			__syncthreads();
+			// e. C = C - V T^T (V^T C): a warp per pair of trailing columns, its
+			// lanes over the rows; w = V^T c by butterfly sums, then w <- T^T w
+			// in place, then c -= V w with the next rows' loads issued before
+			// the current rows' stores
+			for (int l0 = 2 * warp; l0 < nr; l0 += 2 * nw) {
+				const bool two = l0 + 1 < nr;
+				const int col0 = c0 + w + l0, col1 = col0 + (two ? 1 : 0);
+				T w0[16], w1[16];
 #pragma unroll
-						for (int k = 0; k < 16; k++) {
-							const T v = (r > k) ? P[r * 17 + k] : ((r == k) ? T(1) : T(0));
-							cvl = fma(-v, wt[k], cvl);
-						}
-						d.at(c0 + r, col) = cvl;
+				for (int k = 0; k < 16; k++) w0[k] = w1[k] = T(0);
+#pragma unroll 2
+				for (int r = lane; r < pr; r += 32) {
+					const T a0 = d.at(c0 + r, col0), a1 = d.at(c0 + r, col1);
+#pragma unroll
+					for (int k = 0; k < 16; k++) {
+						// V(r, k): 1 on the diagonal, the stored vector below, 0 above
+						const T v = (r > k) ? P[r * 17 + k] : ((r == k) ? T(1) : T(0));
+						w0[k] = fma(v, a0, w0[k]);
+						w1[k] = fma(v, a1, w1[k]);
 					}
+				}
+#pragma unroll
+				for (int k = 0; k < 16; k++)
+#pragma unroll
+					for (int off = 16; off > 0; off >>= 1) {
+						w0[k] += __shfl_xor_sync(0xffffffffu, w0[k], off);
+						w1[k] += __shfl_xor_sync(0xffffffffu, w1[k], off);
+					}
+#pragma unroll
+				for (int k = 15; k >= 0; k--) {
+					T z0 = T(0), z1 = T(0);
+#pragma unroll
+					for (int q = 0; q <= k; q++) {
+						const T tq = Tm[q * 17 + k];
+						z0 = fma(tq, w0[q], z0);
+						z1 = fma(tq, w1[q], z1);
+					}
+					w0[k] = z0;
+					w1[k] = z1;
+				}
+				int r = lane;
+				T a0 = T(0), a1 = T(0);
+				if (r < pr) {
+					a0 = d.at(c0 + r, col0);
+					a1 = d.at(c0 + r, col1);
+				}
+				while (r < pr) {
+					const int rn = r + 32;
+					T n0 = T(0), n1 = T(0);
+					if (rn < pr) {
+						n0 = d.at(c0 + rn, col0);
+						n1 = d.at(c0 + rn, col1);
+					}
+#pragma unroll
+					for (int k = 0; k < 16; k++) {
+						const T v = (r > k) ? P[r * 17 + k] : ((r == k) ? T(1) : T(0));
+						a0 = fma(-v, w0[k], a0);
+						a1 = fma(-v, w1[k], a1);
+					}
+					d.at(c0 + r, col0) = a0;
+					if (two) d.at(c0 + r, col1) = a1;
+					a0 = n0;
+					a1 = n1;
+					r = rn;
 				}
 			}
 		}
@@ -1022,7 +1066,7 @@ inline size_t lu_smem_bytes(int max_m, int max_n, size_t esz) {
 // batches timed on the B200 at n = 32..384: the shared-memory kernel with 128
 // threads for small blocks, the blocked global-memory kernels above (getrf:
 // 128 threads with 4 blocks per SM up to n = 160, with 2 up to 224, then 256
-// threads; geqrf: 128, 256 or 512 threads by size)
+// threads; geqrf: shared memory up to 64 rows, then 256 or 512 threads)
 inline int pick_lu_variant(int variant, int max_m, int max_n, bool qr = false) {
 	if (variant < 0) {
 		const int mx = max_m > max_n ? max_m : max_n;
@@ -1031,7 +1075,7 @@ inline int pick_lu_variant(int variant, int max_m, int max_n, bool qr = false) {
 		else if (!qr)
 			variant = mx <= 160 ? 0 : (mx <= 224 ? 1 : 2);
 		else
-			variant = mx <= 128 ? 0 : (mx <= 256 ? 1 : 2);
+			variant = mx <= 64 ? 3 : (mx <= 192 ? 1 : 2);
 	}
 	return variant;
 }
