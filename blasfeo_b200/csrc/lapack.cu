@@ -336,6 +336,30 @@ __global__ void __launch_bounds__(NT) k_getrf(SizeArg sz, MatArg<T> C, MatArg<T>
 	if (info && tid == 0) info[b] = s_bad;
 }
 
+// 4 consecutive elements at an address aligned to 4 elements (a panel-layout
+// column run of 4 rows), as vector accesses
+__device__ __forceinline__ void ld_run4(const double *p, double &a, double &b, double &c, double &d) {
+	const double2 x = *reinterpret_cast<const double2 *>(p), y = *reinterpret_cast<const double2 *>(p + 2);
+	a = x.x;
+	b = x.y;
+	c = y.x;
+	d = y.y;
+}
+__device__ __forceinline__ void ld_run4(const float *p, float &a, float &b, float &c, float &d) {
+	const float4 x = *reinterpret_cast<const float4 *>(p);
+	a = x.x;
+	b = x.y;
+	c = x.z;
+	d = x.w;
+}
+__device__ __forceinline__ void st_run4(double *p, double a, double b, double c, double d) {
+	*reinterpret_cast<double2 *>(p) = make_double2(a, b);
+	*reinterpret_cast<double2 *>(p + 2) = make_double2(c, d);
+}
+__device__ __forceinline__ void st_run4(float *p, float a, float b, float c, float d) {
+	*reinterpret_cast<float4 *>(p) = make_float4(a, b, c, d);
+}
+
 // LU with row pivoting of one instance per CTA whose block stays in global
 // memory (L2), blocked by 16-column panels (the reference's HP driver is
 // blocked too: kernel_dgetrf_pivot panels and kernel_dgemm_nn corrections,
@@ -519,17 +543,29 @@ __global__ void __launch_bounds__(NT, MINB) k_getrf_blk(SizeArg sz, MatArg<T> C,
 		__syncthreads();
 		// e. U12 = L11^{-1} A12 (unit lower L11)
 		const int nr = n - c0 - w;
+		// a full panel's 16 rows of a column are 4 aligned runs of 4 when the
+		// panel starts on a panel boundary: vector accesses then
+		const bool vecu = w == 16 && ((d.ri + c0) & 3) == 0 && ((uintptr_t)d.p & 15) == 0;
 		for (int l = tid; l < nr; l += NT) {
 			T u[16];
+			if (vecu) {
 #pragma unroll
-			for (int k = 0; k < 16; k++) u[k] = (k < w) ? d.at(c0 + k, c0 + w + l) : T(0);
+				for (int k = 0; k < 16; k += 4) ld_run4(d.addr(c0 + k, c0 + w + l), u[k], u[k + 1], u[k + 2], u[k + 3]);
+			} else {
+#pragma unroll
+				for (int k = 0; k < 16; k++) u[k] = (k < w) ? d.at(c0 + k, c0 + w + l) : T(0);
+			}
 #pragma unroll
 			for (int k = 1; k < 16; k++)
 #pragma unroll
 				for (int kk = 0; kk < k; kk++) u[k] = fma(-P[k * 17 + kk], u[kk], u[k]);
+			if (vecu) {
+#pragma unroll
+				for (int k = 0; k < 16; k += 4) st_run4(d.addr(c0 + k, c0 + w + l), u[k], u[k + 1], u[k + 2], u[k + 3]);
+			}
 #pragma unroll
 			for (int k = 0; k < 16; k++) {
-				if (k < w) d.at(c0 + k, c0 + w + l) = u[k];
+				if (!vecu && k < w) d.at(c0 + k, c0 + w + l) = u[k];
 				Us[k * usld + (l & 3) * q4 + (l >> 2)] = (k < w) ? u[k] : T(0);
 			}
 		}
@@ -540,9 +576,24 @@ __global__ void __launch_bounds__(NT, MINB) k_getrf_blk(SizeArg sz, MatArg<T> C,
 		const int rows = pr - w;
 		if (rows > 0 && nr > 0) {
 			const int ntr = (rows + 3) >> 2, ntc = (nr + 3) >> 2, ntt = ntr * ntc;
+			// a tile's 4 rows of one column are one aligned 4-element run of the
+			// panel layout when its first row is on a panel boundary (tile rows
+			// start at c0 + w + 4 ti) and pA is 16-byte aligned: vector loads
+			// and stores then (full tiles), element by element otherwise
+			const bool vec = ((d.ri + c0 + w) & 3) == 0 && ((uintptr_t)d.p & 15) == 0;
 			auto load_tile = [&](int t, T (&v)[4][4]) {
 				const int ti = t / ntc, tj = t % ntc;
 				const int r0 = w + 4 * ti, l0 = 4 * tj;
+				if (vec && r0 + 4 <= pr) {
+#pragma unroll
+					for (int q = 0; q < 4; q++) {
+						if (l0 + q < nr)
+							ld_run4(d.addr(c0 + r0, c0 + w + l0 + q), v[0][q], v[1][q], v[2][q], v[3][q]);
+						else
+							v[0][q] = v[1][q] = v[2][q] = v[3][q] = T(0);
+					}
+					return;
+				}
 #pragma unroll
 				for (int a = 0; a < 4; a++)
 #pragma unroll
@@ -572,11 +623,17 @@ __global__ void __launch_bounds__(NT, MINB) k_getrf_blk(SizeArg sz, MatArg<T> C,
 #pragma unroll
 						for (int q = 0; q < 4; q++) acc[a][q] = fma(-av[a], bv[q], acc[a][q]);
 				}
-#pragma unroll
-				for (int a = 0; a < 4; a++)
+				if (vec && r0 + 4 <= pr) {
 #pragma unroll
 					for (int q = 0; q < 4; q++)
-						if (r0 + a < pr && l0 + q < nr) d.at(c0 + r0 + a, c0 + w + l0 + q) = acc[a][q];
+						if (l0 + q < nr) st_run4(d.addr(c0 + r0, c0 + w + l0 + q), acc[0][q], acc[1][q], acc[2][q], acc[3][q]);
+				} else {
+#pragma unroll
+					for (int a = 0; a < 4; a++)
+#pragma unroll
+						for (int q = 0; q < 4; q++)
+							if (r0 + a < pr && l0 + q < nr) d.at(c0 + r0 + a, c0 + w + l0 + q) = acc[a][q];
+				}
 			}
 		}
 		__syncthreads();
