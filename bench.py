@@ -69,7 +69,7 @@ def parse():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--no-fp64", action="store_true", help="skip the FP64 batched dgemm/dpotrf roofline legs")
     ap.add_argument("--case", nargs="+", metavar="ARG",
-                    help="run one profiling case instead of the benchmark: OP N BATCH REPS [NMIN]")
+                    help="run one profiling case instead of the benchmark: OP N BATCH REPS [NMIN | M]")
     return ap.parse_args()
 
 
@@ -162,14 +162,16 @@ def run_case(argv):
         torch.cuda.synchronize()
         assert bool((info == 0).all().item())
     elif op in ("getrf", "geqrf"):
-        A, D = bf.DMatBatch(n, n, batch), bf.DMatBatch(n, n, batch)
-        fill_batch(A, torch.rand((batch, n, n), dtype=torch.float64, device=dev) * 2 - 1)
-        ipiv = torch.zeros(batch * n, dtype=torch.int32, device=dev)
+        # m x n instances (m = the optional fifth argument, default n)
+        m = int(argv[4]) if len(argv) > 4 else n
+        A, D = bf.DMatBatch(m, n, batch), bf.DMatBatch(m, n, batch)
+        fill_batch(A, torch.rand((batch, m, n), dtype=torch.float64, device=dev) * 2 - 1)
+        ipiv = torch.zeros(batch * min(m, n), dtype=torch.int32, device=dev)
         for _ in range(reps):
             if op == "getrf":
-                bf.check(lib.blasfeo_dgetrf_rp_batch(batch, n, n, A.ref, 0, 0, D.ref, 0, 0, P(ipiv), None, None))
+                bf.check(lib.blasfeo_dgetrf_rp_batch(batch, m, n, A.ref, 0, 0, D.ref, 0, 0, P(ipiv), None, None))
             else:
-                bf.check(lib.blasfeo_dgeqrf_batch(batch, n, n, A.ref, 0, 0, D.ref, 0, 0, None))
+                bf.check(lib.blasfeo_dgeqrf_batch(batch, m, n, A.ref, 0, 0, D.ref, 0, 0, None))
     elif op in ("chain", "chain_il"):
         from blasfeo_b200.api import DMatBatchIL
         g = torch.Generator(device=dev)
@@ -595,8 +597,15 @@ def main():
     bytes_pass = W.lower_bytes()
     flops = W.chol_flops()
     achieved = bytes_pass / (ms_mixed * 1e-3) / 1e9
+    # DRAM bytes of one call: ncu capture of the same call on 2,000 systems of
+    # this distribution (summary under profiles/, k_posv_f32_cfg3_2000_dram):
+    # 185,386,240 B of DRAM traffic against 178,497,336 algorithmic bytes,
+    # scaled to this call by its algorithmic bytes
+    traffic = bytes_pass * (185386240.0 / 178497336.0)
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak_bw, "unit": "GB/s", "frac": achieved / peak_bw,
-                "traffic": None, "peak_source": peak_src,
+                "traffic": traffic, "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of the same "
+                "call on 2,000 systems of the distribution, scaled by algorithmic bytes (ratio 1.039)",
+                "peak_source": peak_src,
                 "kernel": "k_posv<float,true> (all size classes of one blasfeo_dsposv_l_vbatch call)",
                 "algorithmic_bytes_per_launch": bytes_pass,
                 "fp32_simt": {"achieved_gflops": flops / (ms_mixed * 1e-3) / 1e9, "peak_gflops": fp32_peak,
@@ -797,6 +806,32 @@ def single_dropin(torch, stream, fp64_peak, peak_bw):
         torch.cuda.synchronize()
         out["graph_3calls_us"] = e0.elapsed_time(e1) * 1e3 / reps
         del g
+        # the measured floor: the same timing of an empty kernel launched from
+        # Python, and the potrf through every kernel variant of the batched
+        # routine with one instance (0-3: a CTA of 64-512 threads per instance,
+        # 4: global memory, 5: one warp on the FP64 tensor cores)
+        def tm_async(f, r=reps):
+            for _ in range(50):
+                f()
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            for _ in range(r):
+                f()
+            e1.record(stream)
+            torch.cuda.synchronize()
+            return e0.elapsed_time(e1) * 1e3 / r
+        with torch.cuda.stream(stream):
+            out["empty_kernel_us"] = tm_async(lambda: torch.cuda._sleep(0))
+        from blasfeo_b200.api import descriptor_array
+        arrS, arrL = descriptor_array([dS]), descriptor_array([dL])
+        nv = torch.tensor([n], dtype=torch.int32, device=dS.buf.device)
+        sh = C.c_void_p(stream.cuda_stream)
+        out["dpotrf_l_64_by_variant_us"] = {
+            str(v): tm_async(lambda: lib.blasfeo_dpotrf_l_vbatch_variant(1, C.c_void_p(nv.data_ptr()), n,
+                                                                         C.c_void_p(arrS.data_ptr()),
+                                                                         C.c_void_p(arrL.data_ptr()), None, v, sh))
+            for v in range(int(lib.blasfeo_b200_num_variants(1)))}
     finally:
         bf.set_sync(True)
         bf.set_stream(None)
