@@ -1387,29 +1387,9 @@ def run_e2e(args, W, lib, torch, dev, stream, barrier, world):
     """Mixed path with all inputs in pinned host memory (mapped into the GPU's
     address space): blasfeo_dsposv_l_vbatch_mapped reads the lower triangles
     over the host link and writes x to host memory."""
-    from blasfeo_b200.workloads import DESC_DTYPE, VDESC_DTYPE
     P = lambda t: C.c_void_p(t.data_ptr())
-    hslab = torch.empty(W.slab.numel(), dtype=torch.float64, pin_memory=True)
-    hslab.copy_(W.slab)
-    hb = torch.empty(W.b.numel(), dtype=torch.float64, pin_memory=True)
-    hb.copy_(W.b)
-    hx = torch.zeros_like(hb).pin_memory()
-    hn = torch.from_numpy(W.ns.copy()).pin_memory()
-    d = W.desc.cpu().numpy().view(DESC_DTYPE).copy()
-    shift = hslab.data_ptr() - W.slab.data_ptr()
-    for f in ("mem", "pA", "dA"):
-        d[f] = d[f] + np.uint64(shift) if shift >= 0 else d[f] - np.uint64(-shift)
-    hdesc = torch.from_numpy(d.view(np.uint8).copy()).pin_memory()
-
-    def vd(t):
-        v = np.zeros(len(W.ns), dtype=VDESC_DTYPE)
-        v["mem"] = t.data_ptr() + W.voff * 8
-        v["pa"] = t.data_ptr() + W.voff * 8
-        v["m"] = W.ns
-        v["pm"] = W.vlen
-        v["memsize"] = W.vlen * 8
-        return torch.from_numpy(v.view(np.uint8).copy()).pin_memory()
-    hbd, hxd = vd(hb), vd(hx)
+    H = W.mapped_copy()
+    hx, hn, hdesc, hbd, hxd = H.x, H.n, H.desc, H.bdesc, H.xdesc
     hinfo = torch.zeros(args.num, dtype=torch.int32).pin_memory()
     sh = C.c_void_p(stream.cuda_stream)
 

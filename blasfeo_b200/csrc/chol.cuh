@@ -15,18 +15,18 @@
 //
 // Algorithm: right-looking, 16 columns (4 panels) per block step, two
 // __syncthreads per step:
-//   A. all threads: panel of block column K as a product with the explicit
-//      inverse of the diagonal block, L_IK = A_IK inv(L_KK)^T (no sequential
-//      dependence inside a row);
-//   B. warp 0 (critical path): rank-16 update of the 16x16 diagonal block K+1,
-//      its factorization in FP64 registers (pivot rule of
+//   A. all threads: panel of block column K by substitution with the
+//      factored diagonal block (one row per thread, the reciprocal pivots
+//      multiplied in);
+//   B. warp 0 (critical path): rank-16 update of the 16x16 diagonal block K+1
+//      and its factorization in FP64 registers (pivot rule of
 //      kernel/generic/kernel_dgemm_4x4_lib4.c:5700-5710: c>0 -> sqrt(c) and its
-//      reciprocal, else 0 and 0) and its explicit inverse in FP64;
-//      the warps on the other three schedulers: rank-16 update of the rest of
-//      the trailing matrix (one 4x4 tile per thread), which hides the serial
-//      diagonal work.
-// The inverses of the diagonal blocks are kept (invL_all) for the triangular
-// solves of the refinement loop.
+//      reciprocal, else 0 and 0); the warps on the other three schedulers:
+//      rank-16 update of the rest of the trailing matrix (8 x 4 tile blocks
+//      per warp), which hides the serial diagonal work.
+// With inv_diag the diagonal blocks are replaced at the end by their explicit
+// inverses (FP64 arithmetic, all blocks in parallel) for the blocked
+// triangular solves of the factor+solve kernels.
 #pragma once
 #include "common.cuh"
 

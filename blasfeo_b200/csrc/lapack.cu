@@ -336,6 +336,15 @@ __global__ void __launch_bounds__(NT) k_getrf(SizeArg sz, MatArg<T> C, MatArg<T>
 	if (info && tid == 0) info[b] = s_bad;
 }
 
+// D = A B + D on the FP64 tensor cores (mma.sync m8n8k4 f64): per lane one
+// element of A (row lane/4, column lane%4), one of B (row lane%4, column
+// lane/4) and two of D (row lane/4, columns 2 (lane%4) and 2 (lane%4) + 1)
+__device__ __forceinline__ void lu_dmma(double &d0, double &d1, double a, double b) {
+	asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};"
+	             : "+d"(d0), "+d"(d1)
+	             : "d"(a), "d"(b));
+}
+
 // 4 consecutive elements at an address aligned to 4 elements (a panel-layout
 // column run of 4 rows), as vector accesses
 __device__ __forceinline__ void ld_run4(const double *p, double &a, double &b, double &c, double &d) {
@@ -570,11 +579,62 @@ __global__ void __launch_bounds__(NT, MINB) k_getrf_blk(SizeArg sz, MatArg<T> C,
 			}
 		}
 		__syncthreads();
-		// f. A22 -= L21 U12 (rows c0 + w.., columns c0 + w..), a 4 x 4 tile per
-		// thread and step; the next tile's loads are issued before this one's
-		// products, so a thread always has one tile's L2 round trip in flight
+		// f. A22 -= L21 U12 (rows c0 + w.., columns c0 + w..).  FP64: a 32 x 32
+		// tile per warp as 4 x 4 DMMA fragments, L21 from the panel and U12 from
+		// shared memory (one fragment load per 256 products), C from and back
+		// to global memory.  FP32: a 4 x 4 tile per thread and step; the next
+		// tile's loads are issued before this one's products, so a thread
+		// always has one tile's L2 round trip in flight
 		const int rows = pr - w;
-		if (rows > 0 && nr > 0) {
+		if constexpr (sizeof(T) == 8) {
+			if (rows > 0 && nr > 0) {
+				const int nrt = (rows + 31) >> 5, nct = (nr + 31) >> 5;
+				const int lane = tid & 31, warp = tid >> 5, nw = NT >> 5;
+				const int g = lane >> 2, tq = lane & 3;
+				for (int t = warp; t < nrt * nct; t += nw) {
+					const int r0 = w + 32 * (t / nct), l0 = 32 * (t % nct);
+					double acc[4][4][2];
+#pragma unroll
+					for (int rb = 0; rb < 4; rb++) {
+						const int row = r0 + 8 * rb + g;
+#pragma unroll
+						for (int cb = 0; cb < 4; cb++) {
+							const int col = l0 + 8 * cb + 2 * tq;
+							acc[rb][cb][0] = (row < pr && col < nr) ? d.at(c0 + row, c0 + w + col) : 0.0;
+							acc[rb][cb][1] = (row < pr && col + 1 < nr) ? d.at(c0 + row, c0 + w + col + 1) : 0.0;
+						}
+					}
+#pragma unroll
+					for (int ks = 0; ks < 4; ks++) {
+						double a[4], bb[4];
+#pragma unroll
+						for (int rb = 0; rb < 4; rb++) {
+							const int row = r0 + 8 * rb + g;
+							a[rb] = (row < pr) ? -(double)P[row * 17 + 4 * ks + tq] : 0.0;
+						}
+#pragma unroll
+						for (int cb = 0; cb < 4; cb++) {
+							const int col = l0 + 8 * cb + g;
+							bb[cb] = (col < nr) ? (double)Us[(4 * ks + tq) * usld + (col & 3) * q4 + (col >> 2)] : 0.0;
+						}
+#pragma unroll
+						for (int rb = 0; rb < 4; rb++)
+#pragma unroll
+							for (int cb = 0; cb < 4; cb++) lu_dmma(acc[rb][cb][0], acc[rb][cb][1], a[rb], bb[cb]);
+					}
+#pragma unroll
+					for (int rb = 0; rb < 4; rb++) {
+						const int row = r0 + 8 * rb + g;
+#pragma unroll
+						for (int cb = 0; cb < 4; cb++) {
+							const int col = l0 + 8 * cb + 2 * tq;
+							if (row < pr && col < nr) d.at(c0 + row, c0 + w + col) = (T)acc[rb][cb][0];
+							if (row < pr && col + 1 < nr) d.at(c0 + row, c0 + w + col + 1) = (T)acc[rb][cb][1];
+						}
+					}
+				}
+			}
+		} else if (rows > 0 && nr > 0) {
 			const int ntr = (rows + 3) >> 2, ntc = (nr + 3) >> 2, ntt = ntr * ntc;
 			// a tile's 4 rows of one column are one aligned 4-element run of the
 			// panel layout when its first row is on a panel boundary (tile rows

@@ -114,6 +114,11 @@ class SpdBatch:
         P = self.slab[o:o + pm * pm].reshape(1, -1)
         return from_panel_major(P, n, n, pm, pm)[0].cpu().numpy()
 
+    def mapped_copy(self):
+        """The same systems in pinned host memory (for blasfeo_dsposv_l_vbatch_mapped):
+        matrices, b, x, sizes and descriptors, every pointer a host address."""
+        return MappedSpdBatch(self)
+
     def lower_bytes(self):
         """Algorithmic HBM bytes of one solve pass: lower triangle of A, b and x (FP64)."""
         n = self.ns.astype(np.int64)
@@ -122,6 +127,40 @@ class SpdBatch:
     def chol_flops(self):
         n = self.ns.astype(np.float64)
         return float((n ** 3 / 3 + n ** 2 / 2 + n / 6 + 4 * n ** 2).sum())
+
+
+class MappedSpdBatch:
+    """Pinned host copy of an SpdBatch: slab, b, x, n and the descriptor arrays
+    (struct blasfeo_dmat / blasfeo_dvec with host pointers)."""
+
+    def __init__(self, W):
+        import torch
+        self.slab = torch.empty(W.slab.numel(), dtype=torch.float64, pin_memory=True)
+        self.slab.copy_(W.slab)
+        self.b = torch.empty(W.b.numel(), dtype=torch.float64, pin_memory=True)
+        self.b.copy_(W.b)
+        self.x = torch.zeros(W.b.numel(), dtype=torch.float64).pin_memory()
+        self.n = torch.from_numpy(W.ns.copy()).pin_memory()
+        d = W.desc.cpu().numpy().view(DESC_DTYPE).copy()
+        shift = self.slab.data_ptr() - W.slab.data_ptr()
+        for f in ("mem", "pA", "dA"):
+            d[f] = d[f] + np.uint64(shift) if shift >= 0 else d[f] - np.uint64(-shift)
+        self.desc = torch.from_numpy(d.view(np.uint8).copy()).pin_memory()
+
+        def vd(t):
+            v = np.zeros(len(W.ns), dtype=VDESC_DTYPE)
+            v["mem"] = t.data_ptr() + W.voff * 8
+            v["pa"] = t.data_ptr() + W.voff * 8
+            v["m"] = W.ns
+            v["pm"] = W.vlen
+            v["memsize"] = W.vlen * 8
+            return torch.from_numpy(v.view(np.uint8).copy()).pin_memory()
+        self.bdesc, self.xdesc = vd(self.b), vd(self.x)
+        self.voff = W.voff
+
+    def solution(self, i, n):
+        o = int(self.voff[i])
+        return self.x[o:o + n].numpy().copy()
 
 
 def spd_config3(num=20000, nmin=4, nmax=256, logcond=6.0, seed=0, device="cuda"):
