@@ -387,18 +387,20 @@ def cpu_driver():
     return drv
 
 
-def cpu_baseline(systems, passes=5, p1_passes=3):
+def cpu_baseline(systems, passes=5, p1_passes=3, warmup=3):
     """Median wall time of `passes` passes over all systems with one thread per
-    physical core, and of `p1_passes` passes on one core."""
+    physical core (after `warmup` passes, as the reference arm), and of
+    `p1_passes` passes on one core."""
     cr = CpuRun(systems)
     P = len(cr.cpus)
-    cr.run(P)
+    for _ in range(warmup):
+        cr.run(P)
     tp = float(np.median([cr.run(P) for _ in range(passes)]))
     t1 = float(np.median([cr.run(1) for _ in range(p1_passes)]))
     n = systems.num
     return {"value": n / tp, "unit": UNIT, "cores": P, "kind": cr.kind,
             "sample": "the same %d systems as the GPU arm (seed 1000), %s, dpotrf_l+dtrsv_lnn+dtrsv_ltn per system, "
-                      "one thread per physical core (%d of %d logical CPUs), median of %d passes; worst sampled "
+                      "one thread per physical core (%d of %d logical CPUs), median of %d passes after 3 warm-up passes; worst sampled "
                       "backward error %.1e" % (n, cr.name, P, len(os.sched_getaffinity(0)), passes, cr.check()),
             "p1": {"value": n / t1, "cores": 1, "sample": "same systems, one core, median of %d passes" % p1_passes},
             "ms_per_pass": 1e3 * tp}

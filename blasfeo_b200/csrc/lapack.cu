@@ -792,6 +792,144 @@ __global__ void __launch_bounds__(NT) k_geqrf(SizeArg sz, MatArg<T> C, MatArg<T>
 	}
 }
 
+// shared memory of the blocked QR: the panel, then (FP64) the V^T C buffer
+__host__ __device__ inline size_t qr_panel_bytes(int max_m, size_t esz) {
+	return ((size_t)(max_m + 4) * 17 * esz + 15) / 16 * 16;
+}
+// the trailing columns are updated in chunks of at most QR_CHUNK_CB 32-column
+// blocks, so the buffer stays bounded for wide matrices
+constexpr int QR_CHUNK_CB = 8;
+__host__ __device__ inline int qr_w_slots(int nt, int max_n) {
+	const int nw = nt / 32, ncb0 = (max_n + 31) / 32;
+	const int ncb = ncb0 < QR_CHUNK_CB ? ncb0 : QR_CHUNK_CB;
+	return 512 * (nw > ncb ? nw : ncb);
+}
+
+// V(r, k) of the panel's unit lower trapezoidal reflector block (P: rows of 17)
+__device__ __forceinline__ double qr_v(const double *P, int r, int k) {
+	return (r > k) ? P[r * 17 + k] : ((r == k) ? 1.0 : 0.0);
+}
+
+// C = C - V T^T (V^T C) on the FP64 tensor cores for the trailing columns of
+// a 16-column panel (rows c0.. of the panel layout, columns c0 + w ..):
+// P holds V (pr rows), Tm the 16 x 16 upper triangular T, Wsm the partial
+// sums.  Every thread of the CTA calls it; it ends with a barrier.
+__device__ __noinline__ void qr_update_dmma(const PMat<double> &d, const double *P, const double *Tm, double *Wsm, int c0, int w,
+                               int pr, int nr_all, int NT) {
+	const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nw = NT >> 5;
+	const int g = lane >> 2, tq = lane & 3;
+	for (int cc = 0; cc < nr_all; cc += 32 * QR_CHUNK_CB) {
+		// this chunk's columns: c0 + wc .. (wc = w + cc), nr of them
+		const int nr = min(32 * QR_CHUNK_CB, nr_all - cc), wc = w + cc;
+		const int ncb = (nr + 31) >> 5;
+		const int nsplit = nw / ncb > 1 ? nw / ncb : 1;
+		// rows per split, a multiple of 4 (the DMMA k step)
+		const int rsz = ((pr + nsplit - 1) / nsplit + 3) & ~3;
+		const int wld = 32 * ncb;  // row stride of one 16 x wld partial block
+		// e1. partial W blocks: task (cb, sp) -> rows [sp rsz, (sp+1) rsz), columns [32 cb, 32 cb + 32)
+		for (int task = warp; task < ncb * nsplit; task += nw) {
+			const int cb = task % ncb, sp = task / ncb;
+			const int l0 = 32 * cb, rb0 = sp * rsz, rb1 = min(pr, rb0 + rsz);
+			double acc[2][4][2];
+	#pragma unroll
+			for (int mb = 0; mb < 2; mb++)
+	#pragma unroll
+				for (int nb = 0; nb < 4; nb++) acc[mb][nb][0] = acc[mb][nb][1] = 0.0;
+	#pragma unroll 2
+			for (int r = rb0; r < rb1; r += 4) {
+				const int row = r + tq;
+				double a[2], b[4];
+	#pragma unroll
+				for (int mb = 0; mb < 2; mb++) a[mb] = (row < pr) ? qr_v(P, row, 8 * mb + g) : 0.0;
+	#pragma unroll
+				for (int nb = 0; nb < 4; nb++) {
+					const int col = l0 + 8 * nb + g;
+					b[nb] = (row < pr && col < nr) ? d.at(c0 + row, c0 + wc + col) : 0.0;
+				}
+	#pragma unroll
+				for (int mb = 0; mb < 2; mb++)
+	#pragma unroll
+					for (int nb = 0; nb < 4; nb++) lu_dmma(acc[mb][nb][0], acc[mb][nb][1], a[mb], b[nb]);
+			}
+			double *wp = Wsm + (size_t)sp * 16 * wld;
+	#pragma unroll
+			for (int mb = 0; mb < 2; mb++)
+	#pragma unroll
+				for (int nb = 0; nb < 4; nb++) {
+					const int k = 8 * mb + g, col = l0 + 8 * nb + 2 * tq;
+					wp[k * wld + col] = acc[mb][nb][0];
+					wp[k * wld + col + 1] = acc[mb][nb][1];
+				}
+		}
+		__syncthreads();
+		// e2. W = sum of the partials (split order), then W <- T^T W, a thread per column
+		for (int col = tid; col < nr; col += NT) {
+			double wv[16];
+	#pragma unroll
+			for (int k = 0; k < 16; k++) {
+				double sacc = Wsm[k * wld + col];
+				for (int sp = 1; sp < nsplit; sp++) sacc += Wsm[(size_t)sp * 16 * wld + k * wld + col];
+				wv[k] = sacc;
+			}
+	#pragma unroll
+			for (int k = 15; k >= 0; k--) {
+				double z = 0.0;
+	#pragma unroll
+				for (int q = 0; q <= k; q++) z = fma(Tm[q * 17 + k], wv[q], z);
+				wv[k] = z;
+			}
+	#pragma unroll
+			for (int k = 0; k < 16; k++) Wsm[k * wld + col] = wv[k];
+		}
+		__syncthreads();
+		// e3. C -= V W, 32 x 32 tiles
+		const int nrt = (pr + 31) >> 5;
+		for (int t = warp; t < nrt * ncb; t += nw) {
+			const int r0 = 32 * (t / ncb), l0 = 32 * (t % ncb);
+			double acc[4][4][2];
+	#pragma unroll
+			for (int rb = 0; rb < 4; rb++) {
+				const int row = r0 + 8 * rb + g;
+	#pragma unroll
+				for (int cb = 0; cb < 4; cb++) {
+					const int col = l0 + 8 * cb + 2 * tq;
+					acc[rb][cb][0] = (row < pr && col < nr) ? d.at(c0 + row, c0 + wc + col) : 0.0;
+					acc[rb][cb][1] = (row < pr && col + 1 < nr) ? d.at(c0 + row, c0 + wc + col + 1) : 0.0;
+				}
+			}
+	#pragma unroll
+			for (int ks = 0; ks < 4; ks++) {
+				double a[4], b[4];
+	#pragma unroll
+				for (int rb = 0; rb < 4; rb++) {
+					const int row = r0 + 8 * rb + g;
+					a[rb] = (row < pr) ? -qr_v(P, row, 4 * ks + tq) : 0.0;
+				}
+	#pragma unroll
+				for (int cb = 0; cb < 4; cb++) {
+					const int col = l0 + 8 * cb + g;
+					b[cb] = (col < nr) ? Wsm[(4 * ks + tq) * wld + col] : 0.0;
+				}
+	#pragma unroll
+				for (int rb = 0; rb < 4; rb++)
+	#pragma unroll
+					for (int cb = 0; cb < 4; cb++) lu_dmma(acc[rb][cb][0], acc[rb][cb][1], a[rb], b[cb]);
+			}
+	#pragma unroll
+			for (int rb = 0; rb < 4; rb++) {
+				const int row = r0 + 8 * rb + g;
+	#pragma unroll
+				for (int cb = 0; cb < 4; cb++) {
+					const int col = l0 + 8 * cb + 2 * tq;
+					if (row < pr && col < nr) d.at(c0 + row, c0 + wc + col) = acc[rb][cb][0];
+					if (row < pr && col + 1 < nr) d.at(c0 + row, c0 + wc + col + 1) = acc[rb][cb][1];
+				}
+			}
+		}
+		__syncthreads();
+	}
+}
+
 // Householder QR of one instance per CTA whose block stays in global memory
 // (L2), blocked by 16-column panels with the compact WY form of the panel's
 // reflectors (the reference's HP driver applies 4-column blocks with
@@ -811,8 +949,11 @@ __global__ void __launch_bounds__(NT) k_geqrf(SizeArg sz, MatArg<T> C, MatArg<T>
 //      butterfly sums; the update's next rows loaded before the current ones
 //      are stored).
 // Shared memory: (m + 4) x 17 panel, 16 x 17 T and V^T V.
-template <typename T, int NT>
-__global__ void __launch_bounds__(NT) k_geqrf_blk(SizeArg sz, MatArg<T> C, MatArg<T> D, int smem_cap, int max_m) {
+// DMMA: the trailing update on the FP64 tensor cores (FP64 only; needs the
+// V^T C buffer and more registers, so it pays from ~128 x 256 blocks on)
+template <typename T, int NT, bool DMMA>
+__global__ void __launch_bounds__(NT) k_geqrf_blk(SizeArg sz, MatArg<T> C, MatArg<T> D, int smem_cap, int max_m,
+                                                   int max_n) {
 	extern __shared__ __align__(16) unsigned char smem_raw[];
 	__shared__ T s_red[33];
 	__shared__ T s_tau, s_sc, s_beta;
@@ -828,6 +969,8 @@ __global__ void __launch_bounds__(NT) k_geqrf_blk(SizeArg sz, MatArg<T> C, MatAr
 	const int tid = threadIdx.x;
 	const int warp = tid >> 5, lane = tid & 31, nw = NT >> 5;
 	T *P = (T *)smem_raw;  // panel: row r at P + 17 r
+	// FP64: V^T C partial sums (qr_w_slots(NT, max_n) doubles) after the panel
+	double *Wsm = (double *)(smem_raw + qr_panel_bytes(max_m, sizeof(T)));
 	if (c.p != d.p || c.ri != d.ri || c.cj != d.cj) {
 		for (int e = tid; e < m * n; e += NT) {
 			const int i = e % m, j = e / m;
@@ -937,10 +1080,19 @@ __global__ void __launch_bounds__(NT) k_geqrf_blk(SizeArg sz, MatArg<T> C, MatAr
 				for (int j = 0; j < 16; j++) Tm[k * 17 + j] = t[j];
 			}
 			__syncthreads();
-			// e. C = C - V T^T (V^T C): a warp per pair of trailing columns, its
-			// lanes over the rows; w = V^T c by butterfly sums, then w <- T^T w
-			// in place, then c -= V w with the next rows' loads issued before
-			// the current rows' stores
+			// e. C = C - V T^T (V^T C).  FP64 on the tensor cores (DMMA):
+			//   e1. W = V^T C (16 x nr): a warp per 32-column block and row
+			//       chunk (the rows split so that every warp has a task),
+			//       partial sums in shared memory, added in a fixed order;
+			//   e2. W <- T^T W, a thread per column;
+			//   e3. C -= V W as 32 x 32 tiles per warp.
+			// FP32: a warp per pair of trailing columns, its lanes over the
+			// rows; w = V^T c by butterfly sums, then w <- T^T w in place, then
+			// c -= V w with the next rows' loads issued before the current
+			// rows' stores.
+			if constexpr (sizeof(T) == 8 && DMMA) {
+				qr_update_dmma(d, P, Tm, Wsm, c0, w, pr, nr, NT);
+			} else
 			for (int l0 = 2 * warp; l0 < nr; l0 += 2 * nw) {
 				const bool two = l0 + 1 < nr;
 				const int col0 = c0 + w + l0, col1 = col0 + (two ? 1 : 0);
@@ -1125,10 +1277,10 @@ int syrk_potrf_batch(int batch, int m, int k, BT *sA, int ai, int aj, BT *sB, in
 }
 
 // variant: -1 auto; 0..2: the blocked global-memory kernels (getrf: 128
-// threads with 4 or 2 blocks per SM, 256 threads; geqrf: 128/256/512
-// threads); 3..5: the instances whose block fits in shared memory there
-// (128/256/512 threads), the others in the blocked global-memory kernel (a
-// second launch, 256 threads).
+// threads with 4 or 2 blocks per SM, 256 threads; geqrf: 256 threads with the
+// SIMT trailing update, 256 and 512 threads with the DMMA one); 3..5: the
+// instances whose block fits in shared memory there (128/256/512 threads),
+// the others in the blocked global-memory kernel (a second launch).
 template <typename T, int NT, bool SMEM>
 void launch_getrf(int batch, SizeArg sz, int cap, size_t smem, MatArg<T> C, MatArg<T> D, int *ipiv,
                   long long ipiv_stride, int *info, cudaStream_t s, bool piv = true) {
@@ -1162,17 +1314,19 @@ void launch_geqrf(int batch, SizeArg sz, int cap, size_t smem, MatArg<T> C, MatA
 
 // blocked global-memory QR (k_geqrf_blk) for the instances that do not fit
 // shared memory (cap >= 0) or for all of them (cap < 0)
-template <typename T, int NT>
-void launch_geqrf_blk(int batch, SizeArg sz, int cap, int max_m, MatArg<T> C, MatArg<T> D, cudaStream_t s) {
-	auto kern = k_geqrf_blk<T, NT>;
-	const size_t smem = (size_t)(max_m + 4) * 17 * sizeof(T);
+template <typename T, int NT, bool DMMA>
+void launch_geqrf_blk(int batch, SizeArg sz, int cap, int max_m, int max_n, MatArg<T> C, MatArg<T> D,
+                      cudaStream_t s) {
+	auto kern = k_geqrf_blk<T, NT, DMMA>;
+	const size_t smem = qr_panel_bytes(max_m, sizeof(T)) +
+	                    (sizeof(T) == 8 && DMMA ? (size_t)qr_w_slots(NT, max_n) * sizeof(double) : 0);
 	if (smem > bf::max_smem_optin()) {
 		// a panel beyond shared memory (more than ~1,500 rows): the unblocked kernel
 		launch_geqrf<T, 512, false>(batch, sz, cap, 0, C, D, s);
 		return;
 	}
 	if (smem > 48 * 1024) cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-	kern<<<batch, NT, smem, s>>>(sz, C, D, cap, max_m);
+	kern<<<batch, NT, smem, s>>>(sz, C, D, cap, max_m, max_n);
 }
 
 inline size_t lu_smem_bytes(int max_m, int max_n, size_t esz) {
@@ -1183,7 +1337,8 @@ inline size_t lu_smem_bytes(int max_m, int max_n, size_t esz) {
 // batches timed on the B200 at n = 32..384: the shared-memory kernel with 128
 // threads for small blocks, the blocked global-memory kernels above (getrf:
 // 128 threads with 4 blocks per SM up to n = 160, with 2 up to 224, then 256
-// threads; geqrf: shared memory up to 64 rows, then 256 or 512 threads)
+// threads; geqrf: shared memory up to 64 rows, the SIMT update up to 192,
+// then the DMMA update with 512 threads)
 inline int pick_lu_variant(int variant, int max_m, int max_n, bool qr = false) {
 	if (variant < 0) {
 		const int mx = max_m > max_n ? max_m : max_n;
@@ -1192,7 +1347,7 @@ inline int pick_lu_variant(int variant, int max_m, int max_n, bool qr = false) {
 		else if (!qr)
 			variant = mx <= 160 ? 0 : (mx <= 224 ? 1 : 2);
 		else
-			variant = mx <= 64 ? 3 : (mx <= 192 ? 1 : 2);
+			variant = mx <= 64 ? 3 : (mx <= 192 ? 0 : 2);
 	}
 	return variant;
 }
@@ -1228,14 +1383,15 @@ int geqrf_launch(int batch, SizeArg sz, MatArg<T> C, MatArg<T> D, cudaStream_t s
 	const int cap = (int)smem;
 	variant = pick_lu_variant(variant, max_m, max_n, true);
 	switch (variant) {
-	case 0: launch_geqrf_blk<T, 128>(batch, sz, -1, max_m, C, D, s); break;
-	case 1: launch_geqrf_blk<T, 256>(batch, sz, -1, max_m, C, D, s); break;
-	case 2: launch_geqrf_blk<T, 512>(batch, sz, -1, max_m, C, D, s); break;
+	// blocked: 256 threads with the SIMT update, 256 or 512 threads with the DMMA update
+	case 0: launch_geqrf_blk<T, 256, false>(batch, sz, -1, max_m, max_n, C, D, s); break;
+	case 1: launch_geqrf_blk<T, 256, true>(batch, sz, -1, max_m, max_n, C, D, s); break;
+	case 2: launch_geqrf_blk<T, 512, true>(batch, sz, -1, max_m, max_n, C, D, s); break;
 	case 3: launch_geqrf<T, 128, true>(batch, sz, cap, smem, C, D, s); break;
 	case 4: launch_geqrf<T, 256, true>(batch, sz, cap, smem, C, D, s); break;
 	default: launch_geqrf<T, 512, true>(batch, sz, cap, smem, C, D, s); break;
 	}
-	if (variant >= 3 && need > smem) launch_geqrf_blk<T, 256>(batch, sz, cap, max_m, C, D, s);
+	if (variant >= 3 && need > smem) launch_geqrf_blk<T, 512, true>(batch, sz, cap, max_m, max_n, C, D, s);
 	return bf::check_launch();
 }
 

@@ -204,8 +204,9 @@ def test_getrf_rp_ties_and_zero_pivot(bf, orc, prec):
 
 @pytest.mark.parametrize("prec", ["d", "s"])
 @pytest.mark.parametrize("mn", [(128, 64), (32, 16), (9, 9), (5, 3), (3, 5), (1, 1), (200, 100), (300, 150),
-                                (384, 192)])
+                                (384, 192), (100, 400), (70, 300)])
 def test_geqrf(bf, orc, prec, mn):
+    # wide cases: more than 256 trailing columns, updated in several chunks
     m, n = mn
     rng = np.random.default_rng(m + 7 * n)
     M = rng.standard_normal((m, n))
