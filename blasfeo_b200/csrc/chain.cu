@@ -91,7 +91,10 @@ __global__ void __launch_bounds__(CH_WARPS * 32) k_chain16(int batch, int k, dou
 		}
 		if (!__all_sync(0xffffffffu, ok)) {  // a bulk copy did not complete in time
 			if (act && li == 0 && info) info[b] = -3;
-			if (act) mbar_wait(bar, phase ^ 1u, BF_DRAIN_LIMIT);  // drain the copy still in flight
+			// drain the copy still in flight (again bounded): best effort -- if
+			// this wait also runs out, the block returns with the copy possibly
+			// still landing in its shared memory; info = -3 reports the run
+			if (act) mbar_wait(bar, phase ^ 1u, BF_DRAIN_LIMIT);
 			return;
 		}
 		const double *A = buf;
