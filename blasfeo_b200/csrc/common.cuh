@@ -35,6 +35,9 @@ int num_sms();
 size_t max_smem_optin();
 int posv_engine();                        // engine of the mixed SPD solver (BLASFEO_B200_POSV_*)
 unsigned int wait_limit();                // polls of a bounded mbarrier wait (blasfeo_b200_set_wait_limit)
+// this host thread's second stream on the current device and its fork / join
+// events (false if they cannot be made: then run on one stream)
+bool side_stream(cudaStream_t *stream, cudaEvent_t *fork, cudaEvent_t *join);
 
 template <typename T> struct MatT;
 template <> struct MatT<double> { typedef struct blasfeo_dmat type; typedef struct blasfeo_dmat_batch batch; typedef struct blasfeo_dvec vec; };

@@ -98,6 +98,48 @@ static void *workspace_slot(int slot, size_t bytes, cudaStream_t s) {
 	return w.ptr;
 }
 
+// A second stream and two events per host thread and device, for work a call
+// forks off its stream and joins again (created on first use, released when
+// the thread ends).
+struct ThreadSide {
+	struct Dev {
+		cudaStream_t stream = nullptr;
+		cudaEvent_t ev[2] = {nullptr, nullptr};
+		bool failed = false;
+	};
+	std::vector<Dev> dev;
+	~ThreadSide() {
+		for (auto &d : dev) {
+			for (auto &e : d.ev)
+				if (e) cudaEventDestroy(e);
+			if (d.stream) cudaStreamDestroy(d.stream);
+		}
+		cudaGetLastError();
+	}
+};
+static thread_local ThreadSide g_side;
+
+bool side_stream(cudaStream_t *stream, cudaEvent_t *fork, cudaEvent_t *join) {
+	int dev = 0;
+	if (cudaGetDevice(&dev) != cudaSuccess) return false;
+	if ((int)g_side.dev.size() <= dev) g_side.dev.resize(dev + 1);
+	ThreadSide::Dev &d = g_side.dev[dev];
+	if (d.failed) return false;
+	if (!d.stream) {
+		if (cudaStreamCreateWithFlags(&d.stream, cudaStreamNonBlocking) != cudaSuccess ||
+		    cudaEventCreateWithFlags(&d.ev[0], cudaEventDisableTiming) != cudaSuccess ||
+		    cudaEventCreateWithFlags(&d.ev[1], cudaEventDisableTiming) != cudaSuccess) {
+			cudaGetLastError();
+			d.failed = true;
+			return false;
+		}
+	}
+	*stream = d.stream;
+	*fork = d.ev[0];
+	*join = d.ev[1];
+	return true;
+}
+
 void *workspace(size_t bytes, cudaStream_t s) { return workspace_slot(0, bytes, s); }
 void *workspace_cm(size_t bytes, cudaStream_t s) { return workspace_slot(1, bytes, s); }
 
