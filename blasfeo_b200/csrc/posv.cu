@@ -417,7 +417,6 @@ __global__ void __launch_bounds__(NT, MINB) k_posv(int cls, int max_n, PosvWs ws
 		a.cj = 0;
 		const double *bg = sb[sys].pa;
 		double *xg = sx[sys].pa;
-		const int P = (n + 3) >> 2;
 		const int nv = ((n + 15) >> 4) * 16;
 
 		// lower triangle -> lower panels (converted to T), identity padding; the
