@@ -645,7 +645,8 @@ PosvLayout posv_layout(int batch, int max_n, bool use_slots) {
 	if (MIXED && use_slots) {
 		const int per_sm = 16;  // upper bound of resident CTAs per SM over all classes
 		L.rslots = bf::num_sms() * per_sm;
-		L.need = L.rslots_off + (size_t)L.rslots * lp_size(max_n) * sizeof(double);
+		// one set per stream of the class rotation (two streams)
+		L.need = L.rslots_off + 2 * (size_t)L.rslots * lp_size(max_n) * sizeof(double);
 	}
 	return L;
 }
@@ -690,9 +691,8 @@ int posv_run(int batch, const int *n, int max_n, const void *sA, const void *sb,
 	// systems leave idle (mixed solver, 20,000 systems: 10.5 -> 9.8 ms)
 	cudaStream_t side = nullptr;
 	cudaEvent_t fork = nullptr, join = nullptr;
-	// (not with the mapped path's per-CTA refinement slots, which the classes
-	// share by block index)
-	const bool two = nc > 1 && rslots == 0 && bf::side_stream(&side, &fork, &join);
+	// (the mapped path's per-CTA refinement slots: one set per stream)
+	const bool two = nc > 1 && bf::side_stream(&side, &fork, &join);
 	if (two) {
 		cudaEventRecord(fork, s);
 		cudaStreamWaitEvent(side, fork, 0);
@@ -721,7 +721,8 @@ int posv_run(int batch, const int *n, int max_n, const void *sA, const void *sb,
 			}
 		} else {
 			PosvPlan pl = posv_plan<T, MIXED>(cfg[c].upper, cfg[c].threads);
-			double *rs = rslots ? (double *)(wsp + rslots_off) : nullptr;
+			double *rs = rslots ? (double *)(wsp + rslots_off) + (s != s0 ? (size_t)rslots * lp_size(max_n) : 0)
+			                    : nullptr;
 			int st;
 			if (cfg[c].upper <= 64)
 				st = launch_posv<T, MIXED, 64, 8>(c, cfg[c].upper, pl.total, batch, rslots, ws, n, sA, sb, sx, max_iter,
