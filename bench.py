@@ -872,7 +872,9 @@ def other_configs(lib, torch, dev, stream, peak_bw, cpu=True):
     larger than L2), per instance: algorithmic bytes (inputs read once, outputs
     written once) and flops as in the design record.
       chain:    100,000 instances, n = 16: S = A A^T + 16 I (A 16x32), L = chol(S),
-                X = R L^-T, D = C - X G^T (R, C, G 16x16 ~ N(0,1)); one launch;
+                X = R L^-T, D = C - X G^T (R, C, G 16x16 ~ N(0,1)); one launch on
+                batch-interleaved slabs (the leg's number; also replayed as a
+                CUDA graph), the back-to-back kernel on the same instances beside;
       riccati:  4,096 problems, N = 30, nx = 12, nu = 4, A = I + 0.1 N(0,1) scaled
                 to spectral radius 0.95, B ~ N(0,1)/sqrt(nx), Q = I, R = I, S = 0,
                 P_N = I; the whole backward factorization in one launch, FP64 and FP32."""
@@ -917,8 +919,18 @@ def other_configs(lib, torch, dev, stream, peak_bw, cpu=True):
             out["chain_n16"]["cpu_reference"] = cpu_chain_leg(nb, slabs, L, X, D)
         except Exception as ex:  # reported, never silently replaced
             out["chain_n16"]["cpu_reference"] = {"error": repr(ex)}
+    # the configuration's layout is the batch-interleaved one: its kernel is the
+    # leg's number, the back-to-back kernel on the same instances beside it
     try:
-        out["chain_n16"]["interleaved"] = chain_interleaved(lib, torch, stream, peak_bw, tm, nb, slabs, L, X, D, ms)
+        il = chain_interleaved(lib, torch, stream, peak_bw, tm, nb, slabs, L, X, D, ms)
+        b2b = {k: out["chain_n16"].pop(k) for k in ("ms", "instances_per_s", "gbs", "frac_of_hbm", "gflops")}
+        out["chain_n16"].update({"layout": "batch-interleaved (blasfeo_dsyrk_dpotrf_dtrsm_dgemm_batch_il)",
+                                 "ms": il["ms"], "instances_per_s": il["instances_per_s"], "gbs": il["gbs"],
+                                 "frac_of_hbm": il["frac_of_hbm"], "gflops": fl / il["ms"] / 1e6,
+                                 "graph_replay_ms": il.get("graph_replay_ms"),
+                                 "relfro_vs_back_to_back_first_2000": il["relfro_vs_back_to_back_first_2000"],
+                                 "back_to_back": dict(b2b, kernel="blasfeo_dsyrk_dpotrf_dtrsm_dgemm_batch"),
+                                 "speedup_vs_back_to_back": il["speedup_vs_back_to_back"]})
     except Exception as ex:  # reported, never silently replaced
         out["chain_n16"]["interleaved"] = {"error": repr(ex)}
     del slabs, L, X, D
@@ -945,9 +957,22 @@ def chain_interleaved(lib, torch, stream, peak_bw, tm, nb, slabs, L, X, D, ms_b2
     ins = [DMatBatchIL(slabs[n].m, slabs[n].n, nb).from_batch(slabs[n], sh) for n in "ARCG"]
     outs = [DMatBatchIL(16, 16, nb) for _ in range(3)]
     info = torch.zeros(nb, dtype=torch.int32, device=ins[0].buf.device)
-    ms = tm(lambda: lib.blasfeo_dsyrk_dpotrf_dtrsm_dgemm_batch_il(nb, 16, 32, 16.0, *(x.ref for x in ins),
-                                                                *(x.ref for x in outs), C.c_void_p(info.data_ptr()),
-                                                                sh))
+    call_on = lambda h: lib.blasfeo_dsyrk_dpotrf_dtrsm_dgemm_batch_il(nb, 16, 32, 16.0, *(x.ref for x in ins),
+                                                                      *(x.ref for x in outs),
+                                                                      C.c_void_p(info.data_ptr()), h)
+    ms = tm(lambda: call_on(sh))
+    # the same launch captured in a CUDA graph (on a stream of its own: the
+    # legacy stream cannot be captured) and replayed on the leg's stream
+    try:
+        cap = torch.cuda.Stream()
+        gr = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(gr, stream=cap, capture_error_mode="relaxed"):
+            call_on(C.c_void_p(cap.cuda_stream))
+        with torch.cuda.stream(stream):
+            graph_ms = tm(gr.replay)
+        del gr
+    except Exception as ex:  # reported beside the direct launch
+        graph_ms = {"error": repr(ex)}
     if not bool((info == 0).all().item()):
         raise RuntimeError("interleaved chain reported a non-positive pivot")
     diff = {}
@@ -960,7 +985,8 @@ def chain_interleaved(lib, torch, stream, peak_bw, tm, nb, slabs, L, X, D, ms_b2
         diff[name] = float(np.linalg.norm(a_ - b_) / np.linalg.norm(b_))
     by = 15424.0 * nb
     return {"ms": ms, "instances_per_s": nb / ms * 1e3, "gbs": by / ms / 1e6, "frac_of_hbm": by / ms / 1e6 / peak_bw,
-            "speedup_vs_back_to_back": ms_b2b / ms, "relfro_vs_back_to_back_first_2000": diff}
+            "speedup_vs_back_to_back": ms_b2b / ms, "relfro_vs_back_to_back_first_2000": diff,
+            "graph_replay_ms": graph_ms}
 
 
 def potrf_layouts(lib, torch, dev, stream, peak_bw, g, tm, nb=100000, n=16):
@@ -1079,9 +1105,20 @@ def riccati_legs(lib, torch, dev, stream, peak_bw, g, tm, nbt, N, nx, nu, cpu):
         Ls[prec] = sL.unpack_all().reshape(nbt, N + 1, 16, 16)
         slabs[prec] = (sBA, sRSQ, sL)
     sBA, sRSQ, sL = slabs["d"]
+    # the FP64 factorization's number is the faster layout's (stage-major
+    # batch-interleaved slabs, bit-equal factors); the back-to-back kernel, whose
+    # factors the error and CPU legs below use, beside it
     try:
-        out["riccati_d_N30"]["interleaved"] = riccati_interleaved(lib, torch, sh, peak_bw, tm, nbt, N, nx, nu, BAs,
-                                                                  RSQ, Ls["d"], out["riccati_d_N30"]["ms"])
+        il = riccati_interleaved(lib, torch, sh, peak_bw, tm, nbt, N, nx, nu, BAs, RSQ, Ls["d"],
+                                 out["riccati_d_N30"]["ms"])
+        r = out["riccati_d_N30"]
+        b2b = {k: r.pop(k) for k in ("ms", "problems_per_s", "gbs", "frac_of_hbm", "gflops")}
+        r.update({"layout": "stage-major batch-interleaved (blasfeo_dric_trf_batch_il)", "ms": il["ms"],
+                  "problems_per_s": il["problems_per_s"], "gbs": il["gbs"], "frac_of_hbm": il["frac_of_hbm"],
+                  "gflops": 7.1e3 * N * nbt / il["ms"] / 1e6,
+                  "relfro_vs_back_to_back": il["relfro_vs_back_to_back"],
+                  "back_to_back": dict(b2b, kernel="blasfeo_dric_trf_batch"),
+                  "speedup_vs_back_to_back": il["speedup_vs_back_to_back"]})
     except Exception as ex:  # reported, never silently replaced
         out["riccati_d_N30"]["interleaved"] = {"error": repr(ex)}
     if cpu:
