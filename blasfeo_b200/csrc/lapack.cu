@@ -1186,16 +1186,14 @@ int potrf_launch(int batch, SizeArg sz, int max_m, MatArg<T> C, MatArg<T> D, int
 	if constexpr (sizeof(T) == 8) {
 		if (max_m <= 64 && (variant < 0 || variant == 5)) return dpotrf_dmma_launch(batch, sz, max_m, C, D, info, s);
 		if (variant < 0 && max_m <= dpotrf_ll_max_n()) {
-			// by size (measured fastest per range): n <= 64 one warp on the FP64
-			// tensor cores, 64 < n <= 128 shared memory with 128 threads, larger
-			// n blocked from L2 with FP64 tensor-core updates; one launch per
-			// range, each kernel skips the instances of the other ranges
+			// by size (measured fastest per range, uniform batches n = 32..384):
+			// n <= 64 one warp on the FP64 tensor cores, larger n blocked from
+			// L2 with FP64 tensor-core updates (at n = 128 0.11 ms against
+			// 0.15 ms for the shared-memory kernel); one launch per range, each
+			// kernel skips the instances of the other range
 			int st = dpotrf_dmma_launch(batch, sz, 64, C, D, info, s);
-			if (st) return st;
-			const int m2 = max_m < 128 ? max_m : 128;
-			launch_potrf_smem<T, 128, 4>(batch, sz, m2, potrf_smem_plan<T>(m2).total, C, D, info, s, 64);
-			if ((st = check_launch()) || max_m <= 128) return st;
-			return dpotrf_ll_launch(batch, sz, 128, max_m, C, D, info, s);
+			if (st || max_m <= 64) return st;
+			return dpotrf_ll_launch(batch, sz, 64, max_m, C, D, info, s);
 		}
 	}
 	if (variant == 5) variant = -1;
