@@ -73,6 +73,28 @@ def parse():
     return ap.parse_args()
 
 
+def rank_seed(rank):
+    """Seed of a rank's systems: every replica solves its own batch of the
+    distribution (rank 0's is the batch the reference arm solves)."""
+    return 1000 + rank
+
+
+def reduce_max_ms(ms, world, dist, device):
+    """The job's time of a step: the maximum over the ranks (the slowest replica
+    finishes the job); the same collective on every rank."""
+    if world <= 1:
+        return ms
+    import torch
+    t = torch.tensor([ms], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def aggregate_value(world, num, ms):
+    """Whole-job systems/s: every rank solves `num` systems in `ms` (the max over ranks)."""
+    return world * num / (ms * 1e-3)
+
+
 def run_case(argv):
     """One routine on a small seeded workload, for an ncu capture of its kernel."""
     import torch
@@ -501,7 +523,7 @@ def main():
     lib = bf.lib
     P = lambda t: C.c_void_p(t.data_ptr())
     dev = torch.device("cuda", local)
-    systems = gen_config3(args.num, 1000 + rank, dev)
+    systems = gen_config3(args.num, rank_seed(rank), dev)
     W = SpdBatch(*systems, device=dev)
     # the CPU baseline solves the very same systems from host memory
     host_sys = HostSystems(*systems) if (rank == 0 and world == 1 and not args.no_cpu) else None
@@ -537,12 +559,7 @@ def main():
         e1.record(stream)
         torch.cuda.synchronize()
         barrier()
-        ms = e0.elapsed_time(e1) / steps
-        if world > 1:
-            t = torch.tensor([ms], dtype=torch.float64, device=dev)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            ms = float(t.item())
-        return ms
+        return reduce_max_ms(e0.elapsed_time(e1) / steps, world, dist, dev)
 
     # ---- correctness gate (not timed): every system at FP64-level residual ----
     bf.check(mixed())
@@ -576,8 +593,8 @@ def main():
     ms_plain = timed(plain, args.steps, args.warmup)
     clocks = clk.stop()
     nclass = 9  # classify + size classes (upper bound of launches per call)
-    value = world * args.num / (ms_mixed * 1e-3)
-    plain_value = world * args.num / (ms_plain * 1e-3)
+    value = aggregate_value(world, args.num, ms_mixed)
+    plain_value = aggregate_value(world, args.num, ms_plain)
 
     # ---- e2e: everything in pinned host memory, kernels read it over the host link ----
     e2e = None
@@ -1454,12 +1471,13 @@ def run_e2e(args, W, lib, torch, dev, stream, barrier, world):
     e1.record(stream)
     torch.cuda.synchronize()
     wall = (time.perf_counter() - t0) / args.steps
-    ms = e0.elapsed_time(e1) / args.steps
     barrier()
+    import torch.distributed as dist
+    ms = reduce_max_ms(e0.elapsed_time(e1) / args.steps, world, dist, dev)
     n = W.ns.astype(np.int64)
     h2d = int((n * (n + 1) // 2 * 8).sum() + W.b.numel() * 8 + hn.numel() * 4 + hdesc.numel() + hbd.numel() * 2)
     d2h = int(n.sum() * 8)
-    return {"value": world * args.num / (ms * 1e-3), "unit": UNIT, "h2d_bytes_per_step": h2d,
+    return {"value": aggregate_value(world, args.num, ms), "unit": UNIT, "h2d_bytes_per_step": h2d,
             "d2h_bytes_per_step": d2h, "ms_per_step": ms, "host_wall_ms_per_step": wall * 1e3,
             "path": "blasfeo_dsposv_l_vbatch_mapped, all inputs in pinned host memory",
             "host_link_gbs": (h2d + d2h) / (ms * 1e-3) / 1e9, "residual_system0": float(res)}
