@@ -86,7 +86,7 @@ def test_training_fits_a_smooth_function(bf):
 
 def test_learned_dispatch_regret(bf):
     """Sweep sampled launches of the mixed-op stream, train on 70% of them and
-    judge the held-out picks by regret against the exhaustive best."""
+    score the held-out picks by regret against the exhaustive best."""
     from blasfeo_b200 import autotune as at
     from blasfeo_b200.costmodel import CostModel
     recs = at.sweep(48, seed=7, bmin=256, bmax=2048, nmax=256, reps=3)
