@@ -209,6 +209,8 @@ _sig("blasfeo_memsize_dmat_batch_il", _sz, _i, _i, _i)
 _sig("blasfeo_create_dmat_batch_il", None, _i, _i, _i, _IL, _vp)
 _sig("blasfeo_dmat_batch_to_il", _i, _DB, _IL, _vp)
 _sig("blasfeo_dmat_batch_from_il", _i, _IL, _DB, _vp)
+_sig("blasfeo_pack_dmat_batch_il", _i, _i, _i, _i, _vp, _i, C.c_longlong, _IL, _vp)
+_sig("blasfeo_unpack_dmat_batch_il", _i, _i, _i, _i, _IL, _vp, _i, C.c_longlong, _vp)
 _sig("blasfeo_dpotrf_l_batch_il", _i, _i, _i, _IL, _IL, _vp, _vp)
 _sig("blasfeo_dsyrk_dpotrf_dtrsm_dgemm_batch_il", _i, _i, _i, _i, _d, _IL, _IL, _IL, _IL, _IL, _IL, _IL, _vp, _vp)
 _sig("blasfeo_dric_trf_batch_il", _i, _i, _i, _i, _i, _IL, _IL, _IL, _vp, _vp)

@@ -250,6 +250,23 @@ class DMatBatchIL:
         check(lib.blasfeo_dmat_batch_from_il(self.ref, B.ref, stream))
         return B
 
+    def pack_all(self, arr, stream=None):
+        """arr: (batch, m, n) host array -> the slab, through
+        blasfeo_pack_dmat_batch_il (host column-major, one host copy)."""
+        arr = np.asarray(arr, dtype=np.float64)
+        b, m, n = arr.shape
+        cm = np.ascontiguousarray(arr.transpose(0, 2, 1))  # column-major per instance, lda = m
+        check(lib.blasfeo_pack_dmat_batch_il(b, m, n, cm.ctypes.data_as(C.c_void_p), m, m * n, self.ref, stream))
+        return self
+
+    def unpack_all(self, m=None, n=None, stream=None):
+        m = self.m if m is None else m
+        n = self.n if n is None else n
+        cm = np.zeros((self.batch, n, m), dtype=np.float64)
+        check(lib.blasfeo_unpack_dmat_batch_il(self.batch, m, n, self.ref, cm.ctypes.data_as(C.c_void_p), m, m * n,
+                                               stream))
+        return np.ascontiguousarray(cm.transpose(0, 2, 1))
+
 
 def descriptor_array(mats):
     """Device array of struct blasfeo_dmat descriptors (for the *_vbatch calls)."""

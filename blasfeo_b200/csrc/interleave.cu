@@ -121,6 +121,30 @@ __global__ void __launch_bounds__(256, (G >= 4) ? 2 : 1) k_dpotrf_il(int batch, 
 	}
 }
 
+// host column-major batch (staged densely: instance b, element (i, j) at
+// stage[b m n + j m + i]) <-> interleaved slab, one thread per (group, slot,
+// lane) so that the slab side moves in runs of IL consecutive instances
+template <bool TO_IL>
+__global__ void k_cm_il(long long total, int batch, int m, int n, double *stage, double *il, long long gstride,
+                        int cn) {
+	const long long mn = (long long)m * n;
+	for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < total;
+	     t += (long long)gridDim.x * blockDim.x) {
+		const long long g = t / (mn * IL);
+		const long long r = t % (mn * IL);
+		const int el = (int)(r / IL), l = (int)(r % IL);
+		const long long b = g * IL + l;
+		if (b >= batch) continue;
+		const int i = el % m, j = el / m;
+		double *slot = il + g * gstride + pm_el(i, j, cn) * IL + l;
+		double *dense = stage + b * mn + (long long)j * m + i;
+		if (TO_IL)
+			*slot = *dense;
+		else
+			*dense = *slot;
+	}
+}
+
 inline int grid_for(long long total, int threads) {
 	long long g = (total + threads - 1) / threads;
 	const long long cap = (long long)bf::num_sms() * 16;
@@ -185,6 +209,61 @@ int blasfeo_dmat_batch_from_il(const struct blasfeo_dmat_batch_il *src, struct b
 		                  src->mem + (long long)(b / IL) * src->gstride + b % IL, IL * sizeof(double),
 		                  sizeof(double), g.slots, cudaMemcpyDeviceToDevice, (cudaStream_t)stream);
 	return bf::check_launch();
+}
+
+// host column-major batch <-> interleaved slab: one host copy through a
+// library-owned staging buffer and one conversion kernel; synchronous with
+// `stream` on return (the staging buffer is reused by the next call)
+static int cm_il(int batch, int m, int n, double *A, int lda, long long strideA, const struct blasfeo_dmat_batch_il *sB,
+                 cudaStream_t s, bool to_il) {
+	if (batch < 0 || m < 0 || n < 0 || !sB || !sB->mem || (batch > 0 && m > 0 && n > 0 && !A))
+		return BLASFEO_B200_EINVAL;
+	if (batch == 0 || m == 0 || n == 0) return BLASFEO_B200_OK;
+	if (lda < m || strideA < (long long)lda * (n - 1) + m || m > sB->m || n > sB->n || batch > sB->batch)
+		return BLASFEO_B200_EINVAL;
+	const size_t per = (size_t)m * n;
+	double *stage = (double *)bf::workspace(per * batch * sizeof(double), s);
+	if (!stage) return BLASFEO_B200_ENOMEM;
+	const bool packed = strideA == (long long)lda * n;
+	const long long total = (long long)((batch + IL - 1) / IL) * (long long)per * IL;
+	if (to_il) {
+		if (packed) {
+			if (cudaMemcpy2DAsync(stage, m * sizeof(double), A, (size_t)lda * sizeof(double), m * sizeof(double),
+			                      (size_t)n * batch, cudaMemcpyHostToDevice, s) != cudaSuccess)
+				return BLASFEO_B200_ECUDA;
+		} else {
+			for (int b = 0; b < batch; b++)
+				if (cudaMemcpy2DAsync(stage + per * b, m * sizeof(double), A + strideA * b, (size_t)lda * sizeof(double),
+				                      m * sizeof(double), n, cudaMemcpyHostToDevice, s) != cudaSuccess)
+					return BLASFEO_B200_ECUDA;
+		}
+		k_cm_il<true><<<grid_for(total, 256), 256, 0, s>>>(total, batch, m, n, stage, sB->mem, sB->gstride, sB->cn);
+		if (bf::check_launch()) return BLASFEO_B200_ECUDA;
+	} else {
+		k_cm_il<false><<<grid_for(total, 256), 256, 0, s>>>(total, batch, m, n, stage, sB->mem, sB->gstride, sB->cn);
+		if (bf::check_launch()) return BLASFEO_B200_ECUDA;
+		if (packed) {
+			if (cudaMemcpy2DAsync(A, (size_t)lda * sizeof(double), stage, m * sizeof(double), m * sizeof(double),
+			                      (size_t)n * batch, cudaMemcpyDeviceToHost, s) != cudaSuccess)
+				return BLASFEO_B200_ECUDA;
+		} else {
+			for (int b = 0; b < batch; b++)
+				if (cudaMemcpy2DAsync(A + strideA * b, (size_t)lda * sizeof(double), stage + per * b, m * sizeof(double),
+				                      m * sizeof(double), n, cudaMemcpyDeviceToHost, s) != cudaSuccess)
+					return BLASFEO_B200_ECUDA;
+		}
+	}
+	return cudaStreamSynchronize(s) == cudaSuccess ? BLASFEO_B200_OK : BLASFEO_B200_ECUDA;
+}
+
+int blasfeo_pack_dmat_batch_il(int batch, int m, int n, const double *A, int lda, long long strideA,
+                               struct blasfeo_dmat_batch_il *sB, void *stream) {
+	return cm_il(batch, m, n, (double *)A, lda, strideA, sB, (cudaStream_t)stream, true);
+}
+
+int blasfeo_unpack_dmat_batch_il(int batch, int m, int n, const struct blasfeo_dmat_batch_il *sB, double *A, int lda,
+                                 long long strideA, void *stream) {
+	return cm_il(batch, m, n, A, lda, strideA, sB, (cudaStream_t)stream, false);
 }
 
 int blasfeo_dpotrf_l_batch_il(int batch, int m, struct blasfeo_dmat_batch_il *sC, struct blasfeo_dmat_batch_il *sD,

@@ -293,7 +293,8 @@ __device__ void sym_residual(const double *base, int cn, int n, const double *b,
 			const double *t = res_tile<LP>(base, cn, ti, tj);
 #pragma unroll
 			for (int q = 0; q < 8; q++) {
-				const double2 v = __ldg((const double2 *)(t + 2 * q));
+				// L2 only: the per-CTA copy (LP) is written by this kernel
+				const double2 v = __ldcg((const double2 *)(t + 2 * q));
 				e[2 * q] = v.x;
 				e[2 * q + 1] = v.y;
 			}

@@ -295,6 +295,15 @@ size_t blasfeo_memsize_dmat_batch_il(int m, int n, int batch);
 void blasfeo_create_dmat_batch_il(int m, int n, int batch, struct blasfeo_dmat_batch_il *sA, void *memory);
 int blasfeo_dmat_batch_to_il(const struct blasfeo_dmat_batch *src, struct blasfeo_dmat_batch_il *dst, void *stream);
 int blasfeo_dmat_batch_from_il(const struct blasfeo_dmat_batch_il *src, struct blasfeo_dmat_batch *dst, void *stream);
+/* Host column-major batch (instance b at A + b*strideA, leading dimension lda,
+ * the batched form of blasfeo_pack_dmat / blasfeo_unpack_dmat,
+ * auxiliary/d_aux_lib4.c:1607,2238) <-> the top-left m x n block of an
+ * interleaved slab: one host copy and one conversion kernel; returns when the
+ * copy is complete. */
+int blasfeo_pack_dmat_batch_il(int batch, int m, int n, const double *A, int lda, long long strideA,
+	struct blasfeo_dmat_batch_il *sB, void *stream);
+int blasfeo_unpack_dmat_batch_il(int batch, int m, int n, const struct blasfeo_dmat_batch_il *sB, double *A, int lda,
+	long long strideA, void *stream);
 /* potrf_l (include/blasfeo_d_blasfeo_api.h:280, one instance per lane pair)
  * on interleaved slabs of equal geometry, m <= 16 (else ENOTSUP): the m x m
  * lower factor of each instance of sC into sD with the inverse diagonal in its

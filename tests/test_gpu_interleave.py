@@ -1,5 +1,6 @@
 """GPU tests of the batch-interleaved layout: lossless conversion from and to
-the back-to-back slab (whole and partial groups of 16), and potrf_l on it
+the back-to-back slab and from and to host column-major batches (whole and
+partial groups of 16), and potrf_l on it
 against the oracle, with the reference's pivot rule and per-instance info."""
 import ctypes as C
 
@@ -36,6 +37,57 @@ def test_round_trip(bf, shape):
     for b, i, j in ((0, 0, 0), (nb - 1, m - 1, n - 1), (nb // 2, m // 2, n // 3)):
         e = (i - i % 4) * cn + 4 * j + i % 4
         assert raw[(b // 16) * gs + 16 * e + b % 16] == X[b, i, j]
+
+
+@pytest.mark.parametrize("shape", [(16, 16, 48), (5, 7, 37), (12, 12, 3), (16, 32, 17), (1, 1, 1)])
+def test_host_pack_unpack_il(bf, shape):
+    """Host column-major <-> interleaved slab directly: the same slots as the
+    route through the back-to-back slab, a strided host batch (lda > m,
+    stride > lda n) in both directions, and the slots outside the block left
+    as they were."""
+    import torch
+    from blasfeo_b200.api import DMatBatchIL
+    m, n, nb = shape
+    rng = np.random.default_rng(7 * m + n + nb)
+    X = rng.standard_normal((nb, m, n))
+    il = DMatBatchIL(m, n, nb).pack_all(X)
+    ref = DMatBatchIL(m, n, nb).from_batch(bf.DMatBatch(m, n, nb).pack_all(X))
+    torch.cuda.synchronize()
+    raw, rraw = il.buf.cpu().numpy().view(np.float64), ref.buf.cpu().numpy().view(np.float64)
+    cn, gs = il.s.cn, il.s.gstride
+    for b in range(nb):
+        for i in range(m):
+            for j in range(n):
+                e = (i - i % 4) * cn + 4 * j + i % 4
+                assert raw[(b // 16) * gs + 16 * e + b % 16] == rraw[(b // 16) * gs + 16 * e + b % 16] == X[b, i, j]
+    assert np.array_equal(il.unpack_all(), X)
+    # strided host batch: lda = m + 3, stride = lda n + 5; a sub-block (m', n') of the slab
+    mm, nn = max(1, m - 1), max(1, n - 2)
+    lda, stride = m + 3, (m + 3) * n + 5
+    host = np.full(nb * stride, np.nan)
+    for b in range(nb):
+        for j in range(nn):
+            host[b * stride + j * lda: b * stride + j * lda + mm] = -X[b, :mm, j]
+    st = bf.lib.blasfeo_pack_dmat_batch_il(nb, mm, nn, C.c_void_p(host.ctypes.data), lda, stride, il.ref, None)
+    assert st == 0
+    got = il.unpack_all()
+    want = X.copy()
+    want[:, :mm, :nn] *= -1
+    assert np.array_equal(got, want)
+    back = np.full(nb * stride, 7.0)
+    st = bf.lib.blasfeo_unpack_dmat_batch_il(nb, mm, nn, il.ref, C.c_void_p(back.ctypes.data), lda, stride, None)
+    assert st == 0
+    for b in range(nb):
+        for j in range(nn):
+            col = back[b * stride + j * lda: b * stride + (j + 1) * lda]
+            assert np.array_equal(col[:mm], -X[b, :mm, j]) and (col[mm:] == 7.0).all()
+    # argument errors: lda < m, a block larger than the slab, a batch larger than the slab
+    bad = np.zeros(4 * nb * (m + 1) * (n + 1))
+    P = C.c_void_p(bad.ctypes.data)
+    if m > 1:
+        assert bf.lib.blasfeo_pack_dmat_batch_il(nb, m, n, P, m - 1, m * n, il.ref, None) == 1
+    assert bf.lib.blasfeo_pack_dmat_batch_il(nb, m + 1, n, P, m + 1, (m + 1) * n, il.ref, None) == 1
+    assert bf.lib.blasfeo_unpack_dmat_batch_il(nb + 1, m, n, il.ref, P, m, m * n, None) == 1
 
 
 @pytest.mark.parametrize("n", [1, 5, 12, 16])
