@@ -253,119 +253,128 @@ __device__ double block_max(double v, double *red) {
 }
 
 // r = b - A x (FP64), A symmetric given by its lower triangle, in one pass
-// over the 4x4 tiles of the lower triangle (every tile read once).
-// LP = false: A in BLASFEO panel-major storage (tile (ti,tj) at base + 4*ti*cn + 16*tj);
-// LP = true: A in lower panels (tile at base + lp_off(ti) + 16*tj).
-// Warp w takes tile rows ti = w, w + NW, ...; lane l the tiles tj = l, l + 32
-// of the row.  A tile adds A_tile x_tj to rows ti (row part, reduced over the
-// lanes by a shuffle tree) and, below the diagonal, A_tile^T x_ti to rows tj
-// (column part, kept per lane in registers); after all row parts are written
-// the warps subtract their column parts one after the other in warp order, so
-// the result does not depend on timing and needs no reduction buffer.
+// over the lower triangle (every element read once).
+// LP = false: A in BLASFEO panel-major storage (tile row ti at base + 4*ti*cn);
+// LP = true: A in lower panels (tile row ti at base + lp_off(ti)).
+// Either way the tiles 0..ti of tile row ti are 128 (ti+1) contiguous bytes,
+// tile (ti,tj) column-major.  Warp w takes tile rows ti = w, w + NW, ...
+// and reads a row as contiguous 512-byte pieces, one 16-byte load per lane:
+// piece k, lane l holds rows 2(l&1), 2(l&1)+1 of column 16k + jl of the
+// row, jl = 4(l>>3) + ((l&7)>>1), so every load instruction of the warp
+// covers four whole cache lines.  A lane's column set {16k + jl} is the same
+// in every row, so the transposed contributions (A^T x for the strictly lower
+// part) accumulate per lane in registers (cacc[k]) over all rows of the
+// warp; the row contributions (A x for the lower part with the diagonal) are
+// reduced over the lanes of equal parity by shuffles after each row.  After
+// all rows the warps subtract their column sums one after the other in warp
+// order, so the result does not depend on timing.  KMAX = pieces of the
+// longest row (tile rows <= 4 KMAX, n <= 16 KMAX).
 // RES: the residual into r; NORM: the row sums of |A| into asum.
-// n <= 256 (two tile columns per lane).
 template <bool LP>
-__device__ __forceinline__ const double *res_tile(const double *base, int cn, int ti, int tj) {
-	return LP ? base + lp_off(ti) + 16 * tj : base + (size_t)(4 * ti) * cn + 16 * tj;
+__device__ __forceinline__ const double *res_row(const double *base, int cn, int ti) {
+	return LP ? base + lp_off(ti) : base + (size_t)(4 * ti) * cn;
 }
 
-template <bool LP, bool RES, bool NORM>
+template <bool LP, bool RES, bool NORM, int KMAX>
 __device__ void sym_residual(const double *base, int cn, int n, const double *b, const double *x, double *r,
                              double *asum) {
 	const int tid = threadIdx.x, nt = blockDim.x;
 	const int lane = tid & 31, warp = tid >> 5, nw = nt >> 5;
 	const int P = (n + 3) >> 2;
-	double cacc[2][4], cabs[2][4];
+	const int a0 = 2 * (lane & 1);                           // first of the lane's two rows in a tile
+	const int jl = 4 * (lane >> 3) + ((lane & 7) >> 1);      // the lane's column in a 16-column piece
+	double cacc[KMAX], cabs[KMAX];
 #pragma unroll
-	for (int m = 0; m < 2; m++)
-#pragma unroll
-		for (int q = 0; q < 4; q++) cacc[m][q] = cabs[m][q] = 0.0;
+	for (int k = 0; k < KMAX; k++) cacc[k] = cabs[k] = 0.0;
 	for (int ti = warp; ti < P; ti += nw) {
-		double racc[4] = {0.0, 0.0, 0.0, 0.0}, rabs[4] = {0.0, 0.0, 0.0, 0.0};
-		const double2 xr01 = *(const double2 *)(x + 4 * ti), xr23 = *(const double2 *)(x + 4 * ti + 2);
-		const double xr[4] = {xr01.x, xr01.y, xr23.x, xr23.y};
+		const double *row = res_row<LP>(base, cn, ti) + 2 * lane;
+		const int kr = (ti + 4) >> 2;       // pieces of this row
+		const int kl = ti - (lane >> 3);    // the lane's tile 4k + (lane>>3) is in the row iff 4k <= kl
+		const int gi0 = 4 * ti + a0;
+		// every load of the row first (L2 only: the per-CTA copy (LP) is
+		// written by this kernel); slots past the row stay zero
+		double2 v[KMAX];
 #pragma unroll
-		for (int m = 0; m < 2; m++) {
-			const int tj = lane + 32 * m;
-			if (tj > ti) continue;
-			// e[4*q + a]: row 4ti+a, column 4tj+q; padding and the upper part of the diagonal tile masked
-			double e[16];
-			const double *t = res_tile<LP>(base, cn, ti, tj);
+		for (int k = 0; k < KMAX; k++) {
+			v[k] = make_double2(0.0, 0.0);
+			if (k < kr && 4 * k <= kl) v[k] = __ldcg((const double2 *)(row + 64 * k));
+		}
+		const double xr0 = x[gi0], xr1 = x[gi0 + 1];
+		double r0 = 0.0, r1 = 0.0, s0 = 0.0, s1 = 0.0;
 #pragma unroll
-			for (int q = 0; q < 8; q++) {
-				// L2 only: the per-CTA copy (LP) is written by this kernel
-				const double2 v = __ldcg((const double2 *)(t + 2 * q));
-				e[2 * q] = v.x;
-				e[2 * q + 1] = v.y;
-			}
-#pragma unroll
-			for (int q = 0; q < 4; q++)
-#pragma unroll
-				for (int a = 0; a < 4; a++) {
-					const int gi = 4 * ti + a, gj = 4 * tj + q;
-					if (!(gi < n && gj < n && (tj < ti || gj <= gi))) e[4 * q + a] = 0.0;
-				}
-			const double2 xc01 = *(const double2 *)(x + 4 * tj), xc23 = *(const double2 *)(x + 4 * tj + 2);
-			const double xc[4] = {xc01.x, xc01.y, xc23.x, xc23.y};
-#pragma unroll
-			for (int a = 0; a < 4; a++) {
-				if (RES) racc[a] = fma(e[a], xc[0], fma(e[4 + a], xc[1], fma(e[8 + a], xc[2], fma(e[12 + a], xc[3], racc[a]))));
-				if (NORM) rabs[a] += fabs(e[a]) + fabs(e[4 + a]) + fabs(e[8 + a]) + fabs(e[12 + a]);
-			}
-			if (tj < ti) {
-#pragma unroll
-				for (int q = 0; q < 4; q++) {
-					if (RES) cacc[m][q] = fma(e[4 * q], xr[0], fma(e[4 * q + 1], xr[1], fma(e[4 * q + 2], xr[2], fma(e[4 * q + 3], xr[3], cacc[m][q]))));
-					if (NORM) cabs[m][q] += fabs(e[4 * q]) + fabs(e[4 * q + 1]) + fabs(e[4 * q + 2]) + fabs(e[4 * q + 3]);
-				}
-			} else {
-				// strictly upper part of the diagonal tile mirrors the lower part
+		for (int k = 0; k < KMAX; k++) {
+			if (k < kr) {
+				const int gj = 16 * k + jl;
+				const bool ok = 4 * k <= kl && gj < n;
+				const double xj = x[gj];
+				// row part: j <= i; column part: j < i
+				const double e0 = ok && gi0 < n && gj <= gi0 ? v[k].x : 0.0;
+				const double e1 = ok && gi0 + 1 < n && gj <= gi0 + 1 ? v[k].y : 0.0;
+				const double c0 = gj < gi0 ? e0 : 0.0;
+				const double c1 = gj < gi0 + 1 ? e1 : 0.0;
 				if (RES) {
-					racc[0] = fma(e[1], xc[1], fma(e[2], xc[2], fma(e[3], xc[3], racc[0])));
-					racc[1] = fma(e[6], xc[2], fma(e[7], xc[3], racc[1]));
-					racc[2] = fma(e[11], xc[3], racc[2]);
+					r0 = fma(e0, xj, r0);
+					r1 = fma(e1, xj, r1);
+					cacc[k] = fma(c0, xr0, fma(c1, xr1, cacc[k]));
 				}
 				if (NORM) {
-					rabs[0] += fabs(e[1]) + fabs(e[2]) + fabs(e[3]);
-					rabs[1] += fabs(e[6]) + fabs(e[7]);
-					rabs[2] += fabs(e[11]);
+					s0 += fabs(e0);
+					s1 += fabs(e1);
+					cabs[k] += fabs(c0) + fabs(c1);
 				}
 			}
 		}
 #pragma unroll
-		for (int off = 16; off > 0; off >>= 1)
-#pragma unroll
-			for (int a = 0; a < 4; a++) {
-				if (RES) racc[a] += __shfl_xor_sync(0xffffffffu, racc[a], off);
-				if (NORM) rabs[a] += __shfl_xor_sync(0xffffffffu, rabs[a], off);
+		for (int off = 2; off < 32; off <<= 1) {
+			if (RES) {
+				r0 += __shfl_xor_sync(0xffffffffu, r0, off);
+				r1 += __shfl_xor_sync(0xffffffffu, r1, off);
 			}
-		if (lane < 4) {
-			const int i = 4 * ti + lane;
-			const double ra = lane == 0 ? racc[0] : (lane == 1 ? racc[1] : (lane == 2 ? racc[2] : racc[3]));
-			if (RES) r[i] = (i < n ? b[i] : 0.0) - ra;
-			if (NORM) asum[i] = lane == 0 ? rabs[0] : (lane == 1 ? rabs[1] : (lane == 2 ? rabs[2] : rabs[3]));
+			if (NORM) {
+				s0 += __shfl_xor_sync(0xffffffffu, s0, off);
+				s1 += __shfl_xor_sync(0xffffffffu, s1, off);
+			}
 		}
+		if (lane < 2) {
+			if (RES) {
+				r[gi0] = (gi0 < n ? b[gi0] : 0.0) - r0;
+				r[gi0 + 1] = (gi0 + 1 < n ? b[gi0 + 1] : 0.0) - r1;
+			}
+			if (NORM) {
+				asum[gi0] = s0;
+				asum[gi0 + 1] = s1;
+			}
+		}
+	}
+	// the two lanes of a column (rows 0,1 and 2,3 of each tile) combined
+#pragma unroll
+	for (int k = 0; k < KMAX; k++) {
+		if (RES) cacc[k] += __shfl_xor_sync(0xffffffffu, cacc[k], 1);
+		if (NORM) cabs[k] += __shfl_xor_sync(0xffffffffu, cabs[k], 1);
 	}
 	__syncthreads();
 	// column parts: subtracted from r (added to asum) one warp after the
 	// other, in warp order
 	for (int wv = 0; wv < nw; wv++) {
-		if (warp == wv) {
+		if (warp == wv && !(lane & 1)) {
 #pragma unroll
-			for (int m = 0; m < 2; m++) {
-				const int tj = lane + 32 * m;
-				if (tj < P) {
-#pragma unroll
-					for (int q = 0; q < 4; q++) {
-						if (RES) r[4 * tj + q] -= cacc[m][q];
-						if (NORM) asum[4 * tj + q] += cabs[m][q];
-					}
+			for (int k = 0; k < KMAX; k++) {
+				const int J = 16 * k + jl;
+				if (J < 4 * P) {
+					if (RES) r[J] -= cacc[k];
+					if (NORM) asum[J] += cabs[k];
 				}
 			}
 		}
 		__syncthreads();
 	}
 }
+
+// pieces of the longest tile row the kernel variant takes (its largest n)
+template <int NT, int MINB>
+struct ResShape {
+	static constexpr int KMAX = NT == 64 ? 4 : (MINB == 4 ? 8 : (MINB == 3 ? 11 : (MINB == 2 ? 14 : 16)));
+};
 
 template <typename T, bool MIXED, int NT, int MINB>
 __global__ void __launch_bounds__(NT, MINB) k_posv(int cls, int max_n, PosvWs ws, const int *__restrict__ nvec,
@@ -465,16 +474,17 @@ __global__ void __launch_bounds__(NT, MINB) k_posv(int cls, int max_n, PosvWs ws
 			__syncthreads();
 			// ||A||_inf (row sums of |A|) once, before the first residual
 			// (the first pass also accumulates the row sums of |A|: one read of A)
+			constexpr int KM = ResShape<NT, MINB>::KMAX;
 			if (slot) {
 				if (it == 0)
-					sym_residual<true, true, true>(slot, 0, n, bg, xs, rs, asum);
+					sym_residual<true, true, true, KM>(slot, 0, n, bg, xs, rs, asum);
 				else
-					sym_residual<true, true, false>(slot, 0, n, bg, xs, rs, asum);
+					sym_residual<true, true, false, KM>(slot, 0, n, bg, xs, rs, asum);
 			} else {
 				if (it == 0)
-					sym_residual<false, true, true>(a.p, a.cn, n, bg, xs, rs, asum);
+					sym_residual<false, true, true, KM>(a.p, a.cn, n, bg, xs, rs, asum);
 				else
-					sym_residual<false, true, false>(a.p, a.cn, n, bg, xs, rs, asum);
+					sym_residual<false, true, false, KM>(a.p, a.cn, n, bg, xs, rs, asum);
 			}
 			// norms
 			double rm = 0.0, xm = 0.0;
