@@ -252,6 +252,29 @@ __device__ double block_max(double v, double *red) {
 	return r;
 }
 
+// CTA-wide maxima of N values at once (one reduction, two barriers for all)
+template <int N>
+__device__ void block_max_n(double (&v)[N], double *red) {
+	const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+#pragma unroll
+	for (int off = 16; off > 0; off >>= 1)
+#pragma unroll
+		for (int e = 0; e < N; e++) v[e] = fmax(v[e], __shfl_down_sync(0xffffffffu, v[e], off));
+	if (lane == 0)
+#pragma unroll
+		for (int e = 0; e < N; e++) red[8 * e + warp] = v[e];
+	__syncthreads();
+	if (threadIdx.x < N) {
+		double m = 0.0;
+		for (int w = 0; w < nw; w++) m = fmax(m, red[8 * threadIdx.x + w]);
+		red[32 + threadIdx.x] = m;
+	}
+	__syncthreads();
+#pragma unroll
+	for (int e = 0; e < N; e++) v[e] = red[32 + e];
+	__syncthreads();
+}
+
 // r = b - A x (FP64), A symmetric given by its lower triangle, in one pass
 // over the lower triangle (every element read once).
 // LP = false: A in BLASFEO panel-major storage (tile row ti at base + 4*ti*cn);
@@ -486,19 +509,27 @@ __global__ void __launch_bounds__(NT, MINB) k_posv(int cls, int max_n, PosvWs ws
 				else
 					sym_residual<false, true, false, KM>(a.p, a.cn, n, bg, xs, rs, asum);
 			}
-			// norms
-			double rm = 0.0, xm = 0.0;
-			for (int i = tid; i < n; i += nt) {
-				rm = fmax(rm, fabs(rs[i]));
-				xm = fmax(xm, fabs(xs[i]));
-			}
-			rm = block_max<T>(rm, misc);
-			xm = block_max<T>(xm, misc);
-			if (it == 0) {
-				// ||A||_inf: row sums of |A| accumulated by the first residual pass
-				double am = 0.0;
-				for (int i = tid; i < n; i += nt) am = fmax(am, asum[i]);
-				anorm = block_max<T>(am, misc);
+			// norms (on the first pass also ||A||_inf from the row sums of |A|
+			// that the residual accumulated), reduced together
+			double rm, xm;
+			{
+				double m3[3] = {0.0, 0.0, 0.0};
+				for (int i = tid; i < n; i += nt) {
+					m3[0] = fmax(m3[0], fabs(rs[i]));
+					m3[1] = fmax(m3[1], fabs(xs[i]));
+					if (it == 0) m3[2] = fmax(m3[2], asum[i]);
+				}
+				if (it == 0) {
+					block_max_n<3>(m3, misc);
+					anorm = m3[2];
+				} else {
+					double m2[2] = {m3[0], m3[1]};
+					block_max_n<2>(m2, misc);
+					m3[0] = m2[0];
+					m3[1] = m2[1];
+				}
+				rm = m3[0];
+				xm = m3[1];
 			}
 			it++;
 			bnorm_res = (anorm > 0.0 && xm > 0.0) ? rm / (anorm * xm) : (rm == 0.0 ? 0.0 : INFINITY);
