@@ -618,12 +618,12 @@ def main():
     achieved = bytes_pass / (ms_mixed * 1e-3) / 1e9
     # DRAM bytes of one call: ncu capture of the same call on 2,000 systems of
     # this distribution (summary under profiles/, k_posv_f32_cfg3_2000_dram):
-    # 185,386,240 B of DRAM traffic against 178,497,336 algorithmic bytes,
+    # 185,359,872 B of DRAM traffic against 178,497,336 algorithmic bytes,
     # scaled to this call by its algorithmic bytes
-    traffic = bytes_pass * (185386240.0 / 178497336.0)
+    traffic = bytes_pass * (185359872.0 / 178497336.0)
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak_bw, "unit": "GB/s", "frac": achieved / peak_bw,
                 "traffic": traffic, "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of the same "
-                "call on 2,000 systems of the distribution, scaled by algorithmic bytes (ratio 1.039)",
+                "call on 2,000 systems of the distribution, scaled by algorithmic bytes (ratio 1.038)",
                 "peak_source": peak_src,
                 "kernel": "k_posv<float,true> (all size classes of one blasfeo_dsposv_l_vbatch call)",
                 "algorithmic_bytes_per_launch": bytes_pass,
