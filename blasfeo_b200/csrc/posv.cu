@@ -742,9 +742,12 @@ int posv_run(int batch, const int *n, int max_n, const void *sA, const void *sb,
 	const cudaStream_t s0 = s;
 	int status = BLASFEO_B200_OK;
 	for (int ci = 0; ci < nc && status == BLASFEO_B200_OK; ci++) {
-		// order (measured): the mixed solver smallest class first, the plain
-		// one largest first
-		const int c = MIXED ? ci : nc - 1 - ci;
+		// order (measured): the plain solver largest class first; the mixed
+		// one its largest class first (one CTA per SM, the longest), then the
+		// others smallest first on alternating streams, which fill the SMs
+		// that the largest class's last systems leave idle (20,000 systems:
+		// 8.88 -> 8.75 ms against smallest first throughout)
+		const int c = !MIXED ? nc - 1 - ci : (ci == 0 ? nc - 1 : ci - 1);
 		const cudaStream_t s = (two && (ci & 1)) ? side : s0;
 		const bool glob = need_global && c == nc - 1;
 		if (glob) {
