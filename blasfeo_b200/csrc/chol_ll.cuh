@@ -44,8 +44,9 @@ __device__ __forceinline__ double ll_ld(const PMat<double> &d, int i, int k, int
 
 // Factor the n x n lower triangle of c into d (lower triangle of L, 1/L_jj in
 // d.d[j]); *bad (shared, zeroed by the caller) receives the first
-// non-positive pivot j+1.  All NT threads of the CTA call it.
-template <int NT>
+// non-positive pivot j+1.  All NT threads of the CTA call it.  FR: fragment
+// rows a warp updates at a time (its accumulators: 8 FR doubles per lane).
+template <int NT, int FR = 4>
 __device__ void chol_ll(const PMat<double> &c, const PMat<double> &d, int n, double *smem, int *bad) {
 	constexpr int NW = NT / 32;
 	double *pan = smem;
@@ -57,11 +58,11 @@ __device__ void chol_ll(const PMat<double> &c, const PMat<double> &d, int n, dou
 		const int c0 = 16 * K;
 		const int m = n - c0;
 		const int R = (m + 7) >> 3;
-		// ---- panel update: up to 4 fragment rows per warp at a time ----
-		for (int f0 = warp; f0 < R; f0 += 4 * NW) {
-			double acc[4][2][2];
+		// ---- panel update: up to FR fragment rows per warp at a time ----
+		for (int f0 = warp; f0 < R; f0 += FR * NW) {
+			double acc[FR][2][2];
 #pragma unroll
-			for (int u = 0; u < 4; u++) {
+			for (int u = 0; u < FR; u++) {
 				const int row = c0 + 8 * (f0 + u * NW) + r;
 #pragma unroll
 				for (int fc = 0; fc < 2; fc++)
@@ -80,18 +81,18 @@ __device__ void chol_ll(const PMat<double> &c, const PMat<double> &d, int n, dou
 			}
 #pragma unroll 2
 			for (int k = 0; k < c0; k += 8) {
-				double a0[4], a1[4];
+				double a0[FR], a1[FR];
 				const double b00 = ll_ld(d, c0 + r, k + q, n), b01 = ll_ld(d, c0 + 8 + r, k + q, n);
 				const double b10 = ll_ld(d, c0 + r, k + 4 + q, n), b11 = ll_ld(d, c0 + 8 + r, k + 4 + q, n);
 #pragma unroll
-				for (int u = 0; u < 4; u++) {
+				for (int u = 0; u < FR; u++) {
 					const int row = c0 + 8 * (f0 + u * NW) + r;
 					const bool act = f0 + u * NW < R;
 					a0[u] = act ? ll_ld(d, row, k + q, n) : 0.0;
 					a1[u] = act ? ll_ld(d, row, k + 4 + q, n) : 0.0;
 				}
 #pragma unroll
-				for (int u = 0; u < 4; u++) {
+				for (int u = 0; u < FR; u++) {
 					if (f0 + u * NW < R) {  // warp-uniform
 						ll_dmma(acc[u][0][0], acc[u][0][1], a0[u], b00);
 						ll_dmma(acc[u][1][0], acc[u][1][1], a0[u], b01);
@@ -101,7 +102,7 @@ __device__ void chol_ll(const PMat<double> &c, const PMat<double> &d, int n, dou
 				}
 			}
 #pragma unroll
-			for (int u = 0; u < 4; u++) {
+			for (int u = 0; u < FR; u++) {
 				const int pr = 8 * (f0 + u * NW) + r;  // panel row
 				if (f0 + u * NW < R) {
 #pragma unroll

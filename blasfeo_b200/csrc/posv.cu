@@ -561,6 +561,10 @@ __host__ __device__ inline size_t posv_slot_elems(int max_n) {
 	return p4 * p4 + (size_t)(max_n + 15) / 16 * 16;
 }
 constexpr int POSV_GLOBAL_NT = 128;
+// fragment rows per warp in the factorization's panel updates
+#ifndef POSV_GLOBAL_FR
+#define POSV_GLOBAL_FR 1
+#endif
 __global__ void __launch_bounds__(POSV_GLOBAL_NT, 4)
     k_posv_global(int cls, int max_n, PosvWs ws, const int *__restrict__ nvec, const DevDesc<double> *__restrict__ sA,
                   const DevVec<double> *__restrict__ sb, const DevVec<double> *__restrict__ sx, double *slots,
@@ -597,7 +601,7 @@ __global__ void __launch_bounds__(POSV_GLOBAL_NT, 4)
 		a.ri = a.cj = 0;
 		const double *bg = sb[sys].pa;
 		for (int i = tid; i < n; i += POSV_GLOBAL_NT) y[i] = bg[i];
-		chol_ll<POSV_GLOBAL_NT>(a, L, n, pg_smem, &s_bad);
+		chol_ll<POSV_GLOBAL_NT, POSV_GLOBAL_FR>(a, L, n, pg_smem, &s_bad);
 		trsv_ll_fwd<POSV_GLOBAL_NT>(L, n, y);
 		trsv_ll_bwd<POSV_GLOBAL_NT>(L, n, y);
 		double *xg = sx[sys].pa;

@@ -6,11 +6,19 @@
 
 namespace {
 
-// 128 threads, 4 resident CTAs per SM: the serial panel chain of one instance
-// is hidden behind the other instances on the SM
+// 128 threads, POTRF_LL_MINB resident CTAs per SM: the serial panel chain of
+// one instance is hidden behind the other instances on the SM, so occupancy
+// pays for a few spilled registers; POTRF_LL_FR fragment rows per warp in the
+// panel update
+#ifndef POTRF_LL_MINB
+#define POTRF_LL_MINB 6
+#endif
+#ifndef POTRF_LL_FR
+#define POTRF_LL_FR 1
+#endif
 constexpr int LL_NT = 128;
 
-__global__ void __launch_bounds__(LL_NT, 4)
+__global__ void __launch_bounds__(LL_NT, POTRF_LL_MINB)
     k_potrf_ll(SizeArg sz, MatArg<double> C, MatArg<double> D, int *info, int min_n, int max_n) {
 	extern __shared__ __align__(16) double ll_smem[];
 	__shared__ int s_bad;
@@ -19,7 +27,7 @@ __global__ void __launch_bounds__(LL_NT, 4)
 	if (n <= min_n || n > max_n) return;
 	if (threadIdx.x == 0) s_bad = 0;
 	__syncthreads();
-	chol_ll<LL_NT>(C.get(b), D.get(b), n, ll_smem, &s_bad);
+	chol_ll<LL_NT, POTRF_LL_FR>(C.get(b), D.get(b), n, ll_smem, &s_bad);
 	if (info && threadIdx.x == 0) info[b] = s_bad;
 }
 
