@@ -47,9 +47,9 @@ __device__ __forceinline__ void cp_async16(uint32_t dst, const void *src) {
 // diagonal tile)
 __host__ __device__ constexpr int lower_panels(int n8) { return 8 * (n8 / 4) * (n8 / 4 + 1); }
 
-template <int N8, int WPC>
-__global__ void __launch_bounds__(32 * WPC) k_potrf_dmma(int batch, SizeArg sz, MatArg<double> C, MatArg<double> D,
-                                                         int *info) {
+template <int N8, int WPC, int MINB>
+__global__ void __launch_bounds__(32 * WPC, MINB) k_potrf_dmma(int batch, SizeArg sz, MatArg<double> C,
+                                                               MatArg<double> D, int *info) {
 	constexpr int NB = N8 * (N8 + 1) / 2;
 	const int lane = threadIdx.x & 31;
 	const int b = blockIdx.x * WPC + (threadIdx.x >> 5);
@@ -176,8 +176,12 @@ __global__ void __launch_bounds__(32 * WPC) k_potrf_dmma(int batch, SizeArg sz, 
 template <int N8>
 void launch_n8(int batch, SizeArg sz, MatArg<double> C, MatArg<double> D, int *info, cudaStream_t s) {
 	constexpr int WPC = N8 <= 4 ? 4 : (N8 <= 6 ? 2 : 1);
+	// n in 49..56: 168 registers (the fragments still fit) for 12 resident
+	// warps per SM instead of 8 (measured 3.7 -> 4.4 TF/s at n = 56); at
+	// n = 64 the same cap spills fragments and loses (4.4 -> 2.9 TF/s)
+	constexpr int MINB = N8 == 7 ? 12 : 1;
 	const size_t smem = (size_t)WPC * lower_panels(8 * N8) * sizeof(double);
-	k_potrf_dmma<N8, WPC><<<(batch + WPC - 1) / WPC, 32 * WPC, smem, s>>>(batch, sz, C, D, info);
+	k_potrf_dmma<N8, WPC, MINB><<<(batch + WPC - 1) / WPC, 32 * WPC, smem, s>>>(batch, sz, C, D, info);
 }
 
 }  // namespace
