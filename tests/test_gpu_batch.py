@@ -45,7 +45,7 @@ def batch_of(bf, prec, arr):
 
 
 @pytest.mark.parametrize("prec", ["d", "s"])
-@pytest.mark.parametrize("n", [4, 16, 23, 64])
+@pytest.mark.parametrize("n", [4, 16, 23, 53, 64, 96, 150])
 def test_potrf_batch(bf, orc, prec, n):
     import torch
     rng = np.random.default_rng(n)

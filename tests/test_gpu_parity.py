@@ -83,7 +83,7 @@ def test_syrk_ln(bf, orc, prec, mk):
     assert relfro(dD.unpack(), hD.get()) <= TOL[prec]
 
 
-POTRF_N = [1, 2, 3, 4, 5, 7, 13, 16, 17, 31, 33, 60, 64, 100, 129, 200, 257, 300, 384]
+POTRF_N = [1, 2, 3, 4, 5, 7, 13, 16, 17, 31, 33, 50, 56, 60, 64, 100, 129, 200, 257, 300, 384]
 
 
 @pytest.mark.parametrize("prec", ["d", "s"])
