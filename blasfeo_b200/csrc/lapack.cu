@@ -1334,7 +1334,7 @@ inline size_t lu_smem_bytes(int max_m, int max_n, size_t esz) {
 // built-in rule for getrf (qr = false) and geqrf (qr = true), from uniform
 // batches timed on the B200 at n = 32..384: the shared-memory kernel with 128
 // threads for small blocks, the blocked global-memory kernels above (getrf:
-// 128 threads with 4 blocks per SM up to n = 160, with 2 up to 224, then 256
+// 128 threads with 4 blocks per SM up to n = 96, with 3 up to 224, then 256
 // threads; geqrf: shared memory up to 64 rows, the SIMT update up to 192,
 // then the DMMA update with 512 threads)
 inline int pick_lu_variant(int variant, int max_m, int max_n, bool qr = false) {
@@ -1343,7 +1343,7 @@ inline int pick_lu_variant(int variant, int max_m, int max_n, bool qr = false) {
 		if (mx <= 48)
 			variant = 3;
 		else if (!qr)
-			variant = mx <= 160 ? 0 : (mx <= 224 ? 1 : 2);
+			variant = mx <= 96 ? 0 : (mx <= 224 ? 1 : 2);
 		else
 			variant = mx <= 64 ? 3 : (mx <= 192 ? 0 : 2);
 	}
@@ -1359,9 +1359,10 @@ int getrf_launch(int batch, SizeArg sz, MatArg<T> C, MatArg<T> D, int *ipiv, lon
 	const int cap = (int)smem;
 	variant = pick_lu_variant(variant, max_m, max_n);
 	switch (variant) {
-	// blocked: 128 threads with 4 or 2 blocks per SM (register cap), 256 threads
+	// blocked: 128 threads with 4 or 3 blocks per SM (register cap; FP64 variant 1
+	// spills a little at 3, faster than 2: n = 224 2.25 -> 2.65 TF/s), 256 threads
 	case 0: launch_getrf_blk<T, 128, 4>(batch, sz, -1, max_m, max_n, C, D, ipiv, ipiv_stride, info, s, piv); break;
-	case 1: launch_getrf_blk<T, 128, 2>(batch, sz, -1, max_m, max_n, C, D, ipiv, ipiv_stride, info, s, piv); break;
+	case 1: launch_getrf_blk<T, 128, sizeof(T) == 8 ? 3 : 2>(batch, sz, -1, max_m, max_n, C, D, ipiv, ipiv_stride, info, s, piv); break;
 	case 2: launch_getrf_blk<T, 256, 1>(batch, sz, -1, max_m, max_n, C, D, ipiv, ipiv_stride, info, s, piv); break;
 	case 3: launch_getrf<T, 128, true>(batch, sz, cap, smem, C, D, ipiv, ipiv_stride, info, s, piv); break;
 	case 4: launch_getrf<T, 256, true>(batch, sz, cap, smem, C, D, ipiv, ipiv_stride, info, s, piv); break;

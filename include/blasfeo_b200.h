@@ -425,7 +425,7 @@ int blasfeo_dgeqrf_vbatch(int batch, const int *m, const int *n, int max_m, int 
  * op 1 potrf_l: 0..3 shared memory with 64/128/256/512 threads, 4 global
  *   memory, 5 one warp per instance on the FP64 tensor cores (max_m <= 64;
  *   larger batches take the heuristic);
- * op 2 getrf_rp: 0..2 blocked in global memory (128 threads with 4 or 2
+ * op 2 getrf_rp: 0..2 blocked in global memory (128 threads with 4 or 3
  *   blocks per SM, 256 threads), 3..5 shared memory with 128/256/512 threads;
  * op 3 geqrf: 0..2 blocked in global memory (256 threads with the SIMT
  *   trailing update, 256 and 512 threads with the FP64 tensor-core update), 3..5
