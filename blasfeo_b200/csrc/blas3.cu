@@ -361,7 +361,7 @@ void trsm_rltn_kernel(int batch, SizeArg sz, int m, int n, T alpha, MatArg<T> A,
 	else {
 		const size_t smem = (2 * 64 * 64 + 64) * sizeof(T);
 		auto kern = k_trsm_rltn_blk<T, UNIT, TPR64>;
-		if (smem > 48 * 1024) cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+		bf::smem_optin(kern, smem);
 		kern<<<grid, 64 * TPR64, smem, s>>>(sz, alpha, A, B, D);
 	}
 }

@@ -38,6 +38,17 @@ unsigned int wait_limit();                // polls of a bounded mbarrier wait (b
 // this host thread's second stream on the current device and its fork / join
 // events (false if they cannot be made: then run on one stream)
 bool side_stream(cudaStream_t *stream, cudaEvent_t *fork, cudaEvent_t *join);
+// Let `kern` launch with `dyn` bytes of dynamic shared memory: the 48 KB that
+// a kernel gets without opting in cover its static and dynamic shared memory
+// together, so a launch whose dynamic part alone is below 48 KB can still
+// need the opt-in
+template <typename K>
+inline void smem_optin(K *kern, size_t dyn) {
+	cudaFuncAttributes a;
+	const size_t st = cudaFuncGetAttributes(&a, (const void *)kern) == cudaSuccess ? a.sharedSizeBytes : 0;
+	if (dyn + st > 48 * 1024)
+		cudaFuncSetAttribute((const void *)kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn);
+}
 
 template <typename T> struct MatT;
 template <> struct MatT<double> { typedef struct blasfeo_dmat type; typedef struct blasfeo_dmat_batch batch; typedef struct blasfeo_dvec vec; };

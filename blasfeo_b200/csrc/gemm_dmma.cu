@@ -177,7 +177,7 @@ int launch_dmma(int batch, SizeArg sz, int max_m, int max_n, double alpha, MatAr
 	constexpr int NT = (BM / 32) * (BN / 32) * 32;
 	const size_t smem = (size_t)DM_STAGES * (BM + BN) * DM_BK * sizeof(double);
 	auto kern = k_dgemm_nt_dmma<BM, BN, LOWER>;
-	if (smem > 48 * 1024) cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+	bf::smem_optin(kern, smem);
 	const int tm = cdiv(max_m, BM), tn = cdiv(max_n, BN);
 	const long long ctas = (long long)batch * tm * tn;
 	if (ctas > 0x7fffffffLL) return BLASFEO_B200_ENOTSUP;

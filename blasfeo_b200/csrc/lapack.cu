@@ -951,8 +951,11 @@ __device__ __noinline__ void qr_update_dmma(const PMat<double> &d, const double 
 // Shared memory: (m + 4) x 17 panel, 16 x 17 T and V^T V.
 // DMMA: the trailing update on the FP64 tensor cores (FP64 only; needs the
 // V^T C buffer and more registers, so it pays from ~128 x 256 blocks on)
+// FP64 with DMMA at 256 threads: 128 registers (a few spilled) for 2 CTAs per
+// SM: 2.18 -> 2.90 TF/s at 256 x 128, 3.29 -> 3.87 at 384 x 192 against the
+// 512-thread variant that the size rule took before
 template <typename T, int NT, bool DMMA>
-__global__ void __launch_bounds__(NT) k_geqrf_blk(SizeArg sz, MatArg<T> C, MatArg<T> D, int smem_cap, int max_m,
+__global__ void __launch_bounds__(NT, (DMMA && NT == 256 && sizeof(T) == 8) ? 2 : 1) k_geqrf_blk(SizeArg sz, MatArg<T> C, MatArg<T> D, int smem_cap, int max_m,
                                                    int max_n) {
 	extern __shared__ __align__(16) unsigned char smem_raw[];
 	__shared__ T s_red[33];
@@ -1167,7 +1170,7 @@ template <typename T, int NT, int MINB>
 void launch_potrf_smem(int batch, SizeArg sz, int max_m, size_t smem, MatArg<T> C, MatArg<T> D, int *info,
                        cudaStream_t s, int min_n = 0) {
 	auto kern = k_potrf_smem<T, NT, MINB>;
-	if (smem > 48 * 1024) cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+	bf::smem_optin(kern, smem);
 	kern<<<batch, NT, smem, s>>>(sz, C, D, info, max_m, min_n);
 }
 }  // namespace
@@ -1283,7 +1286,7 @@ template <typename T, int NT, bool SMEM>
 void launch_getrf(int batch, SizeArg sz, int cap, size_t smem, MatArg<T> C, MatArg<T> D, int *ipiv,
                   long long ipiv_stride, int *info, cudaStream_t s, bool piv = true) {
 	auto kern = k_getrf<T, NT, SMEM>;
-	if (smem > 48 * 1024) cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+	bf::smem_optin(kern, smem);
 	kern<<<batch, NT, smem, s>>>(sz, C, D, ipiv, ipiv_stride, info, cap, piv);
 }
 
@@ -1300,13 +1303,13 @@ void launch_getrf_blk(int batch, SizeArg sz, int cap, int max_m, int max_n, MatA
 		launch_getrf<T, 512, false>(batch, sz, cap, 0, C, D, ipiv, ipiv_stride, info, s, piv);
 		return;
 	}
-	if (smem > 48 * 1024) cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+	bf::smem_optin(kern, smem);
 	kern<<<batch, NT, smem, s>>>(sz, C, D, ipiv, ipiv_stride, info, cap, max_m, piv);
 }
 template <typename T, int NT, bool SMEM>
 void launch_geqrf(int batch, SizeArg sz, int cap, size_t smem, MatArg<T> C, MatArg<T> D, cudaStream_t s) {
 	auto kern = k_geqrf<T, NT, SMEM>;
-	if (smem > 48 * 1024) cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+	bf::smem_optin(kern, smem);
 	kern<<<batch, NT, smem, s>>>(sz, C, D, cap);
 }
 
@@ -1323,7 +1326,7 @@ void launch_geqrf_blk(int batch, SizeArg sz, int cap, int max_m, int max_n, MatA
 		launch_geqrf<T, 512, false>(batch, sz, cap, 0, C, D, s);
 		return;
 	}
-	if (smem > 48 * 1024) cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+	bf::smem_optin(kern, smem);
 	kern<<<batch, NT, smem, s>>>(sz, C, D, cap, max_m, max_n);
 }
 
@@ -1335,8 +1338,8 @@ inline size_t lu_smem_bytes(int max_m, int max_n, size_t esz) {
 // batches timed on the B200 at n = 32..384: the shared-memory kernel with 128
 // threads for small blocks, the blocked global-memory kernels above (getrf:
 // 128 threads with 4 blocks per SM up to n = 96, with 3 up to 224, then 256
-// threads; geqrf: shared memory up to 64 rows, the SIMT update up to 192,
-// then the DMMA update with 512 threads)
+// threads; geqrf: shared memory up to 64 rows, then the DMMA update with
+// 256 threads at 2 CTAs per SM)
 inline int pick_lu_variant(int variant, int max_m, int max_n, bool qr = false) {
 	if (variant < 0) {
 		const int mx = max_m > max_n ? max_m : max_n;
@@ -1345,7 +1348,7 @@ inline int pick_lu_variant(int variant, int max_m, int max_n, bool qr = false) {
 		else if (!qr)
 			variant = mx <= 96 ? 0 : (mx <= 224 ? 1 : 2);
 		else
-			variant = mx <= 64 ? 3 : (mx <= 192 ? 0 : 2);
+			variant = mx <= 64 ? 3 : 1;
 	}
 	return variant;
 }

@@ -621,7 +621,7 @@ int launch_posv(int c, int upper, size_t smem, int batch, int rslots, PosvWs ws,
                 const void *sb, const void *sx, int max_iter, double tol, int *iters, double *berr, int *info,
                 double *rs, cudaStream_t s) {
 	auto kern = k_posv<T, MIXED, NT, MINB>;
-	if (smem > 48 * 1024) cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+	bf::smem_optin(kern, smem);
 	int per_sm = 0;
 	cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, NT, smem);
 	if (per_sm < 1) per_sm = 1;
@@ -756,8 +756,7 @@ int posv_run(int batch, const int *n, int max_n, const void *sA, const void *sb,
 		const bool glob = need_global && c == nc - 1;
 		if (glob) {
 			const size_t gsm = ll_smem_bytes(max_n) + (size_t)max_n * sizeof(double);
-			if (gsm > 48 * 1024)
-				cudaFuncSetAttribute(k_posv_global, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)gsm);
+			bf::smem_optin(k_posv_global, gsm);
 			k_posv_global<<<gslots, POSV_GLOBAL_NT, gsm, s>>>(c, max_n, ws, n, (const DevDesc<double> *)sA,
 			                                                  (const DevVec<double> *)sb, (const DevVec<double> *)sx,
 			                                                  (double *)(wsp + slots_off), info);

@@ -50,7 +50,7 @@ int dpotrf_ll_launch(int batch, SizeArg sz, int min_n, int max_m, MatArg<double>
 	if (batch <= 0 || max_m <= min_n) return BLASFEO_B200_OK;
 	if (max_m > dpotrf_ll_max_n()) return BLASFEO_B200_ENOTSUP;
 	const size_t smem = ll_smem_bytes(max_m);
-	if (smem > 48 * 1024) cudaFuncSetAttribute(k_potrf_ll, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+	bf::smem_optin(k_potrf_ll, smem);
 	k_potrf_ll<<<batch, LL_NT, smem, s>>>(sz, C, D, info, min_n, max_m);
 	return check_launch();
 }

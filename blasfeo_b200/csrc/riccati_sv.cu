@@ -350,7 +350,7 @@ __global__ void __launch_bounds__(SV_WARPS * 32) k_ric_sv_refine(SvArgs a, MixAr
 }
 
 inline int grid_of(long long work, size_t smem, const void *kern) {
-	if (smem > 48 * 1024) cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+	bf::smem_optin(kern, smem);
 	int per_sm = 0;
 	cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, SV_WARPS * 32, smem);
 	if (per_sm < 1) per_sm = 1;

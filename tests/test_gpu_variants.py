@@ -142,6 +142,29 @@ def test_geqrf_variants(bf, orc, variant):
         assert relfro(d.diag_array()[:k], hD.diag(k)) <= tol, (m, n)
 
 
+@pytest.mark.parametrize("variant", [0, 1, 2])
+def test_geqrf_blocked_variants_small_batch(bf, orc, variant):
+    """The blocked QR kernels on a batch whose largest matrix is small
+    (96 x 48): the launch's dynamic shared memory is then just under 48 KB and
+    the kernel's static shared memory takes it over, so the launch must opt in
+    all the same."""
+    import torch
+    rng = np.random.default_rng(120 + variant)
+    dims = [(96, 48), (70, 40), (96, 7)]
+    M = [rng.standard_normal(d) for d in dims]
+    dC = [bf.DMat(m, n).pack(x) for (m, n), x in zip(dims, M)]
+    dD = [bf.DMat(m, n) for m, n in dims]
+    aC, aD = bf.descriptor_array(dC), bf.descriptor_array(dD)
+    mv, nv = ivec([d[0] for d in dims]), ivec([d[1] for d in dims])
+    st = bf.lib.blasfeo_dgeqrf_vbatch_variant(len(dims), P(mv), P(nv), 96, 48, P(aC), P(aD), variant, None)
+    assert st == 0
+    torch.cuda.synchronize()
+    for (m, n), x, d in zip(dims, M, dD):
+        hC, hD = host(m, n, x), host(m, n)
+        orc.geqrf("d", m, n, hC, 0, 0, hD, 0, 0)
+        assert relfro(d.unpack(), hD.get()) <= 1e-13, (m, n)
+
+
 def test_variant_out_of_range_rejected(bf):
     nv = ivec([4])
     d = bf.descriptor_array([bf.DMat(4, 4)])
