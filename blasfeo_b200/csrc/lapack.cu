@@ -1337,7 +1337,7 @@ inline size_t lu_smem_bytes(int max_m, int max_n, size_t esz) {
 // built-in rule for getrf (qr = false) and geqrf (qr = true), from uniform
 // batches timed on the B200 at n = 32..384: the shared-memory kernel with 128
 // threads for small blocks, the blocked global-memory kernels above (getrf:
-// 128 threads with 4 blocks per SM up to n = 96, with 3 up to 224, then 256
+// 128 threads with 4 blocks per SM up to n = 96, with 3 up to 288, then 256
 // threads; geqrf: shared memory up to 64 rows, then the DMMA update with
 // 256 threads at 2 CTAs per SM)
 inline int pick_lu_variant(int variant, int max_m, int max_n, bool qr = false) {
@@ -1346,7 +1346,7 @@ inline int pick_lu_variant(int variant, int max_m, int max_n, bool qr = false) {
 		if (mx <= 48)
 			variant = 3;
 		else if (!qr)
-			variant = mx <= 96 ? 0 : (mx <= 224 ? 1 : 2);
+			variant = mx <= 96 ? 0 : (mx <= 288 ? 1 : 2);
 		else
 			variant = mx <= 64 ? 3 : 1;
 	}
