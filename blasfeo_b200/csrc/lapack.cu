@@ -1365,7 +1365,15 @@ int getrf_launch(int batch, SizeArg sz, MatArg<T> C, MatArg<T> D, int *ipiv, lon
 	// blocked: 128 threads with 4 or 3 blocks per SM (register cap; FP64 variant 1
 	// spills a little at 3, faster than 2: n = 224 2.25 -> 2.65 TF/s), 256 threads
 	case 0: launch_getrf_blk<T, 128, 4>(batch, sz, -1, max_m, max_n, C, D, ipiv, ipiv_stride, info, s, piv); break;
-	case 1: launch_getrf_blk<T, 128, sizeof(T) == 8 ? 3 : 2>(batch, sz, -1, max_m, max_n, C, D, ipiv, ipiv_stride, info, s, piv); break;
+	case 1:
+		// FP64: 3 CTAs per SM up to n = 288 (the size rule's range), 2 above,
+		// where batches that mix sizes up to 384 ran faster with fewer spills
+		if (sizeof(T) == 8 && (max_m > 288 || max_n > 288))
+			launch_getrf_blk<T, 128, 2>(batch, sz, -1, max_m, max_n, C, D, ipiv, ipiv_stride, info, s, piv);
+		else
+			launch_getrf_blk<T, 128, sizeof(T) == 8 ? 3 : 2>(batch, sz, -1, max_m, max_n, C, D, ipiv, ipiv_stride,
+			                                                   info, s, piv);
+		break;
 	case 2: launch_getrf_blk<T, 256, 1>(batch, sz, -1, max_m, max_n, C, D, ipiv, ipiv_stride, info, s, piv); break;
 	case 3: launch_getrf<T, 128, true>(batch, sz, cap, smem, C, D, ipiv, ipiv_stride, info, s, piv); break;
 	case 4: launch_getrf<T, 256, true>(batch, sz, cap, smem, C, D, ipiv, ipiv_stride, info, s, piv); break;
