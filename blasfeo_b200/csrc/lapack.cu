@@ -1366,8 +1366,9 @@ int getrf_launch(int batch, SizeArg sz, MatArg<T> C, MatArg<T> D, int *ipiv, lon
 	// spills a little at 3, faster than 2: n = 224 2.25 -> 2.65 TF/s), 256 threads
 	case 0: launch_getrf_blk<T, 128, 4>(batch, sz, -1, max_m, max_n, C, D, ipiv, ipiv_stride, info, s, piv); break;
 	case 1:
-		// FP64: 3 CTAs per SM up to n = 288 (the size rule's range), 2 above,
-		// where batches that mix sizes up to 384 ran faster with fewer spills
+		// FP64: 3 CTAs per SM up to n = 288 (the size rule's range), 2 above:
+		// batches that mix sizes up to 384 ran faster with 2 (mixed-op stream,
+		// LU share 348 -> 329 ms)
 		if (sizeof(T) == 8 && (max_m > 288 || max_n > 288))
 			launch_getrf_blk<T, 128, 2>(batch, sz, -1, max_m, max_n, C, D, ipiv, ipiv_stride, info, s, piv);
 		else
