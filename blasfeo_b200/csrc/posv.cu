@@ -252,7 +252,8 @@ __device__ double block_max(double v, double *red) {
 	return r;
 }
 
-// CTA-wide maxima of N values at once (one reduction, two barriers for all)
+// CTA-wide maxima of N <= 3 values at once (one reduction, two barriers for
+// all); red: 51 doubles, up to 16 warps
 template <int N>
 __device__ void block_max_n(double (&v)[N], double *red) {
 	const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
@@ -262,16 +263,16 @@ __device__ void block_max_n(double (&v)[N], double *red) {
 		for (int e = 0; e < N; e++) v[e] = fmax(v[e], __shfl_down_sync(0xffffffffu, v[e], off));
 	if (lane == 0)
 #pragma unroll
-		for (int e = 0; e < N; e++) red[8 * e + warp] = v[e];
+		for (int e = 0; e < N; e++) red[16 * e + warp] = v[e];
 	__syncthreads();
 	if (threadIdx.x < N) {
 		double m = 0.0;
-		for (int w = 0; w < nw; w++) m = fmax(m, red[8 * threadIdx.x + w]);
-		red[32 + threadIdx.x] = m;
+		for (int w = 0; w < nw; w++) m = fmax(m, red[16 * threadIdx.x + w]);
+		red[48 + threadIdx.x] = m;
 	}
 	__syncthreads();
 #pragma unroll
-	for (int e = 0; e < N; e++) v[e] = red[32 + e];
+	for (int e = 0; e < N; e++) v[e] = red[48 + e];
 	__syncthreads();
 }
 
@@ -405,6 +406,7 @@ __global__ void __launch_bounds__(NT, MINB) k_posv(int cls, int max_n, PosvWs ws
                                               const DevVec<double> *__restrict__ sb,
                                               const DevVec<double> *__restrict__ sx, int max_iter, double tol,
                                               int *iters, double *berr, int *info, double *slots) {
+	static_assert(NT % 32 == 0 && NT <= 512, "block_max_n keeps up to 16 warps' partial maxima");
 	extern __shared__ __align__(16) unsigned char smem[];
 	const PosvPlan pl = posv_plan<T, MIXED>(max_n, NT);
 	// per-CTA FP64 copy of the lower panels (refinement residuals read it from
@@ -419,8 +421,8 @@ __global__ void __launch_bounds__(NT, MINB) k_posv(int cls, int max_n, PosvWs ws
 	double *rs = (double *)(smem + pl.r_off);
 	T *ybuf = (T *)(smem + pl.ybuf_off);
 	double *misc = (double *)(smem + pl.misc_off);
-	int *s_bad = (int *)(misc + 40);
-	int *s_item = (int *)(misc + 41);
+	int *s_bad = (int *)(misc + 60);
+	int *s_item = (int *)(misc + 61);
 	const int tid = threadIdx.x, nt = blockDim.x;
 	const int start = ws.start[cls], count = ws.count[cls];
 
