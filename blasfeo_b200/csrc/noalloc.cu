@@ -17,6 +17,9 @@
 //     device work;
 //   - the array is loaded with the library and stays resident on every GPU
 //     that uses the library until the process exits;
+//   - the size classes run one after the other on the caller's stream (the
+//     allocating entry point spreads them over a second stream that it
+//     creates on a host thread's first call, which can take device memory);
 //   - all calls share the one array: calls whose executions overlap on the
 //     GPU (different streams, or different host threads) race on it and must
 //     be serialised by the caller; one call's kernels reset the counters they
@@ -81,8 +84,10 @@ int blasfeo_dsposv_l_vbatch_noalloc(int batch, const int *n, int max_n, const st
 	void *scratch = nullptr;
 	int st = scratch_address(&scratch);
 	if (st != BLASFEO_B200_OK) return st;
-	return blasfeo_dsposv_l_vbatch(batch, n, max_n, sA, sb, sx, max_iter, tol, iters, berr, info, scratch,
-	                               kScratchBytes, stream);
+	// on the caller's stream only: the allocating entry point's second stream
+	// is created on a host thread's first call
+	return bf::dsposv_one_stream(batch, n, max_n, sA, sb, sx, max_iter, tol, iters, berr, info, scratch,
+	                             kScratchBytes, (cudaStream_t)stream);
 }
 
 }  // extern "C"

@@ -702,7 +702,7 @@ PosvLayout posv_layout(int batch, int max_n, bool use_slots) {
 template <typename T, bool MIXED>
 int posv_run(int batch, const int *n, int max_n, const void *sA, const void *sb, const void *sx, int max_iter,
              double tol, int *iters, double *berr, int *info, void *work, size_t work_bytes, cudaStream_t s,
-             bool use_slots) {
+             bool use_slots, bool one_stream = false) {
 	if (batch < 0 || !n || !sA || !sb || !sx || max_n < 0) return BLASFEO_B200_EINVAL;
 	if (batch == 0 || max_n == 0) return BLASFEO_B200_OK;
 	const PosvLayout lay = posv_layout<T, MIXED>(batch, max_n, use_slots);
@@ -740,7 +740,9 @@ int posv_run(int batch, const int *n, int max_n, const void *sA, const void *sb,
 	cudaStream_t side = nullptr;
 	cudaEvent_t fork = nullptr, join = nullptr;
 	// (the mapped path's per-CTA refinement slots: one set per stream)
-	const bool two = nc > 1 && bf::side_stream(&side, &fork, &join);
+	// (one_stream: the caller's stream only; the second stream and its events
+	// are created on a host thread's first call, which can take device memory)
+	const bool two = !one_stream && nc > 1 && bf::side_stream(&side, &fork, &join);
 	if (two) {
 		cudaEventRecord(fork, s);
 		cudaStreamWaitEvent(side, fork, 0);
@@ -842,3 +844,16 @@ int blasfeo_dsposv_l_vbatch_mapped(int batch, const int *n, int max_n, const str
 }
 
 }  // extern "C"
+
+namespace bf {
+
+// the mixed solver on the caller's stream alone (no per-thread second stream)
+// with a caller-provided workspace: the allocation-free entry point's path
+int dsposv_one_stream(int batch, const int *n, int max_n, const void *sA, const void *sb, const void *sx, int max_iter,
+                      double tol, int *iters, double *berr, int *info, void *work, size_t work_bytes,
+                      cudaStream_t stream) {
+	return posv_run<float, true>(batch, n, max_n, sA, sb, sx, max_iter, tol, iters, berr, info, work, work_bytes,
+	                             stream, false, true);
+}
+
+}  // namespace bf

@@ -40,4 +40,9 @@ namespace bf {
 int posv_tc_launch(int cls, int upper, int batch, PosvWs ws, const int *n, const void *sA, const void *sb,
                    const void *sx, int max_iter, double tol, int *iters, double *berr, int *info, cudaStream_t s);
 
+// The mixed solver on the caller's stream alone, with a caller-provided
+// workspace (posv.cu): the path of the allocation-free entry point.
+int dsposv_one_stream(int batch, const int *n, int max_n, const void *sA, const void *sb, const void *sx, int max_iter,
+                      double tol, int *iters, double *berr, int *info, void *work, size_t work_bytes,
+                      cudaStream_t stream);
 }  // namespace bf

@@ -610,7 +610,10 @@ int blasfeo_b200_mlp_adam(int nparams, float *params, const float *grads, float 
  * BLASFEO_B200_ENOTSUP.  All calls share the array: calls that overlap on the
  * GPU race and must be serialised by the caller.  The first call on a device
  * looks up the array's device address and caches it; make that first call
- * before any stream capture. */
+ * before any stream capture.  Under the CUDA driver's lazy module loading the
+ * first launch of each kernel (so the first call of each solver engine) may
+ * map memory for the kernel's code; a caller that must see no change in
+ * device memory at all makes one call per engine at start-up. */
 #define BLASFEO_B200_NOALLOC_MAX_BATCH 65536
 size_t blasfeo_dsposv_noalloc_scratch_bytes(void);
 int blasfeo_dsposv_l_vbatch_noalloc(int batch, const int *n, int max_n, const struct blasfeo_dmat *sA,

@@ -93,22 +93,33 @@ def test_noalloc_largest_size_and_tensor_engine_allocate_nothing():
     x_ref = W.x.clone()
     # first call on this device (looks up the static array's address; loads the module)
     assert _noalloc_call(lib, W, num, berr, info) == 0
+    # and a first call of the tensor-memory engine: under the driver's lazy
+    # module loading a kernel's first launch may map memory for its code, which
+    # is not an allocation of the entry point (the same call is repeated below)
+    assert lib.blasfeo_b200_set_posv_engine(2) == 0
+    assert _noalloc_call(lib, W, num, berr, info) == 0
+    assert lib.blasfeo_b200_set_posv_engine(0) == 0
     torch.cuda.synchronize()
     out = {}
 
     def worker():
         try:
             torch.cuda.set_device(0)
-            free0 = torch.cuda.mem_get_info()[0]
+            free = []
             for engine in (1, 2):  # SIMT, then the tensor-memory engine (the setting is per host thread)
                 assert lib.blasfeo_b200_set_posv_engine(engine) == 0
                 W.x.zero_()
                 info.fill_(-9)
+                torch.cuda.synchronize()
+                # free memory right around the call (torch's own first kernel
+                # launches on this thread stay outside the window)
+                f0 = torch.cuda.mem_get_info()[0]
                 st = _noalloc_call(lib, W, num, berr, info)
                 torch.cuda.synchronize()
+                free.append((f0, torch.cuda.mem_get_info()[0]))
                 out[engine] = (st, info.cpu().numpy().copy(), berr.cpu().numpy().copy(),
                                ((W.x - x_ref).norm() / x_ref.norm()).item())
-            out["free"] = (free0, torch.cuda.mem_get_info()[0])
+            out["free"] = free
         except Exception as ex:  # reported by the main thread
             out["error"] = repr(ex)
 
@@ -123,5 +134,5 @@ def test_noalloc_largest_size_and_tensor_engine_allocate_nothing():
         # tensor-memory engine rounds differently; both solutions are backward stable
         # to 1e-12, so they agree to about cond(A) * 1e-12 = 1e-6 (cond up to 1e6)
         assert diff <= (1e-12 if engine == 1 else 1e-5), (engine, diff)
-    free0, free1 = out["free"]
-    assert free0 == free1, (free0, free1)
+    for free0, free1 in out["free"]:
+        assert free0 == free1, (free0, free1)
